@@ -1,0 +1,354 @@
+"""Benchmark: U(1) two-site DMRG H_eff matvec and Lanczos step on B200.
+
+Workload (one GPU): spin-1/2 XXZ (Jz = Jxy = 1) two-site effective Hamiltonian with
+U(1) bond dimension D = 4096 (33 sectors q = -16..16, sizes ~ exp(-q^2/72)), MPO bond
+dimension 5, seeded ~N(0,1) Hermitian environments -- the precision configuration of
+the reference's DMRG path.  A "step" is one H_eff matvec over the resident operands.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--D 4096]
+
+Reported (one JSON line from rank 0):
+  value        algorithmic TFLOP/s of the matvec (block-pair GEMM flops of the order
+               L -> M1 -> M2 -> R, counted from the block structure) with inputs in HBM
+  e2e          the same metric through the public API with psi copied from pinned host
+               memory and H psi copied back inside every timed step
+  lanczos_s_per_step   device Lanczos (C++ driver, FP64 recurrence) seconds per iteration
+  roofline     the grouped-GEMM kernel against the measured cuBLAS DGEMM peak
+  cpu_baseline the reference algorithm restated on the host cores (oracle), bounded sample
+With --gpus N (torchrun) every rank runs an independent replica (the path does not
+shard at this size): value = all ranks' flops / max time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--D", type=int, default=4096)
+    ap.add_argument("--lanczos-iters", type=int, default=40)
+    ap.add_argument("--cpu-sample-s", type=float, default=15.0)
+    ap.add_argument("--precision", default="fp64")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        try:
+            import torch
+
+            u = str(torch.cuda.get_device_properties(index).uuid)
+            self.index = u if u.startswith("GPU-") else f"GPU-{u}"
+        except Exception:
+            pass
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                r = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                    "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if r.returncode == 0 and r.stdout.strip():
+                    self.rows.append([x.strip() for x in r.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, n in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def cpu_baseline_matvec(spec, mpo_vals, seed, sample_s, threads):
+    """Reference CPU algorithm (oracle restatement of BlockUniTensor::contract, OpenBLAS
+    dgemm) on the host cores: matvecs in the order L -> M1 -> M2 -> R until sample_s."""
+    import oracle as O
+    from cytnx_b200 import workloads as W
+
+    O.set_threads(threads)
+    psi, L, M1, M2, R = W.build_two_site(spec, mpo_vals, seed=seed, device=-1)
+
+    def to_o(u, labels):
+        bonds = [O.Bond(b.type(), b._qnums, b._degs) for b in u.bonds()]
+        lay = u._layout
+        data = u._data.numpy()
+        blocks = [data[o:o + s].reshape(sh) for o, s, sh in zip(lay.offs, lay.sizes, lay.shapes)]
+        return O.BlockTensor(bonds, labels, u.rowrank(), lay.itoi, blocks)
+
+    ops = {"psi": to_o(psi, ["-1", "-2", "-3", "-4"]), "L": to_o(L, ["-5", "-1", "0"]),
+           "R": to_o(R, ["-7", "-4", "3"]), "M1": to_o(M1, ["-5", "-6", "-2", "1"]),
+           "M2": to_o(M2, ["-6", "-7", "-3", "2"])}
+
+    def mv():
+        t = ops["L"].contract(ops["psi"])
+        t = t.contract(ops["M1"])
+        t = t.contract(ops["M2"])
+        return t.contract(ops["R"])
+
+    mv()  # warm
+    n, t0 = 0, time.perf_counter()
+    while True:
+        mv()
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= sample_s or n >= 50:
+            break
+    return el / n, n
+
+
+def main():
+    args = parse()
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    from cytnx_b200 import workloads as W
+
+    spec = W.xxz_spec(args.D)
+    mpo_vals = W.xxz_mpo_values(1.0, 1.0, 0.0)
+    workload = f"u1_xxz_two_site_heff_D{args.D}"
+    config_base = {"workload": workload, "D": args.D, "sectors": int(len(spec.dv)), "mpo_bond": 5, "d": 2,
+                   "order": "L->M1->M2->R", "l2": "inputs larger than L2 (operands + intermediates > 126 MB)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            if world > 1:
+                dist.destroy_process_group()
+            return
+        threads = os.cpu_count() or 1
+        # algorithmic flops from the block structure (host only)
+        import cytnx_b200 as c
+
+        sec, n = cpu_baseline_matvec(spec, mpo_vals, 0, max(2.0, min(args.cpu_sample_s, 60.0)), threads)
+        flops = _algo_flops_host(spec, mpo_vals)
+        val = flops / sec / 1e12
+        line = {"metric": "U(1) H_eff matvec TFLOP/s & Lanczos s/step, split-prec vs FP64, dE<=1e-9",
+                "impl": "reference", "value": val, "unit": "TFLOP/s", "n_gpus": args.gpus, "steps": n,
+                "warmup": 1, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded numpy PCG64)",
+                "config": dict(config_base, parallelism="cpu"),
+                "cpu_baseline": {"value": val, "unit": "TFLOP/s", "cores": threads, "kind": "port",
+                                 "sample": f"{n} matvecs at D={args.D} (oracle restatement, OpenBLAS dgemm)"},
+                "e2e": {"value": val, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import cytnx_b200 as c
+    from cytnx_b200 import _lib
+
+    dev = torch.device(f"cuda:{local}")
+    psi, L, M1, M2, R = W.build_two_site(spec, mpo_vals, seed=0, device=local)
+    H = c.TwoSiteHeff(L, M1, M2, R, psi, precision=args.precision)
+    H.bind()
+    flops = H.algorithmic_flops()
+    x = psi.flat_view()
+    y = torch.empty_like(x)
+    for _ in range(args.warmup):
+        H.apply_flat(x, y)
+    torch.cuda.synchronize()
+
+    # ---- device-resident timed region
+    sampler = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with sampler:
+        e0.record(st)
+        for _ in range(args.steps):
+            H.apply_flat(x, y)
+        e1.record(st)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        dist.barrier()
+    t_max = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    ms_max = float(t_max.item())
+    ms_step = ms_max / args.steps
+    value = world * flops * args.steps / (ms_max * 1e-3) / 1e12
+
+    # ---- per-kernel timing (CUDA events between the phases, same stream)
+    ms3 = (ctypes_double3 := (__import__("ctypes").c_double * 3)())
+    nl = __import__("ctypes").c_int()
+    _lib.check(_lib.lib().ctn_heff2_profile(H._h, x.data_ptr(), y.data_ptr(), 0, 10, ms3, __import__("ctypes").byref(nl),
+                                           _lib.stream_ptr()), "profile")
+    g1f = _lib.lib().ctn_heff2_gemm_flops(H._h, 1)
+    g4f = _lib.lib().ctn_heff2_gemm_flops(H._h, 4)
+    gemm_ms = ms3[0] + ms3[2]
+
+    # ---- end to end through the public API (pinned host psi in, host H psi out)
+    h_in = torch.empty(x.numel(), dtype=torch.float64, pin_memory=True)
+    h_in.copy_(x.cpu())
+    h_out = torch.empty_like(h_in, pin_memory=True)
+    for _ in range(2):
+        xd = h_in.to(dev, non_blocking=True)
+        out = H.matvec(psi.with_flat(xd))
+        h_out.copy_(out.flat_view(), non_blocking=True)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(st)
+    for _ in range(args.steps):
+        xd = h_in.to(dev, non_blocking=True)
+        out = H.matvec(psi.with_flat(xd))
+        h_out.copy_(out.flat_view(), non_blocking=True)
+    e3.record(st)
+    torch.cuda.synchronize()
+    t2 = torch.tensor([e2.elapsed_time(e3)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+    e2e_val = world * flops * args.steps / (float(t2.item()) * 1e-3) / 1e12
+
+    # ---- Lanczos step time (C++ driver, FP64 recurrence, host tridiagonal solve)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    E, vec, it = H.lanczos(psi, maxiter=args.lanczos_iters, cvgcrit=1e-300)
+    torch.cuda.synchronize()
+    lz = (time.perf_counter() - t0) / max(it, 1)
+
+    # ---- DGEMM peak for the roofline denominator (cuBLAS 8192^3, best of 5)
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    best = 1e9
+    for _ in range(5):
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(st)
+        torch.matmul(a, b)
+        s1.record(st)
+        torch.cuda.synchronize()
+        best = min(best, s0.elapsed_time(s1))
+    dgemm_tflops = 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+    del a, b
+
+    gemm_achieved = (g1f + g4f) / (gemm_ms * 1e-3) / 1e12
+    clocks = sampler.summary()
+    if rank == 0:
+        cpu = None
+        if world == 1 and os.environ.get("CTN_BENCH_NO_CPU") != "1":
+            threads = os.cpu_count() or 1
+            sec, n = cpu_baseline_matvec(spec, mpo_vals, 0, args.cpu_sample_s, threads)
+            cpu = {"value": flops / sec / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": "port",
+                   "sample": f"{n} H_eff matvecs at D={args.D} on the host (oracle restatement of "
+                             f"BlockUniTensor::contract, OpenBLAS dgemm), {sec:.3f} s each"}
+        pk, src = peaks()
+        line = {
+            "metric": "U(1) H_eff matvec TFLOP/s & Lanczos s/step, split-prec vs FP64, dE<=1e-9",
+            "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else args.precision, "data": "synthetic (seeded numpy PCG64)",
+            "config": dict(config_base, parallelism=f"replicas{world}", precision=args.precision),
+            "algorithmic_flops_per_matvec": flops,
+            "lanczos_s_per_step": lz, "lanczos_iters": it, "lanczos_energy": E,
+            "e2e": {"value": e2e_val, "unit": "TFLOP/s", "h2d_bytes_per_step": int(x.numel() * 8),
+                    "d2h_bytes_per_step": int(x.numel() * 8)},
+            "gpu_launches": int(nl.value) * args.steps,
+            "phase_ms": {"gemm_step1": ms3[0], "mpo_steps2_3": ms3[1], "gemm_step4": ms3[2]},
+            "roofline": {"bound": "fp64", "achieved": gemm_achieved, "peak": dgemm_tflops, "unit": "TFLOP/s",
+                         "frac": gemm_achieved / dgemm_tflops, "traffic": None,
+                         "kernel": "k_gemm_grouped_f64 (steps 1 and 4)",
+                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)"},
+            "peaks": {"hbm_gbs": pk.get("hbm_gbs"), "bf16_tflops": pk.get("bf16_tflops"), "source": src,
+                      "dgemm_tflops_measured": dgemm_tflops},
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _algo_flops_host(spec, mpo_vals):
+    """Algorithmic flops without a GPU: the planner counts block pairs on the host."""
+    from cytnx_b200.unitensor import contract_plan_flops, structure_only
+    from cytnx_b200 import workloads as W
+    from cytnx_b200.core import BD_KET, Bond
+
+    Vl = Bond(BD_KET, spec.qv.reshape(-1, 1), spec.dv)
+    Vr = Bond(BD_KET, spec.qv_r.reshape(-1, 1), spec.dv_r)
+    phys = Bond(BD_KET, np.array(spec.phys_q).reshape(-1, 1), [1] * len(spec.phys_q))
+    inner = Bond(BD_KET, np.array(spec.inner_q).reshape(-1, 1), [1] * len(spec.inner_q))
+    P = structure_only([Vl, phys.redirect(), phys.redirect(), Vr.redirect()], ["a", "s1", "s2", "b"])
+    L = structure_only([inner.redirect(), Vl.redirect(), Vl], ["w", "a", "ap"])
+    M1 = structure_only([inner, inner.redirect(), phys, phys.redirect()], ["w", "w1", "s1", "s1p"])
+    M2 = structure_only([inner, inner.redirect(), phys, phys.redirect()], ["w1", "w2", "s2", "s2p"])
+    R = structure_only([inner, Vr, Vr.redirect()], ["w2", "b", "bp"])
+    from cytnx_b200.heff import _struct_contract
+
+    f = contract_plan_flops(L, P)
+    T1 = _struct_contract(L, P)
+    f += contract_plan_flops(T1, M1)
+    T2 = _struct_contract(T1, M1)
+    f += contract_plan_flops(T2, M2)
+    T3 = _struct_contract(T2, M2)
+    f += contract_plan_flops(T3, R)
+    return f
+
+
+if __name__ == "__main__":
+    main()

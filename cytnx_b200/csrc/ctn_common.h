@@ -1,0 +1,49 @@
+// Shared helpers for the cytnx_b200 C ABI: thread-local error text, CUDA checks.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "../../include/cytnx_b200.h"
+
+namespace ctn {
+
+void set_error(const char *fmt, ...);
+
+inline ctn_status cuda_fail(cudaError_t e, const char *what, const char *file, int line) {
+  set_error("%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+  return CTN_ERR_CUDA;
+}
+
+inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+}  // namespace ctn
+
+#define CTN_CUDA(call)                                                 \
+  do {                                                                 \
+    cudaError_t e_ = (call);                                           \
+    if (e_ != cudaSuccess) return ctn::cuda_fail(e_, #call, __FILE__, __LINE__); \
+  } while (0)
+
+#define CTN_CHECK_LAUNCH()                                             \
+  do {                                                                 \
+    cudaError_t e_ = cudaGetLastError();                               \
+    if (e_ != cudaSuccess) return ctn::cuda_fail(e_, "kernel launch", __FILE__, __LINE__); \
+  } while (0)
+
+#define CTN_REQUIRE(cond, ...)                                         \
+  do {                                                                 \
+    if (!(cond)) {                                                     \
+      ctn::set_error(__VA_ARGS__);                                     \
+      return CTN_ERR_INVALID;                                          \
+    }                                                                  \
+  } while (0)
+
+#define CTN_TRY(call)                                                  \
+  do {                                                                 \
+    ctn_status s_ = (call);                                            \
+    if (s_ != CTN_OK) return s_;                                       \
+  } while (0)

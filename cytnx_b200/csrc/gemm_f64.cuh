@@ -1,0 +1,84 @@
+// Device-side task tables of the grouped FP64 GEMM and the owning host object.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "ctn_common.h"
+
+namespace ctn {
+
+struct GemmTaskD {
+  int64_t c_off;
+  int32_t m, n, ldc;
+  int32_t pair_begin, pair_count;
+  int32_t pad_;
+};
+struct GemmPairD {
+  int64_t a_off, b_off;
+  int32_t k, lda, ldb, flags;  // flags bit0: A stored [k][m]; bit1: B stored [n][k]
+};
+struct GemmTileD {
+  int32_t task;
+  int32_t m0, n0;
+};
+
+void build_tiles_f64(const std::vector<GemmTaskD> &tasks, const std::vector<GemmPairD> &pairs,
+                     std::vector<GemmTileD> &tiles);
+ctn_status launch_gemm_f64(const double *A, const double *B, double *C, const GemmTaskD *d_tasks,
+                           const GemmPairD *d_pairs, const GemmTileD *d_tiles, int64_t ntiles,
+                           cudaStream_t st);
+
+// Host tables + their device copy (uploaded once, on the first launch on a device).
+struct GroupedGemmF64 {
+  std::vector<GemmTaskD> tasks;
+  std::vector<GemmPairD> pairs;
+  std::vector<GemmTileD> tiles;
+  void *d_mem = nullptr;
+  int d_dev = -1;
+  double flops = 0.0;
+
+  void finalize() {
+    build_tiles_f64(tasks, pairs, tiles);
+    flops = 0.0;
+    for (const auto &t : tasks)
+      for (int p = 0; p < t.pair_count; ++p)
+        flops += 2.0 * t.m * (double)t.n * (double)pairs[t.pair_begin + p].k;
+  }
+  size_t table_bytes() const {
+    return tasks.size() * sizeof(GemmTaskD) + pairs.size() * sizeof(GemmPairD) +
+           tiles.size() * sizeof(GemmTileD) + 64;
+  }
+  ctn_status upload(cudaStream_t st) {
+    int dev = 0;
+    CTN_CUDA(cudaGetDevice(&dev));
+    if (d_mem && d_dev == dev) return CTN_OK;
+    if (d_mem) {
+      cudaFree(d_mem);
+      d_mem = nullptr;
+    }
+    CTN_CUDA(cudaMalloc(&d_mem, table_bytes()));
+    d_dev = dev;
+    char *p = (char *)d_mem;
+    if (!tasks.empty()) CTN_CUDA(cudaMemcpyAsync(p, tasks.data(), tasks.size() * sizeof(GemmTaskD), cudaMemcpyHostToDevice, st));
+    p += tasks.size() * sizeof(GemmTaskD);
+    if (!pairs.empty()) CTN_CUDA(cudaMemcpyAsync(p, pairs.data(), pairs.size() * sizeof(GemmPairD), cudaMemcpyHostToDevice, st));
+    p += pairs.size() * sizeof(GemmPairD);
+    if (!tiles.empty()) CTN_CUDA(cudaMemcpyAsync(p, tiles.data(), tiles.size() * sizeof(GemmTileD), cudaMemcpyHostToDevice, st));
+    // pageable host memory: make sure the copies finished before the vectors can change
+    CTN_CUDA(cudaStreamSynchronize(st));
+    return CTN_OK;
+  }
+  ctn_status run(const double *A, const double *B, double *C, cudaStream_t st) {
+    CTN_TRY(upload(st));
+    const char *p = (const char *)d_mem;
+    const GemmTaskD *dt = (const GemmTaskD *)p;
+    const GemmPairD *dp = (const GemmPairD *)(p + tasks.size() * sizeof(GemmTaskD));
+    const GemmTileD *dl = (const GemmTileD *)(p + tasks.size() * sizeof(GemmTaskD) + pairs.size() * sizeof(GemmPairD));
+    return launch_gemm_f64(A, B, C, dt, dp, dl, (int64_t)tiles.size(), st);
+  }
+  ~GroupedGemmF64() {
+    if (d_mem) cudaFree(d_mem);
+  }
+};
+
+}  // namespace ctn

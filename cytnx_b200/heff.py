@@ -1,0 +1,156 @@
+"""Two-site effective Hamiltonian as a planned operator (the DMRG Lanczos hot path).
+
+``TwoSiteHeff(L, M1, M2, R, psi)`` takes the network operands of
+example/DMRG/dmrg_two_sites_U1.py:29-34 (leg orders psi[a,s1,s2,b], L[w,a,a'],
+M1[w,w1,s1,s1'], M2[w1,w2,s2,s2'], R[w2,b,b']) and plans the matvec once in C++
+(``ctn_heff2_plan_create``): block pairing, MPO folding and the grouped-GEMM task
+tables are built on the host a single time; every ``matvec`` is then three launches.
+It is a ``LinOp``: ``linalg.Lanczos(Hop=H, Tin=psi, method="Gnd")`` drives it through
+the Python callback, and ``H.lanczos(psi)`` runs the same C++ driver with no Python
+in the loop.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Tuple
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import BlockDesc, CytnxError, Heff2Desc
+from .core import Device, Tensor, Type, require_cuda
+from .network import LinOp
+from .unitensor import UniTensor, UTenType, _desc, contract_plan_flops, layout_for, structure_only
+
+
+def _plain_desc(u: UniTensor, keep):
+    if u.uten_type() != UTenType.Block:
+        raise CytnxError("[TwoSiteHeff] operands must be BlockUniTensors")
+    u = u.contiguous()
+    return u, _desc(u._layout, None, u._layout.itoi, u._layout.shapes, keep)
+
+
+class TwoSiteHeff(LinOp):
+    def __init__(self, L: UniTensor, M1: UniTensor, M2: UniTensor, R: UniTensor, psi: UniTensor,
+                 precision: str = "fp64"):
+        super().__init__("mv", psi.shape()[0] * psi.shape()[1] * psi.shape()[2] * psi.shape()[3], Type.Double,
+                         psi.device())
+        for t, nm in ((L, "L"), (M1, "M1"), (M2, "M2"), (R, "R"), (psi, "psi")):
+            if t.dtype() != Type.Double:
+                raise CytnxError(f"[TwoSiteHeff] {nm} must be float64")
+        keep: list = []
+        self.L, dL = _plain_desc(L, keep)
+        self.M1, dM1 = _plain_desc(M1, keep)
+        self.M2, dM2 = _plain_desc(M2, keep)
+        self.R, dR = _plain_desc(R, keep)
+        self.psi_t, dP = _plain_desc(psi, keep)
+        require_cuda(self.L._data, "TwoSiteHeff")
+        out_bonds = [self.L.bonds()[2], self.M1.bonds()[3], self.M2.bonds()[3], self.R.bonds()[2]]
+        self.out_layout = layout_for(out_bonds)
+        if not np.array_equal(self.out_layout.itoi, self.psi_t._layout.itoi) or \
+                not np.array_equal(self.out_layout.shapes, self.psi_t._layout.shapes):
+            raise CytnxError("[TwoSiteHeff] the output block structure differs from psi's")
+        self.out_bonds = out_bonds
+        dO = _desc(self.out_layout, None, self.out_layout.itoi, self.out_layout.shapes, keep)
+        m1h = self.M1._data.detach().cpu().numpy().astype(np.float64)
+        m2h = self.M2._data.detach().cpu().numpy().astype(np.float64)
+        keep += [m1h, m2h]
+        desc = Heff2Desc(ctypes.pointer(dP), ctypes.pointer(dL), ctypes.pointer(dR), ctypes.pointer(dM1),
+                         ctypes.pointer(dM2), ctypes.pointer(dO), m1h.ctypes.data, m2h.ctypes.data)
+        h = ctypes.c_void_p()
+        _lib.check(_lib.lib().ctn_heff2_plan_create(ctypes.byref(desc), ctypes.byref(h)), "TwoSiteHeff")
+        self._h = h.value
+        self._keep = keep
+        self.n = int(_lib.lib().ctn_heff2_psi_elems(self._h))
+        self.plan_flops = float(_lib.lib().ctn_heff2_flops(self._h))
+        self._ws = {}
+        self._bound = None
+        self.precision = precision
+        self._algo_flops = None
+
+    def __del__(self):
+        try:
+            _lib.lib().ctn_heff2_plan_destroy(self._h)
+        except Exception:
+            pass
+
+    # ---------------------------------------------------------------- binding
+    def bind(self, precision: Optional[str] = None) -> None:
+        prec = _lib.PRECISIONS[(precision or self.precision).lower()]
+        if self._bound == prec:
+            return
+        nbytes = int(_lib.lib().ctn_heff2_workspace_bytes(self._h, prec))
+        ws = self._ws.get(prec)
+        if ws is None:
+            ws = torch.empty(nbytes, dtype=torch.uint8, device=self.L._data.device)
+            self._ws[prec] = ws
+        _lib.check(_lib.lib().ctn_heff2_set_env(self._h, self.L._data.data_ptr(), self.R._data.data_ptr(),
+                                                ws.data_ptr(), prec, _lib.stream_ptr()), "TwoSiteHeff.set_env")
+        self._bound = prec
+
+    # ---------------------------------------------------------------- matvec
+    def apply_flat(self, x: torch.Tensor, y: torch.Tensor, precision: Optional[str] = None) -> None:
+        prec = _lib.PRECISIONS[(precision or self.precision).lower()]
+        self.bind(precision)
+        _lib.check(_lib.lib().ctn_heff2_matvec(self._h, x.data_ptr(), y.data_ptr(), prec, _lib.stream_ptr()),
+                   "TwoSiteHeff.matvec")
+
+    def matvec(self, v: UniTensor) -> UniTensor:
+        lbl = v.labels()
+        x = v.contiguous().flat_view()
+        if x.numel() != self.n:
+            raise CytnxError("[TwoSiteHeff] psi has the wrong size")
+        y = torch.empty_like(x)
+        self.apply_flat(x, y)
+        out = UniTensor._new_block(self.out_bonds, lbl, v.rowrank(), self.out_layout, [0, 1, 2, 3], y)
+        return out
+
+    # ---------------------------------------------------------------- Lanczos without Python callbacks
+    def lanczos(self, psi0: UniTensor, maxiter: int = 40, cvgcrit: float = 1e-14,
+                precision: Optional[str] = None) -> Tuple[float, UniTensor, int]:
+        prec = _lib.PRECISIONS[(precision or self.precision).lower()]
+        self.bind(precision)
+        x0 = psi0.contiguous().flat_view()
+        n = self.n
+        krylov = torch.empty((maxiter + 1) * n, dtype=torch.float64, device=x0.device)
+        work = torch.empty(n + 8 + 1032 + maxiter + 64, dtype=torch.float64, device=x0.device)
+        eig = torch.empty(n, dtype=torch.float64, device=x0.device)
+        e = ctypes.c_double()
+        it = ctypes.c_int()
+        _lib.check(_lib.lib().ctn_heff2_lanczos_gnd(self._h, prec, x0.data_ptr(), maxiter, float(cvgcrit),
+                                                    krylov.data_ptr(), work.data_ptr(), eig.data_ptr(),
+                                                    ctypes.byref(e), ctypes.byref(it), _lib.stream_ptr()),
+                   "TwoSiteHeff.lanczos")
+        vec = UniTensor._new_block(self.out_bonds, psi0.labels(), psi0.rowrank(), self.out_layout, [0, 1, 2, 3], eig)
+        return e.value, vec, it.value
+
+    # ---------------------------------------------------------------- accounting
+    def algorithmic_flops(self) -> float:
+        """Flops of the reference's block-pair GEMMs for one matvec in the order
+        L -> M1 -> M2 -> R (2*m*n*k over every block pair each BlockUniTensor::contract
+        step multiplies), counted on the host from the block structure."""
+        if self._algo_flops is None:
+            P = structure_only(self.psi_t.bonds(), ["a", "s1", "s2", "b"])
+            Ls = structure_only(self.L.bonds(), ["w", "a", "ap"])
+            M1s = structure_only(self.M1.bonds(), ["w", "w1", "s1", "s1p"])
+            M2s = structure_only(self.M2.bonds(), ["w1", "w2", "s2", "s2p"])
+            Rs = structure_only(self.R.bonds(), ["w2", "b", "bp"])
+            f = 0.0
+            f += contract_plan_flops(Ls, P)
+            T1 = _struct_contract(Ls, P)
+            f += contract_plan_flops(T1, M1s)
+            T2 = _struct_contract(T1, M1s)
+            f += contract_plan_flops(T2, M2s)
+            T3 = _struct_contract(T2, M2s)
+            f += contract_plan_flops(T3, Rs)
+            self._algo_flops = f
+        return self._algo_flops
+
+
+def _struct_contract(A: UniTensor, B: UniTensor) -> UniTensor:
+    comm = set(A.labels()) & set(B.labels())
+    bonds = [b for b, l in zip(A.bonds(), A.labels()) if l not in comm] + \
+        [b for b, l in zip(B.bonds(), B.labels()) if l not in comm]
+    labels = [l for l in A.labels() if l not in comm] + [l for l in B.labels() if l not in comm]
+    return structure_only(bonds, labels)

@@ -1,0 +1,75 @@
+"""Convert the reference's binary test fixtures for the hot path into small .npz files.
+
+Run in a container where the reference checkout exists (default
+/root/reference); the GPU-side tests only read the .npz files written here.
+
+Fixtures converted (the reference tests that use them):
+
+* BlockUniTensor contract_{L,R,ans}{1,2,3}  -- tests/BlockUniTensor_test.cpp:679-717
+* BlockUniTensor permute_T{1,2,3} / permute_ans{1,2,3} -- tests/BlockUniTensor_test.cpp:308-360
+* DenseUniTensor denseutensor{1,2}, densecontres{1,2,3}, densepermu{1,2}
+                                               -- tests/DenseUniTensor_test.cpp:2594-2619
+* linalg/Lanczos_Gnd lan_block_{A,B,C}         -- tests/linalg_test/Lanczos_Gnd_test.cpp:102-125,392-445
+
+Usage:  python tests/golden/make_golden.py [reference_root]
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from cytnx_b200 import fileio  # noqa: E402
+
+
+def pack_unitensor(u):
+    out = {
+        "uten_type": np.int64(u["uten_type"]),
+        "rowrank": np.int64(u["rowrank"]),
+        "is_diag": np.bool_(u["is_diag"]),
+        "labels": np.array(u["labels"], dtype="U"),
+        "rank": np.int64(len(u["labels"])),
+    }
+    for i, b in enumerate(u["bonds"]):
+        out[f"bond{i}_type"] = np.int64(b["type"])
+        out[f"bond{i}_qnums"] = np.asarray(b["qnums"], dtype=np.int64)
+        out[f"bond{i}_degs"] = np.asarray(b["degs"], dtype=np.int64)
+        out[f"bond{i}_syms"] = np.array([[s["stype"], s["n"]] for s in b["syms"]], dtype=np.int64).reshape(-1, 2)
+        out[f"bond{i}_dim"] = np.int64(b["dim"])
+    if u["uten_type"] == fileio.UTEN_BLOCK:
+        blocks = u["blocks"]
+        out["itoi"] = np.asarray(u["itoi"], dtype=np.int64)
+        out["block_shapes"] = np.array([b.shape for b in blocks], dtype=np.int64).reshape(len(blocks), -1)
+        out["data"] = np.concatenate([b.ravel() for b in blocks]) if blocks else np.zeros(0)
+    else:
+        out["block"] = u["block"]
+    return out
+
+
+def main(ref_root: str) -> None:
+    base = os.path.join(ref_root, "tests", "test_data_base")
+    jobs = []
+    bdir = os.path.join(base, "common", "BlockUniTensor")
+    for stem in ["contract_L1", "contract_R1", "contract_ans1", "contract_L2", "contract_R2",
+                 "contract_ans2", "contract_L3", "contract_R3", "contract_ans3",
+                 "permute_T1", "permute_ans1", "permute_T2", "permute_ans2",
+                 "permute_T3", "permute_ans3"]:
+        jobs.append((os.path.join(bdir, stem + ".cytnx"), "block_" + stem))
+    ddir = os.path.join(base, "common", "DenseUniTensor")
+    for stem in ["denseutensor1", "denseutensor2", "densecontres1", "densecontres2",
+                 "densecontres3", "densepermu1", "densepermu2"]:
+        jobs.append((os.path.join(ddir, stem + ".cytnx"), "dense_" + stem))
+    for src, dst in jobs:
+        u = fileio.read_unitensor(src)
+        np.savez_compressed(os.path.join(HERE, dst + ".npz"), **pack_unitensor(u))
+        print("wrote", dst)
+    ldir = os.path.join(base, "linalg", "Lanczos_Gnd")
+    lan = {k: fileio.read_tensor(os.path.join(ldir, f"lan_block_{k}.cytn")) for k in "ABC"}
+    np.savez_compressed(os.path.join(HERE, "lanczos_blocks.npz"), **lan)
+    print("wrote lanczos_blocks")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

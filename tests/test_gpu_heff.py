@@ -1,0 +1,169 @@
+"""Two-site H_eff matvec and Lanczos: the planned CUDA path against the oracle."""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+NET = {"psi": ["-1", "-2", "-3", "-4"], "L": ["-5", "-1", "0"], "R": ["-7", "-4", "3"],
+       "M1": ["-5", "-6", "-2", "1"], "M2": ["-6", "-7", "-3", "2"]}
+
+
+def to_oracle(u, labels):
+    bonds = [O.Bond(b.type(), b._qnums, b._degs) for b in u.bonds()]
+    u = u.contiguous()
+    blocks = [u.get_block_(i).numpy() for i in range(u.Nblocks())]
+    return O.BlockTensor(bonds, labels, u.rowrank(), u._layout.itoi, blocks)
+
+
+def oracle_heff(ops, order=("L", "M1", "M2", "R")):
+    """Pairwise oracle contractions in the given order starting from psi; result in TOUT order."""
+    t = ops["psi"]
+    for name in order:
+        t = ops[name].contract(t) if name == "L" else t.contract(ops[name])
+    perm = [t.labels.index(l) for l in ["0", "1", "2", "3"]]
+    return t.permute(perm)
+
+
+def build(D, seed=0):
+    from cytnx_b200 import workloads as W
+
+    spec = W.xxz_spec(D)
+    return W.build_two_site(spec, W.xxz_mpo_values(1.0, 1.0), seed=seed, device=0)
+
+
+@pytest.mark.parametrize("D", [16, 64, 256])
+def test_heff_matvec_matches_oracle(D):
+    import cytnx_b200 as c
+
+    psi, L, M1, M2, R = build(D)
+    H = c.TwoSiteHeff(L, M1, M2, R, psi)
+    out = H.matvec(psi)
+    ops = {"psi": to_oracle(psi, NET["psi"]), "L": to_oracle(L, NET["L"]), "R": to_oracle(R, NET["R"]),
+           "M1": to_oracle(M1, NET["M1"]), "M2": to_oracle(M2, NET["M2"])}
+    ref = oracle_heff(ops)
+    ref_flat = np.concatenate([b.ravel() for b in ref.blocks])
+    assert np.array_equal(ref.itoi, out._layout.itoi)
+    got = out.flat_view().cpu().numpy()
+    err = np.linalg.norm(got - ref_flat) / np.linalg.norm(ref_flat)
+    assert err < 1e-13, err
+
+
+def test_network_launch_matches_planned_heff():
+    """The drop-in path (Network.Launch, default left-fold order) equals the fused plan."""
+    import cytnx_b200 as c
+    from cytnx_b200 import workloads as W
+
+    psi, L, M1, M2, R = build(64, seed=3)
+    net = c.Network()
+    net.FromString(W.heff_network_lines())
+    net.PutUniTensors(["L", "M1", "M2", "R"], [L, M1, M2, R])
+    net.PutUniTensor("psi", psi)
+    out_net = net.Launch().contiguous()
+    H = c.TwoSiteHeff(L, M1, M2, R, psi)
+    out = H.matvec(psi)
+    a, b = out_net.flat_view(), out.flat_view()
+    assert torch.linalg.vector_norm(a - b).item() / torch.linalg.vector_norm(b).item() < 1e-13
+    net.setOrder(True, "")
+    net._order = None
+    out_opt = net.Launch().contiguous()
+    assert torch.linalg.vector_norm(out_opt.flat_view() - b).item() / torch.linalg.vector_norm(b).item() < 1e-13
+
+
+@pytest.mark.parametrize("D", [1024])
+def test_heff_hermitian_and_linear(D):
+    """Size-independent properties at the benchmark size: <x|Hy> = <Hx|y>, H(ax+y) = aHx + Hy."""
+    import cytnx_b200 as c
+
+    psi, L, M1, M2, R = build(D, seed=1)
+    H = c.TwoSiteHeff(L, M1, M2, R, psi)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    x = torch.randn(H.n, dtype=torch.float64, device="cuda", generator=g)
+    y = torch.randn(H.n, dtype=torch.float64, device="cuda", generator=g)
+    hx, hy, hz = torch.empty_like(x), torch.empty_like(x), torch.empty_like(x)
+    H.apply_flat(x, hx)
+    H.apply_flat(y, hy)
+    H.apply_flat(0.3 * x + y, hz)
+    lhs, rhs = torch.dot(x, hy).item(), torch.dot(hx, y).item()
+    assert abs(lhs - rhs) <= 1e-11 * (abs(lhs) + torch.linalg.vector_norm(hx).item() * torch.linalg.vector_norm(y).item())
+    lin = torch.linalg.vector_norm(hz - (0.3 * hx + hy)).item() / torch.linalg.vector_norm(hz).item()
+    assert lin < 1e-13
+
+
+def test_lanczos_heff_matches_oracle():
+    import cytnx_b200 as c
+
+    psi, L, M1, M2, R = build(32, seed=2)
+    H = c.TwoSiteHeff(L, M1, M2, R, psi)
+    E, vec, it = H.lanczos(psi, maxiter=30, cvgcrit=1e-300)
+    ops = {"psi": to_oracle(psi, NET["psi"]), "L": to_oracle(L, NET["L"]), "R": to_oracle(R, NET["R"]),
+           "M1": to_oracle(M1, NET["M1"]), "M2": to_oracle(M2, NET["M2"])}
+    lay_blocks = [b.shape for b in ops["psi"].blocks]
+
+    def mv(x):
+        pos, blocks = 0, []
+        for s in lay_blocks:
+            n = int(np.prod(s))
+            blocks.append(x[pos:pos + n].reshape(s))
+            pos += n
+        p = O.BlockTensor(ops["psi"].bonds, NET["psi"], 1, ops["psi"].itoi, blocks)
+        return np.concatenate([b.ravel() for b in oracle_heff(dict(ops, psi=p)).blocks])
+
+    x0 = psi.flat_view().cpu().numpy()
+    E_ref, v_ref, it_ref = O.lanczos_gnd_ut(mv, x0, 1e-300, 30)
+    assert it == it_ref == 30
+    assert abs(E - E_ref) < 1e-10 * abs(E_ref)
+    v = vec.flat_view().cpu().numpy()
+    assert min(np.linalg.norm(v - v_ref), np.linalg.norm(v + v_ref)) < 1e-6 * np.linalg.norm(v_ref)
+    # the LinOp / callback route gives the same numbers
+    E2, vec2 = c.linalg.Lanczos(Hop=H, Tin=psi, method="Gnd", Maxiter=30, CvgCrit=1e-300)
+    assert abs(E2.item() - E) < 1e-12 * abs(E)
+
+
+def test_lanczos_block_golden():
+    """tests/linalg_test/Lanczos_Gnd_test.cpp:392-422: E vs Eigh to 1e-12, residual < 1e-6."""
+    import cytnx_b200 as c
+    from conftest import load_golden
+
+    z = load_golden("lanczos_blocks")
+    I = c.Bond(c.BD_IN, [[-1], [0], [1]], [9, 9, 9])
+    J = c.Bond(c.BD_OUT, [[-1], [0], [1]], [9, 9, 9])
+    Hm = c.UniTensor([I, J], labels=["a", "b"], device=0)
+    for i, k in enumerate("ABC"):
+        Hm.put_block(c.Tensor.from_numpy(z[k], 0), i)
+    Jv = c.Bond(c.BD_OUT, [[-1], [0], [1]], [1, 1, 1])
+    guess = c.UniTensor([I, Jv], labels=["b", "c"], device=0)
+    rng = np.random.default_rng(1)
+    for i in range(3):
+        guess.put_block(c.Tensor.from_numpy(rng.standard_normal((9, 1)), 0), i)
+
+    class Op(c.LinOp):
+        def matvec(self, v):
+            out = c.Contract(Hm, v)
+            return out.relabel(["b", "c"])
+
+    E, v = c.linalg.Lanczos(Op("mv", 27), guess, "Gnd", 1e-15, 10000)
+    dense = np.zeros((27, 27))
+    for i, k in enumerate("ABC"):
+        dense[9 * i:9 * i + 9, 9 * i:9 * i + 9] = z[k]
+    E0 = np.linalg.eigvalsh(dense).min()
+    assert abs(E.item() - E0) < 1e-12
+    r = (Op("mv", 27).matvec(v) - E.item() * v).norm()
+    assert r < 1e-6
+
+
+def test_lanczos_dense_arange_golden():
+    """tests/linalg_test/Lanczos_Gnd_test.cpp:377-390 (E = -1628.9964650426593, tol 1e-5)."""
+    import cytnx_b200 as c
+
+    A = torch.arange(27 * 27, dtype=torch.float64, device="cuda").reshape(27, 27)
+    Hd = A + A.T
+
+    class Op(c.LinOp):
+        def matvec(self, v):
+            return c.Tensor.from_torch(Hd @ v.to_torch())
+
+    E, v = c.linalg.Lanczos(Op("mv", 27), c.arange(27, device=0), "Gnd", 9.999999999999999988e-15, 10000)
+    assert abs(E.item() - (-1628.9964650426593)) < 1e-5
