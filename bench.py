@@ -44,7 +44,7 @@ def parse():
     ap.add_argument("--D", type=int, default=4096)
     ap.add_argument("--lanczos-iters", type=int, default=40)
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
-    ap.add_argument("--precision", default="fp64")
+    ap.add_argument("--precision", default="3xtf32", help="headline arithmetic form: 3xtf32, bf16x3 or fp64")
     return ap.parse_args()
 
 
@@ -193,53 +193,70 @@ def main():
         print(json.dumps(line), flush=True)
         return
 
+    import ctypes
+
     import cytnx_b200 as c
     from cytnx_b200 import _lib
 
     dev = torch.device(f"cuda:{local}")
+    st = torch.cuda.current_stream()
     psi, L, M1, M2, R = W.build_two_site(spec, mpo_vals, seed=0, device=local)
     H = c.TwoSiteHeff(L, M1, M2, R, psi, precision=args.precision)
-    H.bind()
     flops = H.algorithmic_flops()
     x = psi.flat_view()
-    y = torch.empty_like(x)
-    for _ in range(args.warmup):
-        H.apply_flat(x, y)
-    torch.cuda.synchronize()
+    forms = [args.precision] + (["fp64"] if args.precision != "fp64" else [])
 
-    # ---- device-resident timed region
-    sampler = ClockSampler(local)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    st = torch.cuda.current_stream()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with sampler:
+    def timed_matvecs(form, steps, sampler=None):
+        y = torch.empty_like(x)
+        H.bind(form)
+        for _ in range(args.warmup):
+            H.apply_flat(x, y, form)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if sampler is not None:
+            sampler.__enter__()
         e0.record(st)
-        for _ in range(args.steps):
-            H.apply_flat(x, y)
+        for _ in range(steps):
+            H.apply_flat(x, y, form)
         e1.record(st)
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        dist.barrier()
-    t_max = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-    ms_max = float(t_max.item())
-    ms_step = ms_max / args.steps
-    value = world * flops * args.steps / (ms_max * 1e-3) / 1e12
+        if sampler is not None:
+            sampler.__exit__(None, None, None)
+        t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()), y
 
-    # ---- per-kernel timing (CUDA events between the phases, same stream)
-    ms3 = (ctypes_double3 := (__import__("ctypes").c_double * 3)())
-    nl = __import__("ctypes").c_int()
-    _lib.check(_lib.lib().ctn_heff2_profile(H._h, x.data_ptr(), y.data_ptr(), 0, 10, ms3, __import__("ctypes").byref(nl),
-                                           _lib.stream_ptr()), "profile")
-    g1f = _lib.lib().ctn_heff2_gemm_flops(H._h, 1)
-    g4f = _lib.lib().ctn_heff2_gemm_flops(H._h, 4)
-    gemm_ms = ms3[0] + ms3[2]
+    def phases(form):
+        ms = (ctypes.c_double * 4)()
+        nl = ctypes.c_int()
+        y = torch.empty_like(x)
+        _lib.check(_lib.lib().ctn_heff2_profile(H._h, x.data_ptr(), y.data_ptr(), _lib.PRECISIONS[form], 10, ms,
+                                               ctypes.byref(nl), _lib.stream_ptr()), "profile")
+        return [ms[i] for i in range(4)], int(nl.value)
 
-    # ---- end to end through the public API (pinned host psi in, host H psi out)
+    results = {}
+    sampler = ClockSampler(local)
+    for i, form in enumerate(forms):
+        ms, y = timed_matvecs(form, args.steps, sampler if i == 0 else None)
+        ph, nl = phases(form)
+        results[form] = {"ms_total": ms, "ms_per_matvec": ms / args.steps,
+                         "tflops": world * flops * args.steps / (ms * 1e-3) / 1e12, "phase_ms": ph,
+                         "launches_per_matvec": nl, "y": y}
+    head = results[args.precision]
+    value = head["tflops"]
+
+    # matvec error of the split form against the FP64 form (same input)
+    mv_err = None
+    if args.precision != "fp64":
+        y64 = results["fp64"]["y"]
+        mv_err = float((torch.linalg.vector_norm(head["y"] - y64) / torch.linalg.vector_norm(y64)).item())
+
+    # ---- end to end through the public API (pinned host psi in, host H psi out), headline form
+    H.bind(args.precision)
     h_in = torch.empty(x.numel(), dtype=torch.float64, pin_memory=True)
     h_in.copy_(x.cpu())
     h_out = torch.empty_like(h_in, pin_memory=True)
@@ -263,29 +280,66 @@ def main():
         dist.all_reduce(t2, op=dist.ReduceOp.MAX)
     e2e_val = world * flops * args.steps / (float(t2.item()) * 1e-3) / 1e12
 
-    # ---- Lanczos step time (C++ driver, FP64 recurrence, host tridiagonal solve)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    E, vec, it = H.lanczos(psi, maxiter=args.lanczos_iters, cvgcrit=1e-300)
-    torch.cuda.synchronize()
-    lz = (time.perf_counter() - t0) / max(it, 1)
-
-    # ---- DGEMM peak for the roofline denominator (cuBLAS 8192^3, best of 5)
-    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
-    b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
-    torch.matmul(a, b)
-    best = 1e9
-    for _ in range(5):
-        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s0.record(st)
-        torch.matmul(a, b)
-        s1.record(st)
+    # ---- Lanczos: FP64 and split forms from the same start vector; FP64 Rayleigh-quotient refinement
+    lanczos = {}
+    vecs = {}
+    for form in forms:
         torch.cuda.synchronize()
-        best = min(best, s0.elapsed_time(s1))
-    dgemm_tflops = 2 * 8192 ** 3 / (best * 1e-3) / 1e12
-    del a, b
+        t0 = time.perf_counter()
+        E, vec, it = H.lanczos(psi, maxiter=args.lanczos_iters, cvgcrit=1e-300, precision=form)
+        torch.cuda.synchronize()
+        lanczos[form] = {"energy": E, "iters": it, "s_per_step": (time.perf_counter() - t0) / max(it, 1)}
+        vecs[form] = vec.flat_view()
+    if args.precision != "fp64":
+        v = vecs[args.precision]
+        hv = torch.empty_like(v)
+        H.apply_flat(v, hv, "fp64")
+        e_ref = float((torch.dot(v, hv) / torch.dot(v, v)).item())
+        e64 = lanczos["fp64"]["energy"]
+        lanczos["refined_energy"] = e_ref
+        lanczos["dE_rel_raw"] = abs(lanczos[args.precision]["energy"] - e64) / abs(e64)
+        lanczos["dE_rel_refined"] = abs(e_ref - e64) / abs(e64)
 
-    gemm_achieved = (g1f + g4f) / (gemm_ms * 1e-3) / 1e12
+    # ---- peaks for the roofline denominators (cuBLAS, best of 5)
+    def gemm_peak(dtype, tf32=False):
+        old = torch.backends.cuda.matmul.allow_tf32
+        torch.backends.cuda.matmul.allow_tf32 = tf32
+        a = torch.randn(8192, 8192, dtype=dtype, device=dev)
+        b = torch.randn(8192, 8192, dtype=dtype, device=dev)
+        torch.matmul(a, b)
+        best = 1e9
+        for _ in range(5):
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record(st)
+            torch.matmul(a, b)
+            s1.record(st)
+            torch.cuda.synchronize()
+            best = min(best, s0.elapsed_time(s1))
+        torch.backends.cuda.matmul.allow_tf32 = old
+        del a, b
+        return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+
+    dgemm_tflops = gemm_peak(torch.float64)
+    tf32_tflops = gemm_peak(torch.float32, tf32=True)
+    pk, src = peaks()
+    prec_id = _lib.PRECISIONS[args.precision]
+    if args.precision == "fp64":
+        g_flops = _lib.lib().ctn_heff2_gemm_flops(H._h, 1) + _lib.lib().ctn_heff2_gemm_flops(H._h, 4)
+        g_ms = head["phase_ms"][1] + head["phase_ms"][3]
+        roof = {"bound": "fp64", "achieved": g_flops / (g_ms * 1e-3) / 1e12, "peak": dgemm_tflops,
+                "kernel": "k_gemm_grouped_f64 (steps 1 and 4)",
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run"}
+    else:
+        g_flops = _lib.lib().ctn_heff2_split_gemm_flops(H._h, prec_id, 1) + \
+            _lib.lib().ctn_heff2_split_gemm_flops(H._h, prec_id, 4)
+        g_ms = head["phase_ms"][1] + head["phase_ms"][3]
+        tc_peak = tf32_tflops if args.precision == "3xtf32" else float(pk.get("bf16_tflops", 1590.0))
+        roof = {"bound": "tensor", "achieved": g_flops / (g_ms * 1e-3) / 1e12, "peak": tc_peak / 3.0,
+                "kernel": "k_tc_gemm (tcgen05, steps 1 and 4, stacked per sector)",
+                "peak_source": ("cuBLAS TF32 GEMM 8192^3 measured in this run" if args.precision == "3xtf32"
+                                else f"MEASURED_PEAKS.json bf16_tflops ({src})") + " / 3 split products"}
+    roof.update({"unit": "TFLOP/s", "frac": roof["achieved"] / roof["peak"], "traffic": None,
+                 "kernel_flops_per_matvec": g_flops, "kernel_ms_per_matvec": g_ms})
     clocks = sampler.summary()
     if rank == 0:
         cpu = None
@@ -295,25 +349,25 @@ def main():
             cpu = {"value": flops / sec / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": "port",
                    "sample": f"{n} H_eff matvecs at D={args.D} on the host (oracle restatement of "
                              f"BlockUniTensor::contract, OpenBLAS dgemm), {sec:.3f} s each"}
-        pk, src = peaks()
+        forms_out = {f: {k: v for k, v in r.items() if k != "y"} for f, r in results.items()}
         line = {
             "metric": "U(1) H_eff matvec TFLOP/s & Lanczos s/step, split-prec vs FP64, dE<=1e-9",
             "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else args.precision, "data": "synthetic (seeded numpy PCG64)",
+            "ms_per_step": head["ms_per_matvec"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": args.precision, "data": "synthetic (seeded numpy PCG64)",
             "config": dict(config_base, parallelism=f"replicas{world}", precision=args.precision),
             "algorithmic_flops_per_matvec": flops,
-            "lanczos_s_per_step": lz, "lanczos_iters": it, "lanczos_energy": E,
+            "forms": forms_out,
+            "speedup_vs_fp64": (results["fp64"]["ms_per_matvec"] / head["ms_per_matvec"]) if "fp64" in results else 1.0,
+            "matvec_rel_err_vs_fp64": mv_err,
+            "lanczos": lanczos,
+            "lanczos_s_per_step": lanczos[args.precision]["s_per_step"],
             "e2e": {"value": e2e_val, "unit": "TFLOP/s", "h2d_bytes_per_step": int(x.numel() * 8),
                     "d2h_bytes_per_step": int(x.numel() * 8)},
-            "gpu_launches": int(nl.value) * args.steps,
-            "phase_ms": {"gemm_step1": ms3[0], "mpo_steps2_3": ms3[1], "gemm_step4": ms3[2]},
-            "roofline": {"bound": "fp64", "achieved": gemm_achieved, "peak": dgemm_tflops, "unit": "TFLOP/s",
-                         "frac": gemm_achieved / dgemm_tflops, "traffic": None,
-                         "kernel": "k_gemm_grouped_f64 (steps 1 and 4)",
-                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)"},
+            "gpu_launches": head["launches_per_matvec"] * args.steps,
+            "roofline": roof,
             "peaks": {"hbm_gbs": pk.get("hbm_gbs"), "bf16_tflops": pk.get("bf16_tflops"), "source": src,
-                      "dgemm_tflops_measured": dgemm_tflops},
+                      "dgemm_tflops_measured": dgemm_tflops, "tf32_tflops_measured": tf32_tflops},
             "clocks": clocks,
             "cpu_baseline": cpu,
         }

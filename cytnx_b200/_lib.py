@@ -73,6 +73,8 @@ _SIGS = {
     "ctn_gemm_grouped_plan_flops": (c_dbl, [c_vp]),
     "ctn_gemm_grouped_f64": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp]),
     "ctn_gemm_grouped_plan_destroy": (None, [c_vp]),
+    "ctn_split_gemm_workspace_bytes": (c_size, [c_i64, c_i64, c_i64, c_int]),
+    "ctn_split_gemm_f64": (c_int, [c_i64, c_i64, c_i64, c_vp, c_vp, c_vp, c_int, c_vp, c_vp]),
     "ctn_dot_f64": (c_int, [c_vp, c_vp, c_i64, c_vp, c_vp]),
     "ctn_nrm2_f64": (c_int, [c_vp, c_i64, c_vp, c_vp]),
     "ctn_axpy_f64": (c_int, [c_vp, c_vp, c_i64, c_vp, c_dbl, c_vp]),
@@ -87,6 +89,7 @@ _SIGS = {
     "ctn_heff2_plan_destroy": (None, [c_vp]),
     "ctn_heff2_profile": (c_int, [c_vp, c_vp, c_vp, c_int, c_int, P_dbl, ctypes.POINTER(c_int), c_vp]),
     "ctn_heff2_gemm_flops": (c_dbl, [c_vp, c_int]),
+    "ctn_heff2_split_gemm_flops": (c_dbl, [c_vp, c_int, c_int]),
     "ctn_lanczos_gnd": (c_int, [MATVEC_FN, c_vp, c_vp, c_i64, c_int, c_dbl, c_vp, c_vp, c_vp, P_dbl,
                                 ctypes.POINTER(c_int), c_vp]),
     "ctn_heff2_lanczos_gnd": (c_int, [c_vp, c_int, c_vp, c_int, c_dbl, c_vp, c_vp, c_vp, P_dbl,

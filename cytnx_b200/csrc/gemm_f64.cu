@@ -1,4 +1,4 @@
-// Grouped FP64 GEMM on the B200 FP64 tensor pipe (DMMA, mma.sync m16n8k4 .f64).
+// Grouped FP64 GEMM on the B200 FP64 tensor pipe (DMMA, mma.sync m16n8k16 .f64).
 //
 // One launch computes every output block of a block-sparse contraction:
 //   C_t = sum_{p in pairs(t)} op(A_p) * op(B_p)     (row-major C_t, m_t x n_t)
@@ -37,66 +37,72 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-__device__ __forceinline__ void dmma_16x8x4(double (&c)[4], double a0, double a1, double b0) {
+// D(16x8) += A(16x16) B(16x8), FP64, one warp.  Fragments (groupID g = lane/4,
+// t = lane%4): a[i] = A[g + 8*(i&1)][t + 4*(i>>1)], b[i] = B[t + 4*i][g],
+// c[0..1] = C[g][2t..2t+1], c[2..3] = C[g+8][2t..2t+1].
+__device__ __forceinline__ void dmma_16x8x16(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
   asm volatile(
-      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
-      "{%0,%1,%2,%3};\n"
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
       : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
-      : "d"(a0), "d"(a1), "d"(b0));
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+        "d"(b[1]), "d"(b[2]), "d"(b[3]));
 }
 
-struct Smem {
-  double A[2][BK][BM + PAD];
-  double B[2][BK][BN + PAD];
+// Shared-memory tiles keep the operand's contiguous global axis contiguous, so the
+// cp.async writes are conflict-free; the +4 double padding makes every fragment read
+// pattern below conflict-free as well (bank = 8*x + 2*y for the 4x4 lanes of a phase).
+template <bool TA, bool TB>
+struct SmemT {
+  double A[2][TA ? BK : BM][(TA ? BM : BK) + PAD];
+  double B[2][TB ? BN : BK][(TB ? BK : BN) + PAD];
 };
 
-// load the (m0..m0+BM) x (k0..k0+BK) tile of op(A) and the (k0..)x(n0..) tile of op(B)
-__device__ __forceinline__ void load_stage(Smem &sm, int buf, const double *__restrict__ A,
-                                           const double *__restrict__ B, const GemmPairD &p, int m,
-                                           int n, int m0, int n0, int k0) {
+template <bool TA, bool TB>
+__device__ __forceinline__ void load_stage(SmemT<TA, TB> &sm, int buf, const double *__restrict__ A,
+                                           const double *__restrict__ B, const GemmPairD &p, int m, int n,
+                                           int m0, int n0, int k0) {
   const int tid = threadIdx.x;
-  const bool ta = p.flags & 1, tb = p.flags & 2;
   const double *Ap = A + p.a_off;
   const double *Bp = B + p.b_off;
 #pragma unroll
   for (int i = 0; i < (BM * BK) / NTHREADS; ++i) {
-    int idx = tid + i * NTHREADS;
-    int mm, kk;
-    if (!ta) {  // A[m][k], contiguous along k
-      mm = idx / BK;
-      kk = idx % BK;
-    } else {  // A stored [k][m], contiguous along m
-      kk = idx / BM;
-      mm = idx % BM;
+    const int idx = tid + i * NTHREADS;
+    if (!TA) {  // A[m][k]: k contiguous
+      const int mm = idx / BK, kk = idx % BK;
+      const int gm = m0 + mm, gk = k0 + kk;
+      const bool ok = gm < m && gk < p.k;
+      cp_async8(&sm.A[buf][mm][kk], ok ? Ap + (int64_t)gm * p.lda + gk : Ap, ok);
+    } else {  // A stored [k][m]: m contiguous
+      const int kk = idx / BM, mm = idx % BM;
+      const int gm = m0 + mm, gk = k0 + kk;
+      const bool ok = gm < m && gk < p.k;
+      cp_async8(&sm.A[buf][kk][mm], ok ? Ap + (int64_t)gk * p.lda + gm : Ap, ok);
     }
-    const int gm = m0 + mm, gk = k0 + kk;
-    const bool ok = gm < m && gk < p.k;
-    const double *src = ok ? (ta ? Ap + (int64_t)gk * p.lda + gm : Ap + (int64_t)gm * p.lda + gk) : Ap;
-    cp_async8(&sm.A[buf][kk][mm], src, ok);
   }
 #pragma unroll
   for (int i = 0; i < (BN * BK) / NTHREADS; ++i) {
-    int idx = tid + i * NTHREADS;
-    int nn, kk;
-    if (!tb) {  // B[k][n], contiguous along n
-      kk = idx / BN;
-      nn = idx % BN;
-    } else {  // B stored [n][k], contiguous along k
-      nn = idx / BK;
-      kk = idx % BK;
+    const int idx = tid + i * NTHREADS;
+    if (!TB) {  // B[k][n]: n contiguous
+      const int kk = idx / BN, nn = idx % BN;
+      const int gn = n0 + nn, gk = k0 + kk;
+      const bool ok = gn < n && gk < p.k;
+      cp_async8(&sm.B[buf][kk][nn], ok ? Bp + (int64_t)gk * p.ldb + gn : Bp, ok);
+    } else {  // B stored [n][k]: k contiguous
+      const int nn = idx / BK, kk = idx % BK;
+      const int gn = n0 + nn, gk = k0 + kk;
+      const bool ok = gn < n && gk < p.k;
+      cp_async8(&sm.B[buf][nn][kk], ok ? Bp + (int64_t)gn * p.ldb + gk : Bp, ok);
     }
-    const int gn = n0 + nn, gk = k0 + kk;
-    const bool ok = gn < n && gk < p.k;
-    const double *src = ok ? (tb ? Bp + (int64_t)gn * p.ldb + gk : Bp + (int64_t)gk * p.ldb + gn) : Bp;
-    cp_async8(&sm.B[buf][kk][nn], src, ok);
   }
 }
 
+template <bool TA, bool TB>
 __global__ void __launch_bounds__(NTHREADS) k_gemm_grouped_f64(
     const double *__restrict__ A, const double *__restrict__ B, double *__restrict__ C,
     const GemmTaskD *__restrict__ tasks, const GemmPairD *__restrict__ pairs,
     const GemmTileD *__restrict__ tiles, int64_t ntiles) {
-  __shared__ __align__(16) Smem sm;
+  __shared__ __align__(16) SmemT<TA, TB> sm;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
   const int g = lane >> 2, t4 = lane & 3;
@@ -114,19 +120,17 @@ __global__ void __launch_bounds__(NTHREADS) k_gemm_grouped_f64(
 
     // flattened (pair, k-tile) iteration with a 2-deep cp.async pipeline
     int pi = 0, kt = 0;
-    int npairs = task.pair_count;
-    // skip pairs with k == 0
+    const int npairs = task.pair_count;
     while (pi < npairs && pairs[task.pair_begin + pi].k <= 0) ++pi;
     int buf = 0;
     bool have = pi < npairs;
     GemmPairD cur;
     if (have) {
       cur = pairs[task.pair_begin + pi];
-      load_stage(sm, 0, A, B, cur, task.m, task.n, m0, n0, 0);
+      load_stage<TA, TB>(sm, 0, A, B, cur, task.m, task.n, m0, n0, 0);
     }
     cp_async_commit();
     while (have) {
-      // next stage coordinates
       int npi = pi, nkt = kt + 1;
       GemmPairD nxt = cur;
       if (nkt * BK >= cur.k) {
@@ -136,25 +140,29 @@ __global__ void __launch_bounds__(NTHREADS) k_gemm_grouped_f64(
         if (npi < npairs) nxt = pairs[task.pair_begin + npi];
       }
       const bool have_next = npi < npairs;
-      if (have_next) load_stage(sm, buf ^ 1, A, B, nxt, task.m, task.n, m0, n0, nkt * BK);
+      if (have_next) load_stage<TA, TB>(sm, buf ^ 1, A, B, nxt, task.m, task.n, m0, n0, nkt * BK);
       cp_async_commit();
       cp_async_wait<1>();
       __syncthreads();
+      double a[2][8], b[4][4];
 #pragma unroll
-      for (int kk = 0; kk < BK; kk += 4) {
-        double a[2][2], b[4];
+      for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int i = 0; i < 2; ++i) {
-          a[i][0] = sm.A[buf][kk + t4][wm + i * 16 + g];
-          a[i][1] = sm.A[buf][kk + t4][wm + i * 16 + g + 8];
+        for (int e = 0; e < 8; ++e) {
+          const int r = wm + i * 16 + g + 8 * (e & 1), k = t4 + 4 * (e >> 1);
+          a[i][e] = TA ? sm.A[buf][k][r] : sm.A[buf][r][k];
         }
 #pragma unroll
-        for (int j = 0; j < 4; ++j) b[j] = sm.B[buf][kk + t4][wn + j * 8 + g];
+      for (int j = 0; j < 4; ++j)
 #pragma unroll
-        for (int i = 0; i < 2; ++i)
+        for (int e = 0; e < 4; ++e) {
+          const int k = t4 + 4 * e, cidx = wn + j * 8 + g;
+          b[j][e] = TB ? sm.B[buf][cidx][k] : sm.B[buf][k][cidx];
+        }
 #pragma unroll
-          for (int j = 0; j < 4; ++j) dmma_16x8x4(acc[i][j], a[i][0], a[i][1], b[j]);
-      }
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma_16x8x16(acc[i][j], a[i], b[j]);
       __syncthreads();
       buf ^= 1;
       pi = npi;
@@ -163,7 +171,6 @@ __global__ void __launch_bounds__(NTHREADS) k_gemm_grouped_f64(
       have = have_next;
     }
     cp_async_wait<0>();
-    // epilogue: c0,c1 -> row g, cols 2*t4, 2*t4+1 ; c2,c3 -> row g+8
     double *Cp = C + task.c_off;
 #pragma unroll
     for (int i = 0; i < 2; ++i)
@@ -209,7 +216,7 @@ void build_tiles_f64(const std::vector<GemmTaskD> &tasks, const std::vector<Gemm
 }
 
 ctn_status launch_gemm_f64(const double *A, const double *B, double *C, const GemmTaskD *d_tasks,
-                           const GemmPairD *d_pairs, const GemmTileD *d_tiles, int64_t ntiles,
+                           const GemmPairD *d_pairs, const GemmTileD *d_tiles, int64_t ntiles, int flags,
                            cudaStream_t st) {
   if (ntiles == 0) return CTN_OK;
   int dev = 0, nsm = 148;
@@ -217,7 +224,12 @@ ctn_status launch_gemm_f64(const double *A, const double *B, double *C, const Ge
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   // 128 threads, ~17 KB smem: up to 8+ CTAs per SM resident
   const int64_t grid = std::min<int64_t>(ntiles, (int64_t)nsm * 12);
-  k_gemm_grouped_f64<<<(unsigned)grid, NTHREADS, 0, st>>>(A, B, C, d_tasks, d_pairs, d_tiles, ntiles);
+  switch (flags & 3) {
+    case 0: k_gemm_grouped_f64<false, false><<<(unsigned)grid, NTHREADS, 0, st>>>(A, B, C, d_tasks, d_pairs, d_tiles, ntiles); break;
+    case 1: k_gemm_grouped_f64<true, false><<<(unsigned)grid, NTHREADS, 0, st>>>(A, B, C, d_tasks, d_pairs, d_tiles, ntiles); break;
+    case 2: k_gemm_grouped_f64<false, true><<<(unsigned)grid, NTHREADS, 0, st>>>(A, B, C, d_tasks, d_pairs, d_tiles, ntiles); break;
+    default: k_gemm_grouped_f64<true, true><<<(unsigned)grid, NTHREADS, 0, st>>>(A, B, C, d_tasks, d_pairs, d_tiles, ntiles); break;
+  }
   CTN_CHECK_LAUNCH();
   return CTN_OK;
 }

@@ -25,7 +25,7 @@ struct GemmTileD {
 void build_tiles_f64(const std::vector<GemmTaskD> &tasks, const std::vector<GemmPairD> &pairs,
                      std::vector<GemmTileD> &tiles);
 ctn_status launch_gemm_f64(const double *A, const double *B, double *C, const GemmTaskD *d_tasks,
-                           const GemmPairD *d_pairs, const GemmTileD *d_tiles, int64_t ntiles,
+                           const GemmPairD *d_pairs, const GemmTileD *d_tiles, int64_t ntiles, int flags,
                            cudaStream_t st);
 
 // Host tables + their device copy (uploaded once, on the first launch on a device).
@@ -36,9 +36,14 @@ struct GroupedGemmF64 {
   void *d_mem = nullptr;
   int d_dev = -1;
   double flops = 0.0;
+  int flags = 0;          // operand orientation shared by every pair of the plan
+  bool mixed = false;     // pairs disagree on the orientation (rejected at run time)
 
   void finalize() {
     build_tiles_f64(tasks, pairs, tiles);
+    flags = pairs.empty() ? 0 : (pairs[0].flags & 3);
+    mixed = false;
+    for (const auto &p : pairs) mixed |= ((p.flags & 3) != flags);
     flops = 0.0;
     for (const auto &t : tasks)
       for (int p = 0; p < t.pair_count; ++p)
@@ -69,12 +74,16 @@ struct GroupedGemmF64 {
     return CTN_OK;
   }
   ctn_status run(const double *A, const double *B, double *C, cudaStream_t st) {
+    if (mixed) {
+      set_error("grouped GEMM: all pairs of one plan must share the operand orientation flags");
+      return CTN_ERR_UNSUPPORTED;
+    }
     CTN_TRY(upload(st));
     const char *p = (const char *)d_mem;
     const GemmTaskD *dt = (const GemmTaskD *)p;
     const GemmPairD *dp = (const GemmPairD *)(p + tasks.size() * sizeof(GemmTaskD));
     const GemmTileD *dl = (const GemmTileD *)(p + tasks.size() * sizeof(GemmTaskD) + pairs.size() * sizeof(GemmPairD));
-    return launch_gemm_f64(A, B, C, dt, dp, dl, (int64_t)tiles.size(), st);
+    return launch_gemm_f64(A, B, C, dt, dp, dl, (int64_t)tiles.size(), flags, st);
   }
   ~GroupedGemmF64() {
     if (d_mem) cudaFree(d_mem);

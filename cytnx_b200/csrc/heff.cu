@@ -26,6 +26,7 @@
 #include "ctn_common.h"
 #include "gemm_f64.cuh"
 #include "heff.cuh"
+#include "tc_gemm.cuh"
 
 namespace ctn {
 
@@ -108,22 +109,6 @@ void MpoApply::finalize() {
 
 }  // namespace ctn
 
-struct ctn_heff2_plan {
-  int64_t psi_elems = 0, out_elems = 0, L_elems = 0, R_elems = 0;
-  int64_t x1_elems = 0, x3_elems = 0;
-  // L staged as [a][w][a'] per block (transposed operand of step 1)
-  std::vector<uint64_t> L_shapes;
-  std::vector<int64_t> L_src, L_dst;
-  ctn::GroupedGemmF64 g1, g4;
-  ctn::MpoApply mpo;
-  // bound environment
-  const double *R = nullptr;
-  double *ws = nullptr;  // [Lt | X1 | X3 | reduce ws]
-  bool bound = false;
-  double gemm_flops = 0.0;
-  int64_t n_x1 = 0, n_x3 = 0;
-};
-
 extern "C" ctn_status ctn_heff2_plan_create(const ctn_heff2_desc *d, ctn_heff2_plan **plan) {
   using namespace ctn;
   CTN_REQUIRE(d && d->psi && d->L && d->R && d->M1 && d->M2 && d->out && plan, "ctn_heff2_plan_create: null argument");
@@ -159,6 +144,21 @@ extern "C" ctn_status ctn_heff2_plan_create(const ctn_heff2_desc *d, ctn_heff2_p
   for (int64_t b = 0; b < L.nblocks; ++b) CTN_REQUIRE(sh(L, b, 0) == 1, "ctn_heff2: MPO sectors must have degeneracy 1");
   for (int64_t b = 0; b < R.nblocks; ++b) CTN_REQUIRE(sh(R, b, 0) == 1, "ctn_heff2: MPO sectors must have degeneracy 1");
 
+  auto info = [&](const ctn_block_desc &t, std::vector<BlkInfo> &v) {
+    for (int64_t b = 0; b < t.nblocks; ++b) {
+      BlkInfo bi{};
+      for (int i = 0; i < t.rank && i < 4; ++i) {
+        bi.q[i] = t.itoi[b * t.rank + i];
+        bi.d[i] = t.shapes[b * t.rank + i];
+      }
+      bi.off = t.offs[b];
+      v.push_back(bi);
+    }
+  };
+  info(L, p->Lb);
+  info(P, p->Pb);
+  info(R, p->Rb);
+  info(O, p->Ob);
   // MPO scalars by tuple
   std::unordered_map<Key, double, VecHash> m1v, m2v;
   for (int64_t b = 0; b < M1.nblocks; ++b)
@@ -202,6 +202,7 @@ extern "C" ctn_status ctn_heff2_plan_create(const ctn_heff2_desc *d, ctn_heff2_p
   std::vector<MpoTask> mtasks;
   std::vector<MpoTerm> mterms;
   std::vector<std::vector<std::pair<Key, double>>> x3_terms;
+  std::vector<std::pair<int64_t, int64_t>> x3_or;
   for (int64_t o = 0; o < O.nblocks; ++o) {
     const int64_t ap = it_(O, o, 0), s1p = it_(O, o, 1), s2p = it_(O, o, 2), bp = it_(O, o, 3);
     CTN_REQUIRE(sh(O, o, 1) == 1 && sh(O, o, 2) == 1, "ctn_heff2: physical sectors must have degeneracy 1");
@@ -253,6 +254,7 @@ extern "C" ctn_status ctn_heff2_plan_create(const ctn_heff2_desc *d, ctn_heff2_p
           mterms.push_back(term);
         }
         x3_terms.push_back(terms);
+        x3_or.push_back({o, r});
         mtasks.push_back(mt);
         p->x3_elems += rows * cols;
       }
@@ -309,6 +311,23 @@ extern "C" ctn_status ctn_heff2_plan_create(const ctn_heff2_desc *d, ctn_heff2_p
     for (auto &terms : x3_terms)
       for (auto &tm : terms) mterms[ti++].x1_off = x1_off.at(tm.first);
   }
+  {
+    std::map<Key, int64_t> x1_index;
+    for (size_t i = 0; i < x1_keys.size(); ++i) {
+      x1_index[x1_keys[i]] = (int64_t)i;
+      const X1c c = x1cand.at(x1_keys[i]);
+      p->x1_lp.push_back({c.l, c.p});
+    }
+    for (size_t j = 0; j < x3_terms.size(); ++j) {
+      X3Info xi;
+      xi.o = x3_or[j].first;
+      xi.r = x3_or[j].second;
+      xi.rows = sh(O, xi.o, 0);
+      xi.cols = sh(R, xi.r, 1);
+      for (auto &tm : x3_terms[j]) xi.terms.push_back({x1_index.at(tm.first), tm.second});
+      p->x3.push_back(std::move(xi));
+    }
+  }
   p->mpo.tasks = std::move(mtasks);
   p->mpo.terms = std::move(mterms);
   p->mpo.finalize();
@@ -343,18 +362,27 @@ extern "C" double ctn_heff2_flops(const ctn_heff2_plan *p) {
 }
 extern "C" size_t ctn_heff2_psi_elems(const ctn_heff2_plan *p) { return (size_t)p->psi_elems; }
 
+static int split_kind(int precision) { return precision == CTN_PREC_BF16X3 ? ctn::TC_BF16 : ctn::TC_TF32; }
+
 extern "C" size_t ctn_heff2_workspace_bytes(const ctn_heff2_plan *p, int precision) {
-  (void)precision;
-  return (size_t)(p->L_elems + p->x1_elems + p->x3_elems) * sizeof(double) + 256;
+  if (precision == CTN_PREC_F64) return (size_t)(p->L_elems + p->x1_elems + p->x3_elems) * sizeof(double) + 256;
+  if (precision != CTN_PREC_3XTF32 && precision != CTN_PREC_BF16X3) return 0;
+  auto *pp = const_cast<ctn_heff2_plan *>(p);
+  if (ctn::heff_split_prepare(pp, split_kind(precision)) != CTN_OK) return 0;
+  return ctn::heff_split_ws_bytes(p, split_kind(precision));
 }
 
 extern "C" ctn_status ctn_heff2_set_env(ctn_heff2_plan *p, const double *L, const double *R, void *workspace,
                                         int precision, void *stream) {
   CTN_REQUIRE(p && L && R && workspace, "ctn_heff2_set_env: null argument");
-  if (precision != CTN_PREC_F64) {
-    ctn::set_error("ctn_heff2_set_env: precision %d not built", precision);
-    return CTN_ERR_UNSUPPORTED;
+  if (precision == CTN_PREC_3XTF32 || precision == CTN_PREC_BF16X3) {
+    const int k = split_kind(precision);
+    CTN_TRY(ctn::heff_split_prepare(p, k));
+    CTN_TRY(ctn::heff_split_set_env(p, k, L, R, workspace, ctn::as_stream(stream)));
+    p->split_bound[k] = true;
+    return CTN_OK;
   }
+  CTN_REQUIRE(precision == CTN_PREC_F64, "ctn_heff2_set_env: unknown precision %d", precision);
   const uint64_t mapper[3] = {1, 0, 2};
   p->ws = (double *)workspace;
   CTN_TRY(ctn_permute_blocks(L, p->ws, CTN_FLOAT64, 3, (int64_t)p->L_src.size(), p->L_shapes.data(),
@@ -366,12 +394,15 @@ extern "C" ctn_status ctn_heff2_set_env(ctn_heff2_plan *p, const double *L, cons
 
 extern "C" ctn_status ctn_heff2_matvec(ctn_heff2_plan *p, const double *psi, double *out, int precision,
                                        void *stream) {
-  CTN_REQUIRE(p && p->bound, "ctn_heff2_matvec: environments not bound (call ctn_heff2_set_env)");
-  if (precision != CTN_PREC_F64) {
-    ctn::set_error("ctn_heff2_matvec: precision %d not built", precision);
-    return CTN_ERR_UNSUPPORTED;
-  }
+  CTN_REQUIRE(p, "ctn_heff2_matvec: null plan");
   cudaStream_t st = ctn::as_stream(stream);
+  if (precision == CTN_PREC_3XTF32 || precision == CTN_PREC_BF16X3) {
+    const int k = split_kind(precision);
+    CTN_REQUIRE(p->split_bound[k], "ctn_heff2_matvec: environments not bound for this precision (ctn_heff2_set_env)");
+    return ctn::heff_split_matvec(p, k, psi, out, st, nullptr);
+  }
+  CTN_REQUIRE(precision == CTN_PREC_F64, "ctn_heff2_matvec: unknown precision %d", precision);
+  CTN_REQUIRE(p->bound, "ctn_heff2_matvec: environments not bound (call ctn_heff2_set_env)");
   double *Lt = p->ws;
   double *X1 = Lt + p->L_elems;
   double *X3 = X1 + p->x1_elems;
@@ -404,9 +435,19 @@ extern "C" ctn_status ctn_heff2_lanczos_gnd(ctn_heff2_plan *plan, int precision,
 
 extern "C" ctn_status ctn_heff2_profile(ctn_heff2_plan *p, const double *psi, double *out, int precision, int reps,
                                         double *ms_out, int *launches_out, void *stream) {
-  CTN_REQUIRE(p && p->bound && reps > 0 && ms_out, "ctn_heff2_profile: bad argument");
-  CTN_REQUIRE(precision == CTN_PREC_F64, "ctn_heff2_profile: precision %d not built", precision);
+  CTN_REQUIRE(p && reps > 0 && ms_out, "ctn_heff2_profile: bad argument");
   cudaStream_t st = ctn::as_stream(stream);
+  if (precision == CTN_PREC_3XTF32 || precision == CTN_PREC_BF16X3) {
+    const int k = split_kind(precision);
+    CTN_REQUIRE(p->split_bound[k], "ctn_heff2_profile: environments not bound for this precision");
+    double acc[4] = {0, 0, 0, 0};
+    CTN_TRY(ctn::heff_split_matvec(p, k, psi, out, st, nullptr));  // warm
+    for (int r = 0; r < reps; ++r) CTN_TRY(ctn::heff_split_matvec(p, k, psi, out, st, acc));
+    for (int i = 0; i < 4; ++i) ms_out[i] = acc[i] / reps;
+    if (launches_out) *launches_out = 4;
+    return CTN_OK;
+  }
+  CTN_REQUIRE(p->bound, "ctn_heff2_profile: environments not bound");
   double *Lt = p->ws;
   double *X1 = Lt + p->L_elems;
   double *X3 = X1 + p->x1_elems;
@@ -433,11 +474,18 @@ extern "C" ctn_status ctn_heff2_profile(ctn_heff2_plan *p, const double *psi, do
     }
   }
   for (auto &e : ev) cudaEventDestroy(e);
-  for (int k = 0; k < 3; ++k) ms_out[k] = acc[k] / reps;
+  ms_out[0] = 0.0;
+  for (int k = 0; k < 3; ++k) ms_out[k + 1] = acc[k] / reps;
   if (launches_out) *launches_out = 3;
   return CTN_OK;
 }
 
 extern "C" double ctn_heff2_gemm_flops(const ctn_heff2_plan *p, int step) {
   return step == 1 ? p->g1.flops : step == 4 ? p->g4.flops : 0.0;
+}
+
+extern "C" double ctn_heff2_split_gemm_flops(ctn_heff2_plan *p, int precision, int step) {
+  const int k = split_kind(precision);
+  if (ctn::heff_split_prepare(p, k) != CTN_OK) return 0.0;
+  return ctn::heff_split_gemm_flops(p, k, step);
 }

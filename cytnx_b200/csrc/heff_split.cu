@@ -1,0 +1,382 @@
+// Split-precision (3xTF32 / BF16x3) form of the two-site H_eff matvec on tcgen05.
+//
+// Same algorithm as the FP64 plan (heff.cu), re-laid out for the tensor cores:
+//   step 1: one stacked GEMM per left sector a:
+//           X1_a[(w,a') rows][(s1,s2,b) cols] = L_a^T (rows of every L block (w,a,a'))
+//                                             x psi_a (columns of every psi block (a,..))
+//           A = L (packed once per environment), B = psi (packed per matvec),
+//           FP32 result in a dense per-group matrix;
+//   steps 2+3: X3 blocks = MPO-weighted sums of X1 blocks, written directly as the
+//           split, swizzled A panels of step 4 (no intermediate FP32 X3 array);
+//   step 4: one stacked GEMM per right sector b':
+//           out[(a',s1',s2') rows][b'] = X3_b'[rows][(w2,b) K] x R_b'[(w2,b)][b'],
+//           B = R (packed once), FP64 stores straight into the out blocks.
+// The K offsets of the R blocks inside a step-4 group are padded to multiples of 8 so
+// that every 16-byte panel chunk belongs to one X3 block.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "ctn_common.h"
+#include "gemm_f64.cuh"
+#include "heff.cuh"
+#include "tc_gemm.cuh"
+
+namespace ctn {
+
+struct MpoSegS {
+  int32_t rows, cols;
+  int32_t row0, k0;
+  int64_t panel_off;
+  int32_t kb, pad_;
+  int32_t term_begin, term_count;
+};
+struct MpoTermS {
+  int64_t x1_off;  // FP32 element offset of the X1 block's (0,0)
+  int64_t ld;
+  double coef;
+};
+
+struct HeffSplit {
+  int kind = TC_TF32;
+  TcGemm g1, g4;
+  Packer pk_L, pk_P, pk_R;
+  std::vector<MpoSegS> segs;
+  std::vector<MpoTermS> terms;
+  std::vector<int64_t> seg_begin;
+  int64_t nchunks = 0;
+  void *d_mpo = nullptr;
+  int d_dev = -1;
+  int64_t x1_elems = 0;
+  // workspace layout (bytes)
+  int64_t o_a1h, o_a1l, o_b1h, o_b1l, o_x1, o_a4h, o_a4l, o_b4h, o_b4l, o_err, total;
+  std::vector<std::pair<int64_t, int64_t>> uncovered;  // out ranges no group writes (zero them)
+  uint8_t *ws = nullptr;
+  ~HeffSplit() {
+    if (d_mpo) cudaFree(d_mpo);
+  }
+};
+
+void heff_split_free(HeffSplit *s) { delete s; }
+
+namespace {
+constexpr int KALIGN = 8;
+
+int64_t up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+__device__ __forceinline__ float to_tf32f(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+struct MpoSParams {
+  const MpoSegS *segs;
+  const MpoTermS *terms;
+  const int64_t *begin;
+  int nseg;
+  int64_t nchunks;
+  int kind;
+  const float *x1;
+  uint8_t *hi, *lo;
+};
+
+__global__ void __launch_bounds__(256) k_mpo_split(MpoSParams p) {
+  const int64_t step = (int64_t)gridDim.x * blockDim.x;
+  const int E = p.kind == TC_TF32 ? 4 : 8;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < p.nchunks; c += step) {
+    int a = 0, b = p.nseg - 1;
+    while (a < b) {
+      const int mid = (a + b + 1) >> 1;
+      if (p.begin[mid] <= c) a = mid;
+      else b = mid - 1;
+    }
+    const MpoSegS s = p.segs[a];
+    const int64_t cl = c - p.begin[a];
+    const int kc = (int)(cl % ((s.cols + E - 1) / E));  // k chunks fastest: contiguous X1 reads
+    const int r = (int)(cl / ((s.cols + E - 1) / E));
+    const int kloc = kc * E;
+    double x[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) x[e] = 0.0;
+    for (int t = 0; t < s.term_count; ++t) {
+      const MpoTermS tm = p.terms[s.term_begin + t];
+      const float *src = p.x1 + tm.x1_off + (int64_t)r * tm.ld + kloc;
+#pragma unroll
+      for (int e = 0; e < 8; ++e)
+        if (e < E && kloc + e < s.cols) x[e] = fma(tm.coef, (double)src[e], x[e]);
+    }
+    const int64_t off = s.panel_off + tc_panel_offset(s.row0 + r, s.k0 + kloc, TC_BM, s.kb, p.kind);
+    if (p.kind == TC_TF32) {
+      float h[4], l[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        h[e] = to_tf32f((float)x[e]);
+        l[e] = to_tf32f((float)(x[e] - (double)h[e]));
+      }
+      *(float4 *)(p.hi + off) = make_float4(h[0], h[1], h[2], h[3]);
+      *(float4 *)(p.lo + off) = make_float4(l[0], l[1], l[2], l[3]);
+    } else {
+      __nv_bfloat16 h[8], l[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        h[e] = __double2bfloat16(x[e]);
+        l[e] = __double2bfloat16(x[e] - (double)__bfloat162float(h[e]));
+      }
+      *(uint4 *)(p.hi + off) = *(uint4 *)h;
+      *(uint4 *)(p.lo + off) = *(uint4 *)l;
+    }
+  }
+}
+}  // namespace
+
+ctn_status heff_split_prepare(ctn_heff2_plan *p, int kind) {
+  if (p->split[kind]) return CTN_OK;
+  std::unique_ptr<HeffSplit> s(new HeffSplit());
+  s->kind = kind;
+  s->g1.kind = s->g4.kind = kind;
+  s->g1.bn = s->g4.bn = 128;
+  s->pk_L.kind = s->pk_P.kind = s->pk_R.kind = kind;
+  const int bn = 128;
+  // ---------------- step 1 groups: one per left sector a
+  std::map<int64_t, std::vector<int64_t>> Lg, Pg;
+  for (size_t l = 0; l < p->Lb.size(); ++l) Lg[p->Lb[l].q[1]].push_back((int64_t)l);
+  for (size_t q = 0; q < p->Pb.size(); ++q) Pg[p->Pb[q].q[0]].push_back((int64_t)q);
+  std::vector<int64_t> l_group(p->Lb.size(), -1), l_row(p->Lb.size(), 0);
+  std::vector<int64_t> p_group(p->Pb.size(), -1), p_col(p->Pb.size(), 0);
+  std::vector<int64_t> g1_coff, g1_ldc;
+  int64_t x1 = 0;
+  for (auto &kv : Lg) {
+    auto jt = Pg.find(kv.first);
+    if (jt == Pg.end()) continue;
+    int64_t M = 0, N = 0;
+    const int64_t K = p->Lb[kv.second[0]].d[1];
+    for (int64_t l : kv.second) {
+      l_row[l] = M;
+      M += p->Lb[l].d[0] * p->Lb[l].d[2];
+    }
+    for (int64_t q : jt->second) {
+      p_col[q] = N;
+      N += p->Pb[q].d[1] * p->Pb[q].d[2] * p->Pb[q].d[3];
+    }
+    if (M == 0 || N == 0 || K == 0) continue;
+    const int gi = s->g1.add_group((int)M, (int)N, (int)K, 0, x1, (int)N, 0);
+    for (int64_t l : kv.second) l_group[l] = gi;
+    for (int64_t q : jt->second) p_group[q] = gi;
+    g1_coff.push_back(x1);
+    g1_ldc.push_back(N);
+    x1 += M * N;
+  }
+  s->x1_elems = x1;
+  s->g1.finalize();
+  for (size_t l = 0; l < p->Lb.size(); ++l) {
+    if (l_group[l] < 0) continue;
+    const TcGroup &g = s->g1.groups[l_group[l]];
+    const BlkInfo &b = p->Lb[l];  // [w][a][a'] with d[0] == 1: element (row a', k a) at off + k*d2 + row
+    PackSeg sg{b.off, 1, b.d[2], (int32_t)b.d[2], (int32_t)b.d[1], (int32_t)l_row[l], 0, g.a_off, TC_BM, g.kb};
+    s->pk_L.segs.push_back(sg);
+  }
+  for (size_t q = 0; q < p->Pb.size(); ++q) {
+    if (p_group[q] < 0) continue;
+    const TcGroup &g = s->g1.groups[p_group[q]];
+    const BlkInfo &b = p->Pb[q];  // [a][1][1][b]: element (row b, k a) at off + k*d3 + row
+    PackSeg sg{b.off, 1, b.d[3], (int32_t)b.d[3], (int32_t)b.d[0], (int32_t)p_col[q], 0, g.b_off, bn, g.kb};
+    s->pk_P.segs.push_back(sg);
+  }
+  s->pk_L.finalize();
+  s->pk_P.finalize();
+  // ---------------- step 4 groups: one per right sector b'
+  std::map<int64_t, std::vector<int64_t>> Og, Rg;
+  for (size_t o = 0; o < p->Ob.size(); ++o) Og[p->Ob[o].q[3]].push_back((int64_t)o);
+  for (size_t r = 0; r < p->Rb.size(); ++r) Rg[p->Rb[r].q[2]].push_back((int64_t)r);
+  std::vector<int64_t> o_group(p->Ob.size(), -1), o_row(p->Ob.size(), 0);
+  std::vector<int64_t> r_group(p->Rb.size(), -1), r_k(p->Rb.size(), 0);
+  for (auto &kv : Og) {
+    auto jt = Rg.find(kv.first);
+    if (jt == Rg.end()) continue;
+    int64_t M = 0, K = 0;
+    const int64_t N = p->Ob[kv.second[0]].d[3];
+    for (int64_t o : kv.second) {
+      o_row[o] = M;
+      M += p->Ob[o].d[0];
+    }
+    for (int64_t r : jt->second) {
+      r_k[r] = K;
+      K = up(K + p->Rb[r].d[1], KALIGN);
+    }
+    if (M == 0 || N == 0 || K == 0) continue;
+    const int64_t rm = (int64_t)s->g4.rowmap.size();
+    for (int64_t o : kv.second)
+      for (int64_t i = 0; i < p->Ob[o].d[0]; ++i)
+        s->g4.rowmap.push_back(p->Ob[o].off + i * p->Ob[o].d[1] * p->Ob[o].d[2] * p->Ob[o].d[3]);
+    const int gi = s->g4.add_group((int)M, (int)N, (int)K, 1, 0, (int)N, rm);
+    for (int64_t o : kv.second) o_group[o] = gi;
+    for (int64_t r : jt->second) r_group[r] = gi;
+  }
+  s->g4.finalize();
+  for (size_t r = 0; r < p->Rb.size(); ++r) {
+    if (r_group[r] < 0) continue;
+    const TcGroup &g = s->g4.groups[r_group[r]];
+    const BlkInfo &b = p->Rb[r];  // [w2][b][b']: element (row b', k b) at off + k*d2 + row
+    PackSeg sg{b.off, 1, b.d[2], (int32_t)b.d[2], (int32_t)b.d[1], 0, (int32_t)r_k[r], g.b_off, bn, g.kb};
+    s->pk_R.segs.push_back(sg);
+  }
+  s->pk_R.finalize();
+  // out blocks no step-4 group writes must read as zeros
+  for (size_t o = 0; o < p->Ob.size(); ++o)
+    if (o_group[o] < 0) {
+      const BlkInfo &b = p->Ob[o];
+      s->uncovered.push_back({b.off, b.d[0] * b.d[1] * b.d[2] * b.d[3]});
+    }
+  // ---------------- MPO segments: X3 blocks into the step-4 A panels
+  const int E = kind == TC_TF32 ? 4 : 8;
+  s->seg_begin.push_back(0);
+  for (const X3Info &xi : p->x3) {
+    if (o_group[xi.o] < 0 || r_group[xi.r] < 0 || o_group[xi.o] != r_group[xi.r]) {
+      set_error("heff split plan: inconsistent step-4 grouping");
+      return CTN_ERR_INVALID;
+    }
+    const TcGroup &g = s->g4.groups[o_group[xi.o]];
+    MpoSegS sg;
+    sg.rows = (int32_t)xi.rows;
+    sg.cols = (int32_t)xi.cols;
+    sg.row0 = (int32_t)o_row[xi.o];
+    sg.k0 = (int32_t)r_k[xi.r];
+    sg.panel_off = g.a_off;
+    sg.kb = g.kb;
+    sg.pad_ = 0;
+    sg.term_begin = (int32_t)s->terms.size();
+    sg.term_count = (int32_t)xi.terms.size();
+    for (auto &tm : xi.terms) {
+      const int64_t l = p->x1_lp[tm.first].first, q = p->x1_lp[tm.first].second;
+      const int64_t gi = l_group[l];
+      if (gi < 0 || p_group[q] != gi) {
+        set_error("heff split plan: X1 block outside the step-1 groups");
+        return CTN_ERR_INVALID;
+      }
+      MpoTermS t;
+      t.ld = g1_ldc[gi];
+      t.x1_off = g1_coff[gi] + l_row[l] * t.ld + p_col[q];
+      t.coef = tm.second;
+      s->terms.push_back(t);
+    }
+    s->segs.push_back(sg);
+    s->seg_begin.push_back(s->seg_begin.back() + (int64_t)xi.rows * ((xi.cols + E - 1) / E));
+  }
+  s->nchunks = s->seg_begin.back();
+  // ---------------- workspace layout
+  int64_t o = 0;
+  auto take = [&](int64_t bytes) {
+    const int64_t at = o;
+    o = up(o + bytes, 1024);
+    return at;
+  };
+  s->o_a1h = take(s->g1.a_bytes);
+  s->o_a1l = take(s->g1.a_bytes);
+  s->o_b1h = take(s->g1.b_bytes);
+  s->o_b1l = take(s->g1.b_bytes);
+  s->o_x1 = take(s->x1_elems * 4);
+  s->o_a4h = take(s->g4.a_bytes);
+  s->o_a4l = take(s->g4.a_bytes);
+  s->o_b4h = take(s->g4.b_bytes);
+  s->o_b4l = take(s->g4.b_bytes);
+  s->o_err = take(256);
+  s->total = o;
+  p->split[kind] = s.release();
+  return CTN_OK;
+}
+
+double heff_split_gemm_flops(const ctn_heff2_plan *p, int kind, int step) {
+  const HeffSplit *s = p->split[kind];
+  if (!s) return 0.0;
+  return step == 1 ? s->g1.flops : step == 4 ? s->g4.flops : 0.0;
+}
+
+size_t heff_split_ws_bytes(const ctn_heff2_plan *p, int kind) {
+  return p->split[kind] ? (size_t)p->split[kind]->total : 0;
+}
+
+ctn_status heff_split_set_env(ctn_heff2_plan *p, int kind, const double *L, const double *R, void *ws,
+                              cudaStream_t st) {
+  HeffSplit *s = p->split[kind];
+  CTN_REQUIRE(s, "heff split: not prepared");
+  s->ws = (uint8_t *)ws;
+  CTN_CUDA(cudaMemsetAsync(ws, 0, s->total, st));
+  CTN_TRY(s->pk_L.run(L, 0, s->ws + s->o_a1h, s->ws + s->o_a1l, st));
+  CTN_TRY(s->pk_R.run(R, 0, s->ws + s->o_b4h, s->ws + s->o_b4l, st));
+  // device copy of the MPO segment tables
+  int dev = 0;
+  CTN_CUDA(cudaGetDevice(&dev));
+  if (!s->d_mpo || s->d_dev != dev) {
+    if (s->d_mpo) cudaFree(s->d_mpo);
+    const size_t bytes = s->segs.size() * sizeof(MpoSegS) + s->terms.size() * sizeof(MpoTermS) +
+                         s->seg_begin.size() * sizeof(int64_t) + 64;
+    CTN_CUDA(cudaMalloc(&s->d_mpo, bytes));
+    s->d_dev = dev;
+    char *q = (char *)s->d_mpo;
+    if (!s->segs.empty()) CTN_CUDA(cudaMemcpyAsync(q, s->segs.data(), s->segs.size() * sizeof(MpoSegS), cudaMemcpyHostToDevice, st));
+    q += s->segs.size() * sizeof(MpoSegS);
+    if (!s->terms.empty()) CTN_CUDA(cudaMemcpyAsync(q, s->terms.data(), s->terms.size() * sizeof(MpoTermS), cudaMemcpyHostToDevice, st));
+    q += s->terms.size() * sizeof(MpoTermS);
+    CTN_CUDA(cudaMemcpyAsync(q, s->seg_begin.data(), s->seg_begin.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    CTN_CUDA(cudaStreamSynchronize(st));
+  }
+  CTN_TRY(s->g1.upload(st));
+  CTN_TRY(s->g4.upload(st));
+  CTN_TRY(s->pk_P.upload(st));
+  return CTN_OK;
+}
+
+ctn_status heff_split_matvec(ctn_heff2_plan *p, int kind, const double *psi, double *out, cudaStream_t st,
+                             double *ms4) {
+  HeffSplit *s = p->split[kind];
+  CTN_REQUIRE(s && s->ws, "heff split: environments not bound");
+  uint8_t *w = s->ws;
+  cudaEvent_t ev[5];
+  if (ms4)
+    for (auto &e : ev) CTN_CUDA(cudaEventCreate(&e));
+  if (ms4) CTN_CUDA(cudaEventRecord(ev[0], st));
+  for (auto &u : s->uncovered) CTN_CUDA(cudaMemsetAsync(out + u.first, 0, u.second * sizeof(double), st));
+  CTN_TRY(s->pk_P.run(psi, 0, w + s->o_b1h, w + s->o_b1l, st));
+  if (ms4) CTN_CUDA(cudaEventRecord(ev[1], st));
+  int *err = (int *)(w + s->o_err);
+  CTN_TRY(s->g1.run(w + s->o_a1h, w + s->o_a1l, w + s->o_b1h, w + s->o_b1l, (float *)(w + s->o_x1), nullptr, err, st));
+  if (ms4) CTN_CUDA(cudaEventRecord(ev[2], st));
+  if (s->nchunks) {
+    MpoSParams prm;
+    const char *q = (const char *)s->d_mpo;
+    prm.segs = (const MpoSegS *)q;
+    prm.terms = (const MpoTermS *)(q + s->segs.size() * sizeof(MpoSegS));
+    prm.begin = (const int64_t *)(q + s->segs.size() * sizeof(MpoSegS) + s->terms.size() * sizeof(MpoTermS));
+    prm.nseg = (int)s->segs.size();
+    prm.nchunks = s->nchunks;
+    prm.kind = kind;
+    prm.x1 = (const float *)(w + s->o_x1);
+    prm.hi = w + s->o_a4h;
+    prm.lo = w + s->o_a4l;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t grid = std::min<int64_t>((s->nchunks + 255) / 256, (int64_t)nsm * 16);
+    k_mpo_split<<<(unsigned)grid, 256, 0, st>>>(prm);
+    CTN_CHECK_LAUNCH();
+  }
+  if (ms4) CTN_CUDA(cudaEventRecord(ev[3], st));
+  CTN_TRY(s->g4.run(w + s->o_a4h, w + s->o_a4l, w + s->o_b4h, w + s->o_b4l, nullptr, out, err, st));
+  if (ms4) {
+    CTN_CUDA(cudaEventRecord(ev[4], st));
+    CTN_CUDA(cudaEventSynchronize(ev[4]));
+    for (int k = 0; k < 4; ++k) {
+      float ms = 0.f;
+      CTN_CUDA(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+      ms4[k] += ms;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+  }
+  return CTN_OK;
+}
+
+}  // namespace ctn

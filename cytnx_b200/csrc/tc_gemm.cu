@@ -1,0 +1,577 @@
+// tcgen05 split-precision grouped GEMM (see tc_gemm.cuh for the operand format).
+//
+// Persistent, warp-specialised CTA of 192 threads, one CTA per SM:
+//   warp 0  (1 thread)  producer: per K slice, 4 bulk copies (A_hi, A_lo, B_hi, B_lo)
+//                        into an S-stage shared-memory ring, completion on mbarriers;
+//   warp 1  (1 thread)  MMA issuer: tcgen05.mma kind::tf32 / kind::f16 (BF16), M=128,
+//                        N=BN, accumulating lo*hi + hi*lo + hi*hi into a TMEM buffer;
+//                        tcgen05.commit releases a ring slot / publishes a finished tile;
+//   warps 2-5           epilogue: tcgen05.ld (32x32b) of the accumulator, FP32 or FP64
+//                        stores; two TMEM accumulator buffers let the epilogue of tile i
+//                        overlap the main loop of tile i+1.
+// Every wait is bounded: on expiry the kernel records an error code in p.err, drains
+// its own bulk copies and MMAs (again bounded), frees its TMEM and returns.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cstring>
+
+#include "tc_gemm.cuh"
+
+namespace ctn {
+
+namespace {
+
+constexpr int NTHREADS_TC = 192;
+constexpr long long SPIN_LIMIT = 1ll << 24;  // try_wait probes before giving up (~seconds)
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait; returns false (and records `code`) when the limit is reached
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code) {
+  for (long long i = 0; i < SPIN_LIMIT; ++i) {
+    if (mbar_try(bar, parity)) return true;
+    if ((i & 1023) == 1023 && *(volatile int *)err != 0) return false;  // another role gave up
+  }
+  atomicCAS(err, 0, code);
+  return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ uint64_t smem_desc(const void *p) {
+  const uint64_t a = smem_u32(p);
+  return ((a & 0x3FFFFull) >> 4) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accum, int kind) {
+  if (kind == TC_TF32) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum));
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum));
+  }
+}
+__device__ __forceinline__ void tc_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(addr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+template <int KIND, int BN, int STAGES>
+struct TcSmem {
+  static constexpr int A_BYTES = TC_A_TILE;
+  static constexpr int B_BYTES = BN * TC_ROW_BYTES;
+  static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+  static constexpr int RING = STAGES * STAGE_BYTES;
+  static constexpr int BAR_OFF = RING;                 // full[S], empty[S], tfull[2], tempty[2], drain
+  static constexpr int TOTAL = RING + 8 * (2 * STAGES + 5) + 16;
+};
+
+template <int KIND, int BN, int STAGES>
+__global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
+  using SM = TcSmem<KIND, BN, STAGES>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t *full = (uint64_t *)(smem + SM::BAR_OFF);
+  uint64_t *empty = full + STAGES;
+  uint64_t *tfull = empty + STAGES;
+  uint64_t *tempty = tfull + 2;
+  uint64_t *drain = tempty + 2;
+  uint32_t *tmem_holder = (uint32_t *)(drain + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr uint32_t TMEM_COLS = 2 * BN;  // two accumulator buffers (power of two: 256 or 512)
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&tfull[a], 1);
+      mbar_init(&tempty[a], 4);
+    }
+    mbar_init(drain, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_holder)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_holder;
+
+  constexpr uint32_t FMT = KIND == TC_TF32 ? 2u : 1u;
+  constexpr uint32_t IDESC = (1u << 4) | (FMT << 7) | (FMT << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+  constexpr int KSTEPS = 4;  // MMA K per instruction = 32 bytes of the 128-byte slice
+
+  if (warp == 0 && lane == 0) {
+    // ---------------------------------------------------------------- producer
+    int stage = 0;
+    uint32_t phase = 0;
+    uint32_t filled[STAGES];
+    for (int s = 0; s < STAGES; ++s) filled[s] = 0;
+    bool ok = true;
+    for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
+      const TcTile tl = p.tiles[t];
+      const TcGroup g = p.groups[tl.group];
+      for (int kb = 0; kb < g.kb; ++kb) {
+        if (!mbar_wait(&empty[stage], phase ^ 1, p.err, 1)) {
+          ok = false;
+          break;
+        }
+        uint8_t *st = smem + stage * SM::STAGE_BYTES;
+        mbar_expect_tx(&full[stage], SM::STAGE_BYTES);
+        const int64_t ao = g.a_off + ((int64_t)tl.mt * g.kb + kb) * SM::A_BYTES;
+        const int64_t bo = g.b_off + ((int64_t)tl.nt * g.kb + kb) * SM::B_BYTES;
+        bulk_g2s(st, p.a_hi + ao, SM::A_BYTES, &full[stage]);
+        bulk_g2s(st + SM::A_BYTES, p.a_lo + ao, SM::A_BYTES, &full[stage]);
+        bulk_g2s(st + 2 * SM::A_BYTES, p.b_hi + bo, SM::B_BYTES, &full[stage]);
+        bulk_g2s(st + 2 * SM::A_BYTES + SM::B_BYTES, p.b_lo + bo, SM::B_BYTES, &full[stage]);
+        filled[stage]++;
+        if (++stage == STAGES) {
+          stage = 0;
+          phase ^= 1;
+        }
+      }
+    }
+    // drain: every issued fill must have landed before the CTA may exit
+    for (int s = 0; s < STAGES; ++s)
+      if (filled[s]) mbar_wait(&full[s], (filled[s] - 1) & 1, p.err, 5);
+  } else if (warp == 1 && lane == 0) {
+    // ---------------------------------------------------------------- MMA issuer
+    int stage = 0;
+    uint32_t phase = 0;
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    bool ok = true;
+    bool issued = false;
+    for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
+      const TcTile tl = p.tiles[t];
+      const TcGroup g = p.groups[tl.group];
+      if (!mbar_wait(&tempty[acc], acc_phase ^ 1, p.err, 2)) break;
+      tc_fence_after();
+      const uint32_t d = tmem_base + (uint32_t)(acc * BN);
+      for (int kb = 0; kb < g.kb; ++kb) {
+        if (!mbar_wait(&full[stage], phase, p.err, 3)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        uint8_t *st = smem + stage * SM::STAGE_BYTES;
+        const uint64_t ahi = smem_desc(st), alo = smem_desc(st + SM::A_BYTES);
+        const uint64_t bhi = smem_desc(st + 2 * SM::A_BYTES), blo = smem_desc(st + 2 * SM::A_BYTES + SM::B_BYTES);
+#pragma unroll
+        for (int j = 0; j < KSTEPS; ++j) {
+          const uint64_t adv = (uint64_t)(j * 32) >> 4;  // +32 bytes along K inside the swizzle row
+          tc_mma(d, alo + adv, bhi + adv, IDESC, (kb | j) != 0, KIND);
+          tc_mma(d, ahi + adv, blo + adv, IDESC, 1u, KIND);
+          tc_mma(d, ahi + adv, bhi + adv, IDESC, 1u, KIND);
+        }
+        issued = true;
+        tc_commit(&empty[stage]);
+        if (++stage == STAGES) {
+          stage = 0;
+          phase ^= 1;
+        }
+      }
+      if (!ok) break;
+      tc_commit(&tfull[acc]);
+      if (++acc == 2) {
+        acc = 0;
+        acc_phase ^= 1;
+      }
+    }
+    // all MMAs of this CTA complete before TMEM is released
+    if (issued) {
+      tc_commit(drain);
+      mbar_wait(drain, 0, p.err, 6);
+    }
+  } else if (warp >= 2) {
+    // ---------------------------------------------------------------- epilogue
+    const int q = warp & 3;  // TMEM lane quarter this warp may access
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    for (int64_t t = blockIdx.x; t < p.ntiles; t += gridDim.x) {
+      const TcTile tl = p.tiles[t];
+      const TcGroup g = p.groups[tl.group];
+      // warp-uniform bounded wait (the TMEM loads below are .sync.aligned)
+      int okw = 0;
+      if (lane == 0) okw = mbar_wait(&tfull[acc], acc_phase, p.err, 4) ? 1 : 0;
+      okw = __shfl_sync(0xffffffffu, okw, 0);
+      __syncwarp();
+      if (!okw) break;
+      tc_fence_after();
+      const int r = tl.mt * TC_BM + q * 32 + lane;
+      const uint32_t base = tmem_base + (uint32_t)(acc * BN) + ((uint32_t)(q * 32) << 16);
+      const bool row_ok = r < g.M;
+      int64_t dst = 0;
+      if (row_ok) dst = g.mode == 0 ? g.c_off + (int64_t)r * g.ldc : p.rowmap[g.rm_off + r];
+#pragma unroll 1
+      for (int c0 = 0; c0 < BN; c0 += 16) {
+        uint32_t v[16];
+        tmem_ld16(base + c0, v);
+        tmem_wait_ld();
+        const int cg = tl.nt * BN + c0;
+        if (row_ok && cg < g.N) {
+          if (g.mode == 0) {
+            float *o = p.c32 + dst + cg;
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+              if (cg + i < g.N) o[i] = __uint_as_float(v[i]);
+          } else {
+            double *o = p.c64 + dst + cg;
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+              if (cg + i < g.N) o[i] = (double)__uint_as_float(v[i]);
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty[acc]);
+      if (++acc == 2) {
+        acc = 0;
+        acc_phase ^= 1;
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
+  }
+}
+
+// ------------------------------------------------------------------ packing
+__device__ __forceinline__ float to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+struct PackParams {
+  const PackSeg *segs;
+  const int64_t *begin;  // chunk prefix per segment (nseg + 1)
+  int nseg;
+  int64_t nchunks;
+  int kind;
+  int src_f32;
+  const void *src;
+  uint8_t *hi, *lo;
+};
+
+__global__ void __launch_bounds__(256) k_pack(PackParams p) {
+  const int64_t step = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < p.nchunks; c += step) {
+    int lo_s = 0, hi_s = p.nseg - 1;
+    while (lo_s < hi_s) {  // last segment with begin <= c
+      const int mid = (lo_s + hi_s + 1) >> 1;
+      if (p.begin[mid] <= c) lo_s = mid;
+      else hi_s = mid - 1;
+    }
+    const PackSeg s = p.segs[lo_s];
+    const int64_t cl = c - p.begin[lo_s];
+    const int r = (int)(cl % s.rows);
+    const int kc = (int)(cl / s.rows);
+    const int E = p.kind == TC_TF32 ? 4 : 8;  // elements per 16-byte chunk
+    const int kloc = kc * E;
+    double x[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      x[e] = 0.0;
+      if (e < E && kloc + e < s.cols) {
+        const int64_t idx = s.src_off + (int64_t)r * s.sr + (int64_t)(kloc + e) * s.sk;
+        x[e] = p.src_f32 ? (double)((const float *)p.src)[idx] : ((const double *)p.src)[idx];
+      }
+    }
+    const int64_t off = s.panel_off + tc_panel_offset(s.row0 + r, s.k0 + kloc, s.tile_rows, s.kb, p.kind);
+    if (p.kind == TC_TF32) {
+      float h[4], l[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        h[e] = to_tf32((float)x[e]);
+        l[e] = to_tf32((float)(x[e] - (double)h[e]));
+      }
+      *(float4 *)(p.hi + off) = make_float4(h[0], h[1], h[2], h[3]);
+      *(float4 *)(p.lo + off) = make_float4(l[0], l[1], l[2], l[3]);
+    } else {
+      __nv_bfloat16 h[8], l[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        h[e] = __double2bfloat16(x[e]);
+        l[e] = __double2bfloat16(x[e] - (double)__bfloat162float(h[e]));
+      }
+      *(uint4 *)(p.hi + off) = *(uint4 *)h;
+      *(uint4 *)(p.lo + off) = *(uint4 *)l;
+    }
+  }
+}
+
+int nsm_count() {
+  int dev = 0, n = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n > 0 ? n : 148;
+}
+
+template <int KIND, int BN, int STAGES>
+ctn_status launch_tc(const TcParams &prm, int64_t ntiles, cudaStream_t st) {
+  using SM = TcSmem<KIND, BN, STAGES>;
+  const int smem = SM::TOTAL + 1024;
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_set[dev & 63]) {
+    CTN_CUDA(cudaFuncSetAttribute(k_tc_gemm<KIND, BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr_set[dev & 63] = true;
+  }
+  const int grid = (int)std::min<int64_t>(ntiles, nsm_count());
+  k_tc_gemm<KIND, BN, STAGES><<<grid, NTHREADS_TC, smem, st>>>(prm);
+  CTN_CHECK_LAUNCH();
+  return CTN_OK;
+}
+
+}  // namespace
+
+int TcGemm::add_group(int M, int N, int K, int mode, int64_t c_off, int ldc, int64_t rm_off) {
+  TcGroup g;
+  const int ks = tc_k_per_slice(kind);
+  g.M = M;
+  g.N = N;
+  g.K = K;
+  g.mt = (M + TC_BM - 1) / TC_BM;
+  g.nt = (N + bn - 1) / bn;
+  g.kb = (K + ks - 1) / ks;
+  g.mode = mode;
+  g.c_off = c_off;
+  g.ldc = ldc;
+  g.rm_off = rm_off;
+  g.a_off = a_bytes;
+  g.b_off = b_bytes;
+  a_bytes += (int64_t)g.mt * g.kb * TC_A_TILE;
+  b_bytes += (int64_t)g.nt * g.kb * bn * TC_ROW_BYTES;
+  groups.push_back(g);
+  flops += 2.0 * M * (double)N * K;
+  return (int)groups.size() - 1;
+}
+
+void TcGemm::finalize() {
+  std::vector<std::pair<int, TcTile>> tmp;
+  for (size_t i = 0; i < groups.size(); ++i) {
+    const TcGroup &g = groups[i];
+    if (g.kb == 0) continue;
+    for (int m = 0; m < g.mt; ++m)
+      for (int n = 0; n < g.nt; ++n) tmp.push_back({g.kb, TcTile{(int32_t)i, m, n, 0}});
+  }
+  std::stable_sort(tmp.begin(), tmp.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
+  tiles.clear();
+  for (auto &x : tmp) tiles.push_back(x.second);
+}
+
+ctn_status TcGemm::upload(cudaStream_t st) {
+  int dev = 0;
+  CTN_CUDA(cudaGetDevice(&dev));
+  if (d_mem && d_dev == dev) return CTN_OK;
+  if (d_mem) cudaFree(d_mem);
+  d_mem = nullptr;
+  const size_t bytes = groups.size() * sizeof(TcGroup) + tiles.size() * sizeof(TcTile) +
+                       rowmap.size() * sizeof(int64_t) + 256;
+  CTN_CUDA(cudaMalloc(&d_mem, bytes));
+  d_dev = dev;
+  char *q = (char *)d_mem;
+  if (!groups.empty()) CTN_CUDA(cudaMemcpyAsync(q, groups.data(), groups.size() * sizeof(TcGroup), cudaMemcpyHostToDevice, st));
+  q += groups.size() * sizeof(TcGroup);
+  if (!tiles.empty()) CTN_CUDA(cudaMemcpyAsync(q, tiles.data(), tiles.size() * sizeof(TcTile), cudaMemcpyHostToDevice, st));
+  q += tiles.size() * sizeof(TcTile);
+  if (!rowmap.empty()) CTN_CUDA(cudaMemcpyAsync(q, rowmap.data(), rowmap.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+  CTN_CUDA(cudaStreamSynchronize(st));
+  return CTN_OK;
+}
+
+ctn_status TcGemm::run(const uint8_t *a_hi, const uint8_t *a_lo, const uint8_t *b_hi, const uint8_t *b_lo,
+                       float *c32, double *c64, int *err, cudaStream_t st) {
+  if (tiles.empty()) return CTN_OK;
+  CTN_TRY(upload(st));
+  TcParams prm;
+  const char *q = (const char *)d_mem;
+  prm.groups = (const TcGroup *)q;
+  prm.tiles = (const TcTile *)(q + groups.size() * sizeof(TcGroup));
+  prm.rowmap = (const int64_t *)(q + groups.size() * sizeof(TcGroup) + tiles.size() * sizeof(TcTile));
+  prm.ntiles = (int64_t)tiles.size();
+  prm.a_hi = a_hi;
+  prm.a_lo = a_lo;
+  prm.b_hi = b_hi;
+  prm.b_lo = b_lo;
+  prm.c32 = c32;
+  prm.c64 = c64;
+  prm.err = err;
+  if (kind == TC_TF32 && bn == 128) return launch_tc<TC_TF32, 128, 3>(prm, prm.ntiles, st);
+  if (kind == TC_BF16 && bn == 128) return launch_tc<TC_BF16, 128, 3>(prm, prm.ntiles, st);
+  if (kind == TC_TF32 && bn == 256) return launch_tc<TC_TF32, 256, 2>(prm, prm.ntiles, st);
+  if (kind == TC_BF16 && bn == 256) return launch_tc<TC_BF16, 256, 2>(prm, prm.ntiles, st);
+  set_error("tcgen05 GEMM: unsupported tile width %d", bn);
+  return CTN_ERR_UNSUPPORTED;
+}
+
+TcGemm::~TcGemm() {
+  if (d_mem) cudaFree(d_mem);
+}
+
+void Packer::finalize() {
+  seg_chunk_begin.assign(segs.size() + 1, 0);
+  const int E = kind == TC_TF32 ? 4 : 8;
+  for (size_t i = 0; i < segs.size(); ++i) {
+    const int64_t kc = (segs[i].cols + E - 1) / E;
+    seg_chunk_begin[i + 1] = seg_chunk_begin[i] + kc * segs[i].rows;
+  }
+  nchunks = seg_chunk_begin.back();
+}
+
+ctn_status Packer::upload(cudaStream_t st) {
+  int dev = 0;
+  CTN_CUDA(cudaGetDevice(&dev));
+  if (d_mem && d_dev == dev) return CTN_OK;
+  if (d_mem) cudaFree(d_mem);
+  d_mem = nullptr;
+  const size_t bytes = segs.size() * sizeof(PackSeg) + seg_chunk_begin.size() * sizeof(int64_t) + 64;
+  CTN_CUDA(cudaMalloc(&d_mem, bytes));
+  d_dev = dev;
+  if (!segs.empty()) CTN_CUDA(cudaMemcpyAsync(d_mem, segs.data(), segs.size() * sizeof(PackSeg), cudaMemcpyHostToDevice, st));
+  CTN_CUDA(cudaMemcpyAsync((char *)d_mem + segs.size() * sizeof(PackSeg), seg_chunk_begin.data(),
+                           seg_chunk_begin.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+  CTN_CUDA(cudaStreamSynchronize(st));
+  return CTN_OK;
+}
+
+ctn_status Packer::run(const void *src, int src_is_f32, uint8_t *hi, uint8_t *lo, cudaStream_t st) {
+  if (nchunks == 0) return CTN_OK;
+  CTN_TRY(upload(st));
+  PackParams prm;
+  prm.segs = (const PackSeg *)d_mem;
+  prm.begin = (const int64_t *)((const char *)d_mem + segs.size() * sizeof(PackSeg));
+  prm.nseg = (int)segs.size();
+  prm.nchunks = nchunks;
+  prm.kind = kind;
+  prm.src_f32 = src_is_f32;
+  prm.src = src;
+  prm.hi = hi;
+  prm.lo = lo;
+  const int64_t grid = std::min<int64_t>((nchunks + 255) / 256, (int64_t)nsm_count() * 16);
+  k_pack<<<(unsigned)grid, 256, 0, st>>>(prm);
+  CTN_CHECK_LAUNCH();
+  return CTN_OK;
+}
+
+Packer::~Packer() {
+  if (d_mem) cudaFree(d_mem);
+}
+
+}  // namespace ctn
+
+// ------------------------------------------------------------------ dense split GEMM (C ABI)
+// C[M][N] (FP64, row-major) = A[M][K] * B[K][N] computed with the tcgen05 split kernel:
+// the packing, the tcgen05 GEMM and the FP64 epilogue in one call.  Workspace:
+// ctn_split_gemm_workspace_bytes.  Mostly a building block and a test vehicle.
+namespace {
+struct SplitDense {
+  ctn::TcGemm g;
+  ctn::Packer pa, pb;
+};
+int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+}  // namespace
+
+extern "C" size_t ctn_split_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K, int precision) {
+  const int kind = precision == CTN_PREC_BF16X3 ? ctn::TC_BF16 : ctn::TC_TF32;
+  const int ks = ctn::tc_k_per_slice(kind);
+  const int64_t kb = (K + ks - 1) / ks;
+  const int64_t a = round_up(M, 128) * kb * 128;
+  const int64_t b = round_up(N, 128) * kb * 128;
+  return (size_t)(2 * a + 2 * b + 256 + 64);
+}
+
+extern "C" ctn_status ctn_split_gemm_f64(int64_t M, int64_t N, int64_t K, const double *A, const double *B, double *C,
+                                         int precision, void *workspace, void *stream) {
+  CTN_REQUIRE(M > 0 && N > 0 && K > 0 && A && B && C && workspace, "ctn_split_gemm_f64: bad argument");
+  CTN_REQUIRE(precision == CTN_PREC_3XTF32 || precision == CTN_PREC_BF16X3, "ctn_split_gemm_f64: precision must be split");
+  CTN_REQUIRE(M < (1 << 30) && N < (1 << 30) && K < (1 << 30), "ctn_split_gemm_f64: too large");
+  cudaStream_t st = ctn::as_stream(stream);
+  SplitDense s;
+  const int kind = precision == CTN_PREC_BF16X3 ? ctn::TC_BF16 : ctn::TC_TF32;
+  s.g.kind = kind;
+  s.g.bn = 128;
+  s.pa.kind = s.pb.kind = kind;
+  std::vector<int64_t> rows(M);
+  for (int64_t r = 0; r < M; ++r) rows[r] = r * N;
+  s.g.rowmap = rows;
+  s.g.add_group((int)M, (int)N, (int)K, 1, 0, (int)N, 0);
+  s.g.finalize();
+  const ctn::TcGroup &g = s.g.groups[0];
+  ctn::PackSeg sa{0, K, 1, (int32_t)M, (int32_t)K, 0, 0, g.a_off, 128, g.kb};
+  ctn::PackSeg sb{0, 1, N, (int32_t)N, (int32_t)K, 0, 0, g.b_off, 128, g.kb};  // B^T rows = n, k stride N
+  s.pa.segs.push_back(sa);
+  s.pb.segs.push_back(sb);
+  s.pa.finalize();
+  s.pb.finalize();
+  uint8_t *ws = (uint8_t *)workspace;
+  uint8_t *a_hi = ws, *a_lo = a_hi + s.g.a_bytes, *b_hi = a_lo + s.g.a_bytes, *b_lo = b_hi + s.g.b_bytes;
+  int *err = (int *)(b_lo + s.g.b_bytes);
+  CTN_CUDA(cudaMemsetAsync(ws, 0, 2 * s.g.a_bytes + 2 * s.g.b_bytes + 64, st));
+  CTN_TRY(s.pa.run(A, 0, a_hi, a_lo, st));
+  CTN_TRY(s.pb.run(B, 0, b_hi, b_lo, st));
+  CTN_TRY(s.g.run(a_hi, a_lo, b_hi, b_lo, nullptr, C, err, st));
+  int herr = 0;
+  CTN_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CTN_CUDA(cudaStreamSynchronize(st));
+  if (herr) {
+    ctn::set_error("tcgen05 GEMM: a bounded wait expired (code %d)", herr);
+    return CTN_ERR_TIMEOUT;
+  }
+  return CTN_OK;
+}

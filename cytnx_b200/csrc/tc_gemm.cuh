@@ -1,0 +1,113 @@
+// Split-precision grouped GEMM on the 5th-generation tensor cores (tcgen05 + TMEM).
+//
+// Operands are stored "pre-tiled": every group's A (M x K) and B^T (N x K) matrices are
+// cut into tiles of 128 (A) or BN (B) rows by one 128-byte K slice (32 TF32 or 64 BF16
+// values), each tile laid out exactly as the UMMA K-major SWIZZLE_128B canonical layout
+// expects in shared memory (8-row x 128-byte atoms, 16-byte chunk index XOR row % 8).
+// A tile therefore moves global -> shared with ONE contiguous bulk copy (TMA engine,
+// cp.async.bulk + mbarrier complete_tx), no tensor map needed, for any block shape;
+// padding rows/columns are zeros written once.  Each operand is split into a "hi" and a
+// "lo" panel (x = hi + lo, both exactly representable in TF32 or BF16) and every K slice
+// issues three MMAs lo*hi + hi*lo + hi*hi into one FP32 TMEM accumulator.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "ctn_common.h"
+
+namespace ctn {
+
+constexpr int TC_BM = 128;            // UMMA M (rows of an A tile, TMEM lanes)
+constexpr int TC_ROW_BYTES = 128;     // one swizzle row = one K slice
+constexpr int TC_A_TILE = TC_BM * TC_ROW_BYTES;  // 16 KiB
+
+enum TcKind { TC_TF32 = 0, TC_BF16 = 1 };
+
+inline int tc_k_per_slice(int kind) { return kind == TC_TF32 ? 32 : 64; }
+inline int tc_elem_bytes(int kind) { return kind == TC_TF32 ? 4 : 2; }
+
+// One stacked GEMM: C[M][N] = A[M][K] * B[K][N] over pre-tiled panels.
+struct TcGroup {
+  int64_t a_off;      // byte offset of tile (0,0) in the A panels (hi and lo identical layout)
+  int64_t b_off;      // byte offset of tile (0,0) in the B panels
+  int32_t M, N, K;    // logical sizes
+  int32_t mt, nt, kb; // tile counts (128-row A tiles, BN-row B tiles, K slices)
+  int32_t mode;       // 0: C32[c_off + r*ldc + c] (FP32), 1: C64[rowmap[rm_off + r] + c] (FP64)
+  int32_t ldc;
+  int64_t c_off;
+  int64_t rm_off;
+};
+struct TcTile {
+  int32_t group, mt, nt, pad_;
+};
+
+struct TcParams {
+  const TcGroup *groups;
+  const TcTile *tiles;
+  int64_t ntiles;
+  const uint8_t *a_hi, *a_lo, *b_hi, *b_lo;
+  float *c32;
+  double *c64;
+  const int64_t *rowmap;
+  int *err;  // device error word: 0 ok, else the code of the wait that gave up
+};
+
+// byte offset of element (r, k) inside a panel of tiles with `rows` rows per tile
+// (tile index = (r / rows) * kb + k / kslice), K-major SWIZZLE_128B
+__host__ __device__ inline int64_t tc_panel_offset(int64_t r, int64_t k, int rows, int kb, int kind) {
+  const int ks = kind == TC_TF32 ? 32 : 64;
+  const int eb = kind == TC_TF32 ? 4 : 2;
+  const int64_t tile = (r / rows) * kb + k / ks;
+  const int rr = (int)(r % rows);
+  const int byte = (int)(k % ks) * eb;
+  const int chunk = (byte >> 4) ^ (rr & 7);
+  return tile * (int64_t)rows * TC_ROW_BYTES + (rr >> 3) * 1024 + (rr & 7) * 128 + chunk * 16 + (byte & 15);
+}
+
+// Host plan object for one grouped GEMM (device tables uploaded on first use).
+struct TcGemm {
+  int kind = TC_TF32;
+  int bn = 128;
+  std::vector<TcGroup> groups;
+  std::vector<TcTile> tiles;
+  std::vector<int64_t> rowmap;
+  int64_t a_bytes = 0, b_bytes = 0;  // panel sizes (one of hi/lo)
+  void *d_mem = nullptr;
+  int d_dev = -1;
+  double flops = 0.0;  // 2*M*N*K summed over groups (useful flops, one product)
+
+  // append a group; returns its index.  Panels are laid out back to back.
+  int add_group(int M, int N, int K, int mode, int64_t c_off, int ldc, int64_t rm_off);
+  void finalize();  // builds the tile list (largest K first)
+  ctn_status upload(cudaStream_t st);
+  ctn_status run(const uint8_t *a_hi, const uint8_t *a_lo, const uint8_t *b_hi, const uint8_t *b_lo, float *c32,
+                 double *c64, int *err, cudaStream_t st);
+  ~TcGemm();
+};
+
+// Pack segments: a source FP64 (or FP32) matrix region -> hi/lo panel tiles.
+struct PackSeg {
+  int64_t src_off;      // element offset of (0,0)
+  int64_t sr, sk;       // source strides of rows and of k
+  int32_t rows, cols;   // region size (cols = K extent)
+  int32_t row0, k0;     // destination row / k of (0,0) inside the group panel
+  int64_t panel_off;    // byte offset of the group's tile (0,0)
+  int32_t tile_rows;    // 128 (A) or BN (B)
+  int32_t kb;           // K slices of the group
+};
+
+struct Packer {
+  int kind = TC_TF32;
+  std::vector<PackSeg> segs;
+  std::vector<int64_t> seg_chunk_begin;  // prefix sums of 16-byte chunks per segment
+  int64_t nchunks = 0;
+  void *d_mem = nullptr;
+  int d_dev = -1;
+  void finalize();
+  ctn_status upload(cudaStream_t st);
+  // src is FP64 (src_is_f32 == 0) or FP32
+  ctn_status run(const void *src, int src_is_f32, uint8_t *hi, uint8_t *lo, cudaStream_t st);
+  ~Packer();
+};
+
+}  // namespace ctn

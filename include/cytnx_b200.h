@@ -146,7 +146,8 @@ void ctn_contract_plan_destroy(ctn_contract_plan *plan);
  * Each task: {c_off, m, n, ldc, pair_begin, pair_count}; a task with no pair
  * writes zeros.  Each pair: {a_off, b_off, k, lda, ldb, flags} with flags bit0:
  * A stored [k][m] (transposed), bit1: B stored [n][k].  Offsets are elements
- * from the A/B/C base pointers given at execution.  The plan copies the tables
+ * from the A/B/C base pointers given at execution; all pairs of one plan share the
+ * same flags (execution returns CTN_ERR_UNSUPPORTED otherwise).  The plan copies the tables
  * to the device on its first execution on a device (run that first call before
  * any stream capture). */
 typedef struct {
@@ -166,6 +167,16 @@ double ctn_gemm_grouped_plan_flops(const ctn_gemm_plan *plan);
 ctn_status ctn_gemm_grouped_f64(ctn_gemm_plan *plan, const double *A, const double *B, double *C,
                                 void *stream);
 void ctn_gemm_grouped_plan_destroy(ctn_gemm_plan *plan);
+
+/* ---------------------------------------------------------------- split-precision GEMM
+ * C[M][N] (FP64, row-major) = A[M][K] B[K][N] (FP64, row-major) on the tcgen05 tensor
+ * cores: operands split as x = hi + lo (TF32 for CTN_PREC_3XTF32, BF16 for
+ * CTN_PREC_BF16X3), products lo*hi + hi*lo + hi*hi accumulated in FP32 (TMEM).
+ * workspace >= ctn_split_gemm_workspace_bytes(M, N, K, precision) device bytes.
+ * Synchronises the stream (reads back the kernel's error word). */
+size_t ctn_split_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K, int precision);
+ctn_status ctn_split_gemm_f64(int64_t M, int64_t N, int64_t K, const double *A, const double *B, double *C,
+                              int precision, void *workspace, void *stream);
 
 /* ---------------------------------------------------------------- BLAS-1 (FP64)
  * Results of reductions land in device memory (out points to device doubles). */
@@ -204,13 +215,15 @@ ctn_status ctn_heff2_set_env(ctn_heff2_plan *plan, const double *L, const double
 ctn_status ctn_heff2_matvec(ctn_heff2_plan *plan, const double *psi, double *out, int precision,
                             void *stream);
 /* measurement aid: run `reps` matvecs with CUDA events between the phases on
- * `stream`; ms_out[0..2] receive the mean device time of step 1 (grouped GEMM),
- * steps 2+3 (MPO combination) and step 4 (grouped GEMM); launches_out the number
- * of kernel launches one matvec issues. */
+ * `stream`; ms_out[0..3] receive the mean device time of operand packing (split
+ * forms only, 0 for FP64), step 1 (grouped GEMM), steps 2+3 (MPO combination) and
+ * step 4 (grouped GEMM); launches_out the number of kernel launches one matvec issues. */
 ctn_status ctn_heff2_profile(ctn_heff2_plan *plan, const double *psi, double *out, int precision, int reps,
                              double *ms_out, int *launches_out, void *stream);
 /* flops of the planned grouped GEMM of step 1 or step 4 (2*m*n*k over its block pairs) */
 double ctn_heff2_gemm_flops(const ctn_heff2_plan *plan, int step);
+/* the same for the stacked tensor-core GEMMs of a split precision (one product counted) */
+double ctn_heff2_split_gemm_flops(ctn_heff2_plan *plan, int precision, int step);
 void ctn_heff2_plan_destroy(ctn_heff2_plan *plan);
 
 /* ---------------------------------------------------------------- Lanczos

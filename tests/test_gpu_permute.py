@@ -28,7 +28,7 @@ def test_all_24_perms_rank4_f64():
         assert np.array_equal(out.view(np.uint64), ref.view(np.uint64)), p
 
 
-@pytest.mark.parametrize("dtype", [np.float64, np.float32, np.int64, np.int32, np.int16, np.uint8,
+@pytest.mark.parametrize("dtype", [np.float64, np.float32, np.int64, np.int32, np.int16, np.uint16,
                                    np.complex128, np.complex64, np.bool_])
 def test_dtypes_bit_exact(dtype):
     rng = np.random.default_rng(1)
