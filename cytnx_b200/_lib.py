@@ -75,6 +75,7 @@ _SIGS = {
     "ctn_gemm_grouped_plan_destroy": (None, [c_vp]),
     "ctn_split_gemm_workspace_bytes": (c_size, [c_i64, c_i64, c_i64, c_int]),
     "ctn_split_gemm_f64": (c_int, [c_i64, c_i64, c_i64, c_vp, c_vp, c_vp, c_int, c_vp, c_vp]),
+    "ctn_split_gemm_f64_noalloc": (c_int, [c_i64, c_i64, c_i64, c_vp, c_vp, c_vp, c_int, c_vp]),
     "ctn_dot_f64": (c_int, [c_vp, c_vp, c_i64, c_vp, c_vp]),
     "ctn_nrm2_f64": (c_int, [c_vp, c_i64, c_vp, c_vp]),
     "ctn_axpy_f64": (c_int, [c_vp, c_vp, c_i64, c_vp, c_dbl, c_vp]),

@@ -460,6 +460,47 @@ ctn_status TcGemm::run(const uint8_t *a_hi, const uint8_t *a_lo, const uint8_t *
   return CTN_ERR_UNSUPPORTED;
 }
 
+ctn_status tc_launch_tables(int kind, int bn, const TcGroup *d_groups, const TcTile *d_tiles, int64_t ntiles,
+                            const int64_t *d_rowmap, const uint8_t *a_hi, const uint8_t *a_lo, const uint8_t *b_hi,
+                            const uint8_t *b_lo, float *c32, double *c64, int *err, cudaStream_t st) {
+  if (ntiles == 0) return CTN_OK;
+  TcParams prm;
+  prm.groups = d_groups;
+  prm.tiles = d_tiles;
+  prm.rowmap = d_rowmap;
+  prm.ntiles = ntiles;
+  prm.a_hi = a_hi;
+  prm.a_lo = a_lo;
+  prm.b_hi = b_hi;
+  prm.b_lo = b_lo;
+  prm.c32 = c32;
+  prm.c64 = c64;
+  prm.err = err;
+  if (kind == TC_TF32 && bn == 128) return launch_tc<TC_TF32, 128, 3>(prm, ntiles, st);
+  if (kind == TC_BF16 && bn == 128) return launch_tc<TC_BF16, 128, 3>(prm, ntiles, st);
+  set_error("tcgen05 GEMM: unsupported tile width %d", bn);
+  return CTN_ERR_UNSUPPORTED;
+}
+
+ctn_status pack_launch_tables(int kind, const PackSeg *d_segs, const int64_t *d_begin, int nseg, int64_t nchunks,
+                              const void *src, int src_is_f32, uint8_t *hi, uint8_t *lo, cudaStream_t st) {
+  if (nchunks == 0) return CTN_OK;
+  PackParams prm;
+  prm.segs = d_segs;
+  prm.begin = d_begin;
+  prm.nseg = nseg;
+  prm.nchunks = nchunks;
+  prm.kind = kind;
+  prm.src_f32 = src_is_f32;
+  prm.src = src;
+  prm.hi = hi;
+  prm.lo = lo;
+  const int64_t grid = std::min<int64_t>((nchunks + 255) / 256, (int64_t)nsm_count() * 16);
+  k_pack<<<(unsigned)grid, 256, 0, st>>>(prm);
+  CTN_CHECK_LAUNCH();
+  return CTN_OK;
+}
+
 TcGemm::~TcGemm() {
   if (d_mem) cudaFree(d_mem);
 }

@@ -110,4 +110,11 @@ struct Packer {
   ~Packer();
 };
 
+
+// Launch helpers over device-resident tables (the caller owns every buffer).
+ctn_status tc_launch_tables(int kind, int bn, const TcGroup *d_groups, const TcTile *d_tiles, int64_t ntiles,
+                            const int64_t *d_rowmap, const uint8_t *a_hi, const uint8_t *a_lo, const uint8_t *b_hi,
+                            const uint8_t *b_lo, float *c32, double *c64, int *err, cudaStream_t st);
+ctn_status pack_launch_tables(int kind, const PackSeg *d_segs, const int64_t *d_begin, int nseg, int64_t nchunks,
+                              const void *src, int src_is_f32, uint8_t *hi, uint8_t *lo, cudaStream_t st);
 }  // namespace ctn

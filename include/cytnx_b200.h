@@ -178,6 +178,18 @@ size_t ctn_split_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K, int preci
 ctn_status ctn_split_gemm_f64(int64_t M, int64_t N, int64_t K, const double *A, const double *B, double *C,
                               int precision, void *workspace, void *stream);
 
+/* Allocation-free form of ctn_split_gemm_f64 for callers that cannot allocate device
+ * memory (programs whose device memory is owned by their own pool, fixed memory
+ * budgets, foreign-language callers without a device allocator).  No counterpart in
+ * the reference.  Scratch lives in a 32 MiB static device array held by every GPU
+ * that loads the library until exit; problems needing more are rejected with
+ * CTN_ERR_INVALID.  The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress) and should come before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU race, so serialise them.  Synchronises
+ * the stream. */
+ctn_status ctn_split_gemm_f64_noalloc(int64_t M, int64_t N, int64_t K, const double *A, const double *B, double *C,
+                                      int precision, void *stream);
+
 /* ---------------------------------------------------------------- BLAS-1 (FP64)
  * Results of reductions land in device memory (out points to device doubles). */
 ctn_status ctn_dot_f64(const double *x, const double *y, int64_t n, double *out, void *stream);
