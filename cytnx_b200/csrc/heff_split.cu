@@ -40,8 +40,14 @@ struct MpoTermS {
   double coef;
 };
 
+struct WorkItem {
+  int32_t seg, pad_;
+  int64_t chunk0;
+};
+
 struct HeffSplit {
   int kind = TC_TF32;
+  std::vector<WorkItem> items;
   TcGemm g1, g4;
   Packer pk_L, pk_P, pk_R;
   std::vector<MpoSegS> segs;
@@ -76,58 +82,103 @@ __device__ __forceinline__ float to_tf32f(float x) {
 struct MpoSParams {
   const MpoSegS *segs;
   const MpoTermS *terms;
-  const int64_t *begin;
-  int nseg;
-  int64_t nchunks;
+  const WorkItem *items;
+  int64_t nitems;
   int kind;
   const float *x1;
   uint8_t *hi, *lo;
 };
 
-__global__ void __launch_bounds__(256) k_mpo_split(MpoSParams p) {
-  const int64_t step = (int64_t)gridDim.x * blockDim.x;
-  const int E = p.kind == TC_TF32 ? 4 : 8;
-  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < p.nchunks; c += step) {
-    int a = 0, b = p.nseg - 1;
-    while (a < b) {
-      const int mid = (a + b + 1) >> 1;
-      if (p.begin[mid] <= c) a = mid;
-      else b = mid - 1;
+constexpr int MPO_THREADS = 256;
+constexpr int MPO_UNROLL = 2;
+constexpr int MPO_ITEM = MPO_THREADS * MPO_UNROLL;  // chunks per work item
+constexpr int MPO_MAXT = 32;                        // terms staged in shared memory
+
+// round-to-nearest (ties away) to TF32 / round-to-nearest-even to BF16 with integer ops
+// (ALU pipe; the conversion unit is the bottleneck of a cvt-based version)
+__device__ __forceinline__ float tf32_rna(float x) {
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
+__device__ __forceinline__ uint32_t bf16_rne_bits(float x) {
+  const uint32_t u = __float_as_uint(x);
+  return (u + 0x7FFFu + ((u >> 16) & 1u)) >> 16;
+}
+
+// One CTA per work item (MPO_ITEM consecutive 16-byte chunks of one X3 block): the
+// block's term list is staged in shared memory once; every thread computes MPO_UNROLL
+// chunks in FP32 (X1 is FP32) and splits them into hi/lo panel chunks.
+__global__ void __launch_bounds__(MPO_THREADS) k_mpo_split(MpoSParams p) {
+  __shared__ MpoTermS sterm[MPO_MAXT];
+  __shared__ float scoef[MPO_MAXT];
+  const bool tf32 = p.kind == TC_TF32;
+  const int E = tf32 ? 4 : 8;
+  for (int64_t it = blockIdx.x; it < p.nitems; it += gridDim.x) {
+    const WorkItem wi = p.items[it];
+    const MpoSegS s = p.segs[wi.seg];
+    __syncthreads();
+    const int nt = s.term_count;
+    if (threadIdx.x < MPO_MAXT && threadIdx.x < nt) {
+      sterm[threadIdx.x] = p.terms[s.term_begin + threadIdx.x];
+      scoef[threadIdx.x] = (float)p.terms[s.term_begin + threadIdx.x].coef;
     }
-    const MpoSegS s = p.segs[a];
-    const int64_t cl = c - p.begin[a];
-    const int kc = (int)(cl % ((s.cols + E - 1) / E));  // k chunks fastest: contiguous X1 reads
-    const int r = (int)(cl / ((s.cols + E - 1) / E));
-    const int kloc = kc * E;
-    double x[8];
+    __syncthreads();
+    const int nkc = (s.cols + E - 1) / E;
+    const int total = s.rows * nkc;
 #pragma unroll
-    for (int e = 0; e < 8; ++e) x[e] = 0.0;
-    for (int t = 0; t < s.term_count; ++t) {
-      const MpoTermS tm = p.terms[s.term_begin + t];
-      const float *src = p.x1 + tm.x1_off + (int64_t)r * tm.ld + kloc;
+    for (int j = 0; j < MPO_UNROLL; ++j) {
+      const int cl = (int)wi.chunk0 + threadIdx.x + j * MPO_THREADS;
+      if (cl >= total) break;
+      const int r = cl / nkc;
+      const int kloc = (cl - r * nkc) * E;
+      const int nvalid = min(E, s.cols - kloc);
+      float x[8];
 #pragma unroll
-      for (int e = 0; e < 8; ++e)
-        if (e < E && kloc + e < s.cols) x[e] = fma(tm.coef, (double)src[e], x[e]);
-    }
-    const int64_t off = s.panel_off + tc_panel_offset(s.row0 + r, s.k0 + kloc, TC_BM, s.kb, p.kind);
-    if (p.kind == TC_TF32) {
-      float h[4], l[4];
+      for (int e = 0; e < 8; ++e) x[e] = 0.f;
+      for (int t = 0; t < nt; ++t) {
+        const MpoTermS tm = t < MPO_MAXT ? sterm[t] : p.terms[s.term_begin + t];
+        const float cf = t < MPO_MAXT ? scoef[t] : (float)tm.coef;
+        const float *src = p.x1 + tm.x1_off + (int64_t)r * tm.ld + kloc;
+        if (nvalid == E && tf32 && ((reinterpret_cast<uintptr_t>(src) & 15) == 0)) {
+          const float4 v = __ldg(reinterpret_cast<const float4 *>(src));
+          x[0] = fmaf(cf, v.x, x[0]);
+          x[1] = fmaf(cf, v.y, x[1]);
+          x[2] = fmaf(cf, v.z, x[2]);
+          x[3] = fmaf(cf, v.w, x[3]);
+        } else {
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        h[e] = to_tf32f((float)x[e]);
-        l[e] = to_tf32f((float)(x[e] - (double)h[e]));
+          for (int e = 0; e < 8; ++e)
+            if (e < nvalid) x[e] = fmaf(cf, __ldg(src + e), x[e]);
+        }
       }
-      *(float4 *)(p.hi + off) = make_float4(h[0], h[1], h[2], h[3]);
-      *(float4 *)(p.lo + off) = make_float4(l[0], l[1], l[2], l[3]);
-    } else {
-      __nv_bfloat16 h[8], l[8];
+      // panel offset (32-bit index math except the final byte offset)
+      const int row = s.row0 + r, kabs = s.k0 + kloc;
+      const int rr = row & (TC_BM - 1);
+      const int kslice = tf32 ? (kabs >> 5) : (kabs >> 6);
+      const int byte = tf32 ? ((kabs & 31) << 2) : ((kabs & 63) << 1);
+      const int64_t off = s.panel_off + ((int64_t)(row >> 7) * s.kb + kslice) * TC_A_TILE + (rr >> 3) * 1024 +
+                          (rr & 7) * 128 + (((byte >> 4) ^ (rr & 7)) << 4);
+      if (tf32) {
+        float h[4], l[4];
 #pragma unroll
-      for (int e = 0; e < 8; ++e) {
-        h[e] = __double2bfloat16(x[e]);
-        l[e] = __double2bfloat16(x[e] - (double)__bfloat162float(h[e]));
+        for (int e = 0; e < 4; ++e) {
+          h[e] = tf32_rna(x[e]);
+          l[e] = tf32_rna(x[e] - h[e]);  // exact in FP32
+        }
+        *(float4 *)(p.hi + off) = make_float4(h[0], h[1], h[2], h[3]);
+        *(float4 *)(p.lo + off) = make_float4(l[0], l[1], l[2], l[3]);
+      } else {
+        uint32_t hw[4], lw[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const uint32_t h0 = bf16_rne_bits(x[2 * e]), h1 = bf16_rne_bits(x[2 * e + 1]);
+          const uint32_t l0 = bf16_rne_bits(x[2 * e] - __uint_as_float(h0 << 16));
+          const uint32_t l1 = bf16_rne_bits(x[2 * e + 1] - __uint_as_float(h1 << 16));
+          hw[e] = h0 | (h1 << 16);
+          lw[e] = l0 | (l1 << 16);
+        }
+        *(uint4 *)(p.hi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+        *(uint4 *)(p.lo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
       }
-      *(uint4 *)(p.hi + off) = *(uint4 *)h;
-      *(uint4 *)(p.lo + off) = *(uint4 *)l;
     }
   }
 }
@@ -138,9 +189,10 @@ ctn_status heff_split_prepare(ctn_heff2_plan *p, int kind) {
   std::unique_ptr<HeffSplit> s(new HeffSplit());
   s->kind = kind;
   s->g1.kind = s->g4.kind = kind;
-  s->g1.bn = s->g4.bn = 128;
+  s->g1.bn = 128;
+  s->g4.bn = 128;
   s->pk_L.kind = s->pk_P.kind = s->pk_R.kind = kind;
-  const int bn = 128;
+  const int bn = s->g1.bn;
   // ---------------- step 1 groups: one per left sector a
   std::map<int64_t, std::vector<int64_t>> Lg, Pg;
   for (size_t l = 0; l < p->Lb.size(); ++l) Lg[p->Lb[l].q[1]].push_back((int64_t)l);
@@ -163,12 +215,13 @@ ctn_status heff_split_prepare(ctn_heff2_plan *p, int kind) {
       N += p->Pb[q].d[1] * p->Pb[q].d[2] * p->Pb[q].d[3];
     }
     if (M == 0 || N == 0 || K == 0) continue;
-    const int gi = s->g1.add_group((int)M, (int)N, (int)K, 0, x1, (int)N, 0);
+    const int64_t ldc = up(N, 4);  // FP32 rows start on 16-byte boundaries (TMA bulk stores)
+    const int gi = s->g1.add_group((int)M, (int)N, (int)K, 0, x1, (int)ldc, 0);
     for (int64_t l : kv.second) l_group[l] = gi;
     for (int64_t q : jt->second) p_group[q] = gi;
     g1_coff.push_back(x1);
-    g1_ldc.push_back(N);
-    x1 += M * N;
+    g1_ldc.push_back(ldc);
+    x1 += M * ldc;
   }
   s->x1_elems = x1;
   s->g1.finalize();
@@ -221,7 +274,7 @@ ctn_status heff_split_prepare(ctn_heff2_plan *p, int kind) {
     if (r_group[r] < 0) continue;
     const TcGroup &g = s->g4.groups[r_group[r]];
     const BlkInfo &b = p->Rb[r];  // [w2][b][b']: element (row b', k b) at off + k*d2 + row
-    PackSeg sg{b.off, 1, b.d[2], (int32_t)b.d[2], (int32_t)b.d[1], 0, (int32_t)r_k[r], g.b_off, bn, g.kb};
+    PackSeg sg{b.off, 1, b.d[2], (int32_t)b.d[2], (int32_t)b.d[1], 0, (int32_t)r_k[r], g.b_off, s->g4.bn, g.kb};
     s->pk_R.segs.push_back(sg);
   }
   s->pk_R.finalize();
@@ -267,6 +320,10 @@ ctn_status heff_split_prepare(ctn_heff2_plan *p, int kind) {
     s->seg_begin.push_back(s->seg_begin.back() + (int64_t)xi.rows * ((xi.cols + E - 1) / E));
   }
   s->nchunks = s->seg_begin.back();
+  for (size_t i = 0; i < s->segs.size(); ++i) {
+    const int64_t n = s->seg_begin[i + 1] - s->seg_begin[i];
+    for (int64_t c = 0; c < n; c += MPO_ITEM) s->items.push_back(WorkItem{(int32_t)i, 0, c});
+  }
   // ---------------- workspace layout
   int64_t o = 0;
   auto take = [&](int64_t bytes) {
@@ -313,7 +370,7 @@ ctn_status heff_split_set_env(ctn_heff2_plan *p, int kind, const double *L, cons
   if (!s->d_mpo || s->d_dev != dev) {
     if (s->d_mpo) cudaFree(s->d_mpo);
     const size_t bytes = s->segs.size() * sizeof(MpoSegS) + s->terms.size() * sizeof(MpoTermS) +
-                         s->seg_begin.size() * sizeof(int64_t) + 64;
+                         s->items.size() * sizeof(WorkItem) + 64;
     CTN_CUDA(cudaMalloc(&s->d_mpo, bytes));
     s->d_dev = dev;
     char *q = (char *)s->d_mpo;
@@ -321,7 +378,7 @@ ctn_status heff_split_set_env(ctn_heff2_plan *p, int kind, const double *L, cons
     q += s->segs.size() * sizeof(MpoSegS);
     if (!s->terms.empty()) CTN_CUDA(cudaMemcpyAsync(q, s->terms.data(), s->terms.size() * sizeof(MpoTermS), cudaMemcpyHostToDevice, st));
     q += s->terms.size() * sizeof(MpoTermS);
-    CTN_CUDA(cudaMemcpyAsync(q, s->seg_begin.data(), s->seg_begin.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    if (!s->items.empty()) CTN_CUDA(cudaMemcpyAsync(q, s->items.data(), s->items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, st));
     CTN_CUDA(cudaStreamSynchronize(st));
   }
   CTN_TRY(s->g1.upload(st));
@@ -345,14 +402,13 @@ ctn_status heff_split_matvec(ctn_heff2_plan *p, int kind, const double *psi, dou
   int *err = (int *)(w + s->o_err);
   CTN_TRY(s->g1.run(w + s->o_a1h, w + s->o_a1l, w + s->o_b1h, w + s->o_b1l, (float *)(w + s->o_x1), nullptr, err, st));
   if (ms4) CTN_CUDA(cudaEventRecord(ev[2], st));
-  if (s->nchunks) {
+  if (!s->items.empty()) {
     MpoSParams prm;
     const char *q = (const char *)s->d_mpo;
     prm.segs = (const MpoSegS *)q;
     prm.terms = (const MpoTermS *)(q + s->segs.size() * sizeof(MpoSegS));
-    prm.begin = (const int64_t *)(q + s->segs.size() * sizeof(MpoSegS) + s->terms.size() * sizeof(MpoTermS));
-    prm.nseg = (int)s->segs.size();
-    prm.nchunks = s->nchunks;
+    prm.items = (const WorkItem *)(q + s->segs.size() * sizeof(MpoSegS) + s->terms.size() * sizeof(MpoTermS));
+    prm.nitems = (int64_t)s->items.size();
     prm.kind = kind;
     prm.x1 = (const float *)(w + s->o_x1);
     prm.hi = w + s->o_a4h;
@@ -360,8 +416,8 @@ ctn_status heff_split_matvec(ctn_heff2_plan *p, int kind, const double *psi, dou
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const int64_t grid = std::min<int64_t>((s->nchunks + 255) / 256, (int64_t)nsm * 16);
-    k_mpo_split<<<(unsigned)grid, 256, 0, st>>>(prm);
+    const int64_t grid = std::min<int64_t>(prm.nitems, (int64_t)nsm * 8);
+    k_mpo_split<<<(unsigned)grid, MPO_THREADS, 0, st>>>(prm);
     CTN_CHECK_LAUNCH();
   }
   if (ms4) CTN_CUDA(cudaEventRecord(ev[3], st));

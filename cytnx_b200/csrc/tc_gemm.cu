@@ -65,6 +65,7 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
                : "memory");
 }
 
+
 __device__ __forceinline__ uint64_t smem_desc(const void *p) {
   const uint64_t a = smem_u32(p);
   return ((a & 0x3FFFFull) >> 4) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
@@ -107,7 +108,8 @@ struct TcSmem {
   static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
   static constexpr int RING = STAGES * STAGE_BYTES;
   static constexpr int BAR_OFF = RING;                 // full[S], empty[S], tfull[2], tempty[2], drain
-  static constexpr int TOTAL = RING + 8 * (2 * STAGES + 5) + 16;
+  static constexpr int BAR_BYTES = 8 * (2 * STAGES + 5) + 16;
+  static constexpr int TOTAL = RING + 256;
 };
 
 template <int KIND, int BN, int STAGES>
@@ -249,26 +251,46 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
       tc_fence_after();
       const int r = tl.mt * TC_BM + q * 32 + lane;
       const uint32_t base = tmem_base + (uint32_t)(acc * BN) + ((uint32_t)(q * 32) << 16);
-      const bool row_ok = r < g.M;
-      int64_t dst = 0;
-      if (row_ok) dst = g.mode == 0 ? g.c_off + (int64_t)r * g.ldc : p.rowmap[g.rm_off + r];
+      int64_t dst = -1;  // this lane's row start in the output (-1: row beyond M)
+      if (r < g.M) dst = g.mode == 0 ? g.c_off + (int64_t)r * g.ldc : p.rowmap[g.rm_off + r];
+      // Each lane owns one accumulator row (TMEM lane = row) and stores its 32-column
+      // pieces straight from registers with 16-byte vector stores (FP32 rows are padded to
+      // 16-byte boundaries; FP64 rows use 16-byte stores when aligned, 8-byte otherwise).
+      // A shared-memory transpose for coalesced row stores measured ~2x slower: its
+      // shuffle/ld.shared/st.global chains serialise the four epilogue warps.
 #pragma unroll 1
-      for (int c0 = 0; c0 < BN; c0 += 16) {
-        uint32_t v[16];
-        tmem_ld16(base + c0, v);
+      for (int c0 = 0; c0 < BN; c0 += 32) {
+        uint32_t v[32];
+        tmem_ld16(base + c0, *reinterpret_cast<uint32_t(*)[16]>(&v[0]));
+        tmem_ld16(base + c0 + 16, *reinterpret_cast<uint32_t(*)[16]>(&v[16]));
         tmem_wait_ld();
-        const int cg = tl.nt * BN + c0;
-        if (row_ok && cg < g.N) {
-          if (g.mode == 0) {
-            float *o = p.c32 + dst + cg;
+        const int cg0 = tl.nt * BN + c0;
+        if (cg0 >= g.N || dst < 0) continue;
+        const int ncol = min(32, g.N - cg0);
+        if (g.mode == 0) {
+          float *o = p.c32 + dst + cg0;
+          if (ncol == 32) {
 #pragma unroll
-            for (int i = 0; i < 16; ++i)
-              if (cg + i < g.N) o[i] = __uint_as_float(v[i]);
+            for (int j = 0; j < 8; ++j)
+              *reinterpret_cast<float4 *>(o + 4 * j) = make_float4(
+                  __uint_as_float(v[4 * j]), __uint_as_float(v[4 * j + 1]), __uint_as_float(v[4 * j + 2]),
+                  __uint_as_float(v[4 * j + 3]));
           } else {
-            double *o = p.c64 + dst + cg;
 #pragma unroll
-            for (int i = 0; i < 16; ++i)
-              if (cg + i < g.N) o[i] = (double)__uint_as_float(v[i]);
+            for (int e = 0; e < 32; ++e)
+              if (e < ncol) o[e] = __uint_as_float(v[e]);
+          }
+        } else {
+          double *o = p.c64 + dst + cg0;
+          if (ncol == 32 && ((reinterpret_cast<uintptr_t>(o) & 15) == 0)) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+              *reinterpret_cast<double2 *>(o + 2 * j) =
+                  make_double2((double)__uint_as_float(v[2 * j]), (double)__uint_as_float(v[2 * j + 1]));
+          } else {
+#pragma unroll
+            for (int e = 0; e < 32; ++e)
+              if (e < ncol) o[e] = (double)__uint_as_float(v[e]);
           }
         }
       }
@@ -347,6 +369,129 @@ __global__ void __launch_bounds__(256) k_pack(PackParams p) {
       for (int e = 0; e < 8; ++e) {
         h[e] = __double2bfloat16(x[e]);
         l[e] = __double2bfloat16(x[e] - (double)__bfloat162float(h[e]));
+      }
+      *(uint4 *)(p.hi + off) = *(uint4 *)h;
+      *(uint4 *)(p.lo + off) = *(uint4 *)l;
+    }
+  }
+}
+
+constexpr int PACK_THREADS = 256;
+constexpr int PACK_UNROLL = 4;
+constexpr int PACK_ITEM = PACK_THREADS * PACK_UNROLL;
+
+struct PackItemParams {
+  const PackSeg *segs;
+  const PackItem *items;
+  int64_t nitems;
+  int kind;
+  int src_f32;
+  const void *src;
+  uint8_t *hi, *lo;
+};
+
+// One CTA per work item of PACK_ITEM chunks of one segment; rows fastest, so the
+// source reads (rows are the contiguous axis of every operand packed here) coalesce.
+__global__ void __launch_bounds__(PACK_THREADS) k_pack_items(PackItemParams p) {
+  const int E = p.kind == TC_TF32 ? 4 : 8;
+  for (int64_t it = blockIdx.x; it < p.nitems; it += gridDim.x) {
+    const PackItem wi = p.items[it];
+    const PackSeg s = p.segs[wi.seg];
+    const int64_t total = (int64_t)s.rows * ((s.cols + E - 1) / E);
+#pragma unroll
+    for (int j = 0; j < PACK_UNROLL; ++j) {
+      const int64_t cl = wi.chunk0 + threadIdx.x + j * PACK_THREADS;
+      if (cl >= total) break;
+      const int r = (int)(cl % s.rows);
+      const int kloc = (int)(cl / s.rows) * E;
+      double x[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        x[e] = 0.0;
+        if (e < E && kloc + e < s.cols) {
+          const int64_t idx = s.src_off + (int64_t)r * s.sr + (int64_t)(kloc + e) * s.sk;
+          x[e] = p.src_f32 ? (double)__ldg((const float *)p.src + idx) : __ldg((const double *)p.src + idx);
+        }
+      }
+      const int64_t off = s.panel_off + tc_panel_offset(s.row0 + r, s.k0 + kloc, s.tile_rows, s.kb, p.kind);
+      if (p.kind == TC_TF32) {
+        float h[4], l[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          h[e] = to_tf32((float)x[e]);
+          l[e] = to_tf32((float)(x[e] - (double)h[e]));
+        }
+        *(float4 *)(p.hi + off) = make_float4(h[0], h[1], h[2], h[3]);
+        *(float4 *)(p.lo + off) = make_float4(l[0], l[1], l[2], l[3]);
+      } else {
+        __nv_bfloat16 h[8], l[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          h[e] = __double2bfloat16(x[e]);
+          l[e] = __double2bfloat16(x[e] - (double)__bfloat162float(h[e]));
+        }
+        *(uint4 *)(p.hi + off) = *(uint4 *)h;
+        *(uint4 *)(p.lo + off) = *(uint4 *)l;
+      }
+    }
+  }
+}
+
+// Transposing pack for segments whose rows are the contiguous source axis (sr == 1):
+// a CTA loads a 32-row x 32-k (TF32) or 32 x 64 (BF16) tile with coalesced reads along
+// the rows into shared memory, then each thread writes one 16-byte chunk with the 8
+// chunks of a panel row on 8 consecutive threads (whole 128-byte rows per 8 threads).
+using PackTileItem = PackTileItemH;  // rows r0..r0+31, local k chunks kc0..kc0+7
+struct PackTileParams {
+  const PackSeg *segs;
+  const PackTileItem *items;
+  int64_t nitems;
+  int kind;
+  int src_f32;
+  const void *src;
+  uint8_t *hi, *lo;
+};
+
+__global__ void __launch_bounds__(256) k_pack_tile(PackTileParams p) {
+  __shared__ double T[64][33];
+  const int E = p.kind == TC_TF32 ? 4 : 8;
+  const int KT = 8 * E;  // k values per item: 8 chunks
+  for (int64_t it = blockIdx.x; it < p.nitems; it += gridDim.x) {
+    const PackTileItem wi = p.items[it];
+    const PackSeg s = p.segs[wi.seg];
+    const int k0 = wi.kc0 * E;
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < 32 * KT; idx += 256) {
+      const int r = idx & 31, k = idx >> 5;
+      double v = 0.0;
+      if (wi.r0 + r < s.rows && k0 + k < s.cols) {
+        const int64_t src = s.src_off + (int64_t)(wi.r0 + r) * s.sr + (int64_t)(k0 + k) * s.sk;
+        v = p.src_f32 ? (double)__ldg((const float *)p.src + src) : __ldg((const double *)p.src + src);
+      }
+      T[k][r] = v;
+    }
+    __syncthreads();
+    const int r = threadIdx.x >> 3, c = threadIdx.x & 7;
+    const int kl = k0 + c * E;  // local k of this chunk
+    if (wi.r0 + r >= s.rows || kl >= s.cols) continue;
+    const int64_t off = s.panel_off + tc_panel_offset(s.row0 + wi.r0 + r, s.k0 + kl, s.tile_rows, s.kb, p.kind);
+    if (p.kind == TC_TF32) {
+      float h[4], l[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const double x = T[c * 4 + e][r];
+        h[e] = to_tf32((float)x);
+        l[e] = to_tf32((float)(x - (double)h[e]));
+      }
+      *(float4 *)(p.hi + off) = make_float4(h[0], h[1], h[2], h[3]);
+      *(float4 *)(p.lo + off) = make_float4(l[0], l[1], l[2], l[3]);
+    } else {
+      __nv_bfloat16 h[8], l[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const double x = T[c * 8 + e][r];
+        h[e] = __double2bfloat16(x);
+        l[e] = __double2bfloat16(x - (double)__bfloat162float(h[e]));
       }
       *(uint4 *)(p.hi + off) = *(uint4 *)h;
       *(uint4 *)(p.lo + off) = *(uint4 *)l;
@@ -513,6 +658,21 @@ void Packer::finalize() {
     seg_chunk_begin[i + 1] = seg_chunk_begin[i] + kc * segs[i].rows;
   }
   nchunks = seg_chunk_begin.back();
+  items.clear();
+  for (size_t i = 0; i < segs.size(); ++i) {
+    const int64_t n = seg_chunk_begin[i + 1] - seg_chunk_begin[i];
+    for (int64_t c = 0; c < n; c += PACK_ITEM) items.push_back(PackItem{(int32_t)i, 0, c});
+  }
+  tile_items.clear();
+  transposing = !segs.empty();
+  for (const auto &sg : segs) transposing &= (sg.sr == 1);
+  if (transposing) {
+    for (size_t i = 0; i < segs.size(); ++i) {
+      const int nkc = (segs[i].cols + E - 1) / E;
+      for (int r0 = 0; r0 < segs[i].rows; r0 += 32)
+        for (int kc = 0; kc < nkc; kc += 8) tile_items.push_back(PackTileItemH{(int32_t)i, r0, kc, 0});
+    }
+  }
 }
 
 ctn_status Packer::upload(cudaStream_t st) {
@@ -521,12 +681,17 @@ ctn_status Packer::upload(cudaStream_t st) {
   if (d_mem && d_dev == dev) return CTN_OK;
   if (d_mem) cudaFree(d_mem);
   d_mem = nullptr;
-  const size_t bytes = segs.size() * sizeof(PackSeg) + seg_chunk_begin.size() * sizeof(int64_t) + 64;
+  const size_t bytes = segs.size() * sizeof(PackSeg) + items.size() * sizeof(PackItem) +
+                       tile_items.size() * sizeof(PackTileItem) + 64;
   CTN_CUDA(cudaMalloc(&d_mem, bytes));
   d_dev = dev;
   if (!segs.empty()) CTN_CUDA(cudaMemcpyAsync(d_mem, segs.data(), segs.size() * sizeof(PackSeg), cudaMemcpyHostToDevice, st));
-  CTN_CUDA(cudaMemcpyAsync((char *)d_mem + segs.size() * sizeof(PackSeg), seg_chunk_begin.data(),
-                           seg_chunk_begin.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+  if (!items.empty())
+    CTN_CUDA(cudaMemcpyAsync((char *)d_mem + segs.size() * sizeof(PackSeg), items.data(), items.size() * sizeof(PackItem),
+                             cudaMemcpyHostToDevice, st));
+  if (!tile_items.empty())
+    CTN_CUDA(cudaMemcpyAsync((char *)d_mem + segs.size() * sizeof(PackSeg) + items.size() * sizeof(PackItem),
+                             tile_items.data(), tile_items.size() * sizeof(PackTileItem), cudaMemcpyHostToDevice, st));
   CTN_CUDA(cudaStreamSynchronize(st));
   return CTN_OK;
 }
@@ -534,18 +699,32 @@ ctn_status Packer::upload(cudaStream_t st) {
 ctn_status Packer::run(const void *src, int src_is_f32, uint8_t *hi, uint8_t *lo, cudaStream_t st) {
   if (nchunks == 0) return CTN_OK;
   CTN_TRY(upload(st));
-  PackParams prm;
+  if (transposing) {
+    PackTileParams tp;
+    tp.segs = (const PackSeg *)d_mem;
+    tp.items = (const PackTileItem *)((const char *)d_mem + segs.size() * sizeof(PackSeg) + items.size() * sizeof(PackItem));
+    tp.nitems = (int64_t)tile_items.size();
+    tp.kind = kind;
+    tp.src_f32 = src_is_f32;
+    tp.src = src;
+    tp.hi = hi;
+    tp.lo = lo;
+    const int64_t g2 = std::min<int64_t>(tp.nitems, (int64_t)nsm_count() * 8);
+    k_pack_tile<<<(unsigned)g2, 256, 0, st>>>(tp);
+    CTN_CHECK_LAUNCH();
+    return CTN_OK;
+  }
+  PackItemParams prm;
   prm.segs = (const PackSeg *)d_mem;
-  prm.begin = (const int64_t *)((const char *)d_mem + segs.size() * sizeof(PackSeg));
-  prm.nseg = (int)segs.size();
-  prm.nchunks = nchunks;
+  prm.items = (const PackItem *)((const char *)d_mem + segs.size() * sizeof(PackSeg));
+  prm.nitems = (int64_t)items.size();
   prm.kind = kind;
   prm.src_f32 = src_is_f32;
   prm.src = src;
   prm.hi = hi;
   prm.lo = lo;
-  const int64_t grid = std::min<int64_t>((nchunks + 255) / 256, (int64_t)nsm_count() * 16);
-  k_pack<<<(unsigned)grid, 256, 0, st>>>(prm);
+  const int64_t grid = std::min<int64_t>(prm.nitems, (int64_t)nsm_count() * 8);
+  k_pack_items<<<(unsigned)grid, PACK_THREADS, 0, st>>>(prm);
   CTN_CHECK_LAUNCH();
   return CTN_OK;
 }

@@ -96,10 +96,22 @@ struct PackSeg {
   int32_t kb;           // K slices of the group
 };
 
+struct PackItem {
+  int32_t seg, pad_;
+  int64_t chunk0;  // first chunk of this CTA work item inside the segment
+};
+
+struct PackTileItemH {
+  int32_t seg, r0, kc0, pad_;
+};
+
 struct Packer {
   int kind = TC_TF32;
+  std::vector<struct PackTileItemH> tile_items;  // transposing work items (all segments row-contiguous)
+  bool transposing = false;
   std::vector<PackSeg> segs;
   std::vector<int64_t> seg_chunk_begin;  // prefix sums of 16-byte chunks per segment
+  std::vector<PackItem> items;           // CTA work items (one segment each, no search on device)
   int64_t nchunks = 0;
   void *d_mem = nullptr;
   int d_dev = -1;
