@@ -44,7 +44,7 @@ def parse():
     ap.add_argument("--D", type=int, default=4096)
     ap.add_argument("--lanczos-iters", type=int, default=40)
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
-    ap.add_argument("--precision", default="3xtf32", help="headline arithmetic form: 3xtf32, bf16x3 or fp64")
+    ap.add_argument("--precision", default="bf16x3", help="headline arithmetic form: bf16x3, 3xtf32 or fp64")
     return ap.parse_args()
 
 
@@ -203,8 +203,9 @@ def main():
     psi, L, M1, M2, R = W.build_two_site(spec, mpo_vals, seed=0, device=local)
     H = c.TwoSiteHeff(L, M1, M2, R, psi, precision=args.precision)
     flops = H.algorithmic_flops()
+    tiles = {f: H.autotune(f) for f in ("bf16x3", "3xtf32")}
     x = psi.flat_view()
-    forms = [args.precision] + (["fp64"] if args.precision != "fp64" else [])
+    forms = [args.precision] + [f for f in ("3xtf32", "bf16x3", "fp64") if f != args.precision]
 
     def timed_matvecs(form, steps, sampler=None):
         y = torch.empty_like(x)
@@ -250,10 +251,12 @@ def main():
     value = head["tflops"]
 
     # matvec error of the split form against the FP64 form (same input)
-    mv_err = None
-    if args.precision != "fp64":
-        y64 = results["fp64"]["y"]
-        mv_err = float((torch.linalg.vector_norm(head["y"] - y64) / torch.linalg.vector_norm(y64)).item())
+    y64 = results["fp64"]["y"]
+    errs = {f: float((torch.linalg.vector_norm(r["y"] - y64) / torch.linalg.vector_norm(y64)).item())
+            for f, r in results.items() if f != "fp64"}
+    for f, e in errs.items():
+        results[f]["matvec_rel_err_vs_fp64"] = e
+    mv_err = errs.get(args.precision)
 
     # ---- end to end through the public API (pinned host psi in, host H psi out), headline form
     H.bind(args.precision)
@@ -290,15 +293,17 @@ def main():
         torch.cuda.synchronize()
         lanczos[form] = {"energy": E, "iters": it, "s_per_step": (time.perf_counter() - t0) / max(it, 1)}
         vecs[form] = vec.flat_view()
-    if args.precision != "fp64":
-        v = vecs[args.precision]
+    e64 = lanczos["fp64"]["energy"]
+    for form in forms:
+        if form == "fp64":
+            continue
+        v = vecs[form]
         hv = torch.empty_like(v)
         H.apply_flat(v, hv, "fp64")
         e_ref = float((torch.dot(v, hv) / torch.dot(v, v)).item())
-        e64 = lanczos["fp64"]["energy"]
-        lanczos["refined_energy"] = e_ref
-        lanczos["dE_rel_raw"] = abs(lanczos[args.precision]["energy"] - e64) / abs(e64)
-        lanczos["dE_rel_refined"] = abs(e_ref - e64) / abs(e64)
+        lanczos[form]["refined_energy"] = e_ref
+        lanczos[form]["dE_rel_raw"] = abs(lanczos[form]["energy"] - e64) / abs(e64)
+        lanczos[form]["dE_rel_refined"] = abs(e_ref - e64) / abs(e64)
 
     # ---- peaks for the roofline denominators (cuBLAS, best of 5)
     def gemm_peak(dtype, tf32=False):
@@ -357,8 +362,9 @@ def main():
             "dtype": args.precision, "data": "synthetic (seeded numpy PCG64)",
             "config": dict(config_base, parallelism=f"replicas{world}", precision=args.precision),
             "algorithmic_flops_per_matvec": flops,
+            "autotuned_tiles": tiles,
             "forms": forms_out,
-            "speedup_vs_fp64": (results["fp64"]["ms_per_matvec"] / head["ms_per_matvec"]) if "fp64" in results else 1.0,
+            "speedup_vs_fp64": results["fp64"]["ms_per_matvec"] / head["ms_per_matvec"],
             "matvec_rel_err_vs_fp64": mv_err,
             "lanczos": lanczos,
             "lanczos_s_per_step": lanczos[args.precision]["s_per_step"],

@@ -79,6 +79,7 @@ struct ctn_heff2_plan {
   std::vector<ctn::X3Info> x3;
   // split-precision state per kind (0: 3xTF32, 1: BF16x3)
   ctn::HeffSplit *split[2] = {nullptr, nullptr};
+  int split_bn[2][2] = {{128, 128}, {128, 128}};  // tile widths of steps 1 and 4 per split kind
   bool split_bound[2] = {false, false};
   ~ctn_heff2_plan() {
     for (auto *s : split) ctn::heff_split_free(s);

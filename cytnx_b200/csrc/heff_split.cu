@@ -189,8 +189,8 @@ ctn_status heff_split_prepare(ctn_heff2_plan *p, int kind) {
   std::unique_ptr<HeffSplit> s(new HeffSplit());
   s->kind = kind;
   s->g1.kind = s->g4.kind = kind;
-  s->g1.bn = 128;
-  s->g4.bn = 128;
+  s->g1.bn = p->split_bn[kind][0];
+  s->g4.bn = p->split_bn[kind][1];
   s->pk_L.kind = s->pk_P.kind = s->pk_R.kind = kind;
   const int bn = s->g1.bn;
   // ---------------- step 1 groups: one per left sector a

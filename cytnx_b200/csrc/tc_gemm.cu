@@ -125,7 +125,8 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
   uint32_t *tmem_holder = (uint32_t *)(drain + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  constexpr uint32_t TMEM_COLS = 2 * BN;  // two accumulator buffers (power of two: 256 or 512)
+  // two accumulator buffers; the allocation is a power of two >= 32 columns
+  constexpr uint32_t TMEM_COLS = 2 * BN <= 64 ? 64 : 2 * BN <= 128 ? 128 : 2 * BN <= 256 ? 256 : 512;
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full[s], 1);
@@ -266,7 +267,7 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
         tmem_wait_ld();
         const int cg0 = tl.nt * BN + c0;
         if (cg0 >= g.N || dst < 0) continue;
-        const int ncol = min(32, g.N - cg0);
+        const int ncol = min(min(32, BN - c0), g.N - cg0);  // a 32-column piece may pass the tile edge
         if (g.mode == 0) {
           float *o = p.c32 + dst + cg0;
           if (ncol == 32) {
@@ -523,7 +524,31 @@ ctn_status launch_tc(const TcParams &prm, int64_t ntiles, cudaStream_t st) {
   return CTN_OK;
 }
 
+// tile widths compiled (UMMA M=128 allows N = 16..256 in steps of 16); the ring depth is
+// the largest that fits next to 2 x 16 KiB A tiles and 2 x BN x 128 B B tiles per stage
+template <int KIND>
+ctn_status launch_tc_kind(int bn, const TcParams &prm, cudaStream_t st) {
+  switch (bn) {
+    case 64: return launch_tc<KIND, 64, 4>(prm, prm.ntiles, st);
+    case 96: return launch_tc<KIND, 96, 3>(prm, prm.ntiles, st);
+    case 128: return launch_tc<KIND, 128, 3>(prm, prm.ntiles, st);
+    case 144: return launch_tc<KIND, 144, 3>(prm, prm.ntiles, st);
+    case 160: return launch_tc<KIND, 160, 3>(prm, prm.ntiles, st);
+    case 192: return launch_tc<KIND, 192, 2>(prm, prm.ntiles, st);
+    case 256: return launch_tc<KIND, 256, 2>(prm, prm.ntiles, st);
+  }
+  set_error("tcgen05 GEMM: unsupported tile width %d (64, 96, 128, 144, 160, 192, 256)", bn);
+  return CTN_ERR_UNSUPPORTED;
+}
+ctn_status launch_tc_any(int kind, int bn, const TcParams &prm, cudaStream_t st) {
+  return kind == TC_TF32 ? launch_tc_kind<TC_TF32>(bn, prm, st) : launch_tc_kind<TC_BF16>(bn, prm, st);
+}
+
 }  // namespace
+
+bool tc_tile_width_supported(int bn) {
+  return bn == 64 || bn == 96 || bn == 128 || bn == 144 || bn == 160 || bn == 192 || bn == 256;
+}
 
 int TcGemm::add_group(int M, int N, int K, int mode, int64_t c_off, int ldc, int64_t rm_off) {
   TcGroup g;
@@ -597,12 +622,7 @@ ctn_status TcGemm::run(const uint8_t *a_hi, const uint8_t *a_lo, const uint8_t *
   prm.c32 = c32;
   prm.c64 = c64;
   prm.err = err;
-  if (kind == TC_TF32 && bn == 128) return launch_tc<TC_TF32, 128, 3>(prm, prm.ntiles, st);
-  if (kind == TC_BF16 && bn == 128) return launch_tc<TC_BF16, 128, 3>(prm, prm.ntiles, st);
-  if (kind == TC_TF32 && bn == 256) return launch_tc<TC_TF32, 256, 2>(prm, prm.ntiles, st);
-  if (kind == TC_BF16 && bn == 256) return launch_tc<TC_BF16, 256, 2>(prm, prm.ntiles, st);
-  set_error("tcgen05 GEMM: unsupported tile width %d", bn);
-  return CTN_ERR_UNSUPPORTED;
+  return launch_tc_any(kind, bn, prm, st);
 }
 
 ctn_status tc_launch_tables(int kind, int bn, const TcGroup *d_groups, const TcTile *d_tiles, int64_t ntiles,
@@ -621,10 +641,7 @@ ctn_status tc_launch_tables(int kind, int bn, const TcGroup *d_groups, const TcT
   prm.c32 = c32;
   prm.c64 = c64;
   prm.err = err;
-  if (kind == TC_TF32 && bn == 128) return launch_tc<TC_TF32, 128, 3>(prm, ntiles, st);
-  if (kind == TC_BF16 && bn == 128) return launch_tc<TC_BF16, 128, 3>(prm, ntiles, st);
-  set_error("tcgen05 GEMM: unsupported tile width %d", bn);
-  return CTN_ERR_UNSUPPORTED;
+  return launch_tc_any(kind, bn, prm, st);
 }
 
 ctn_status pack_launch_tables(int kind, const PackSeg *d_segs, const int64_t *d_begin, int nseg, int64_t nchunks,

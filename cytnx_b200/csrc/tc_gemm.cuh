@@ -123,6 +123,8 @@ struct Packer {
 };
 
 
+bool tc_tile_width_supported(int bn);
+
 // Launch helpers over device-resident tables (the caller owns every buffer).
 ctn_status tc_launch_tables(int kind, int bn, const TcGroup *d_groups, const TcTile *d_tiles, int64_t ntiles,
                             const int64_t *d_rowmap, const uint8_t *a_hi, const uint8_t *a_lo, const uint8_t *b_hi,

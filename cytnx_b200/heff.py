@@ -65,7 +65,7 @@ class TwoSiteHeff(LinOp):
         self.n = int(_lib.lib().ctn_heff2_psi_elems(self._h))
         self.plan_flops = float(_lib.lib().ctn_heff2_flops(self._h))
         self._ws = {}
-        self._bound = None
+        self._bound = set()  # precisions whose environments are bound (each has its own workspace)
         self.precision = precision
         self._algo_flops = None
 
@@ -78,7 +78,7 @@ class TwoSiteHeff(LinOp):
     # ---------------------------------------------------------------- binding
     def bind(self, precision: Optional[str] = None) -> None:
         prec = _lib.PRECISIONS[(precision or self.precision).lower()]
-        if self._bound == prec:
+        if prec in self._bound:
             return
         nbytes = int(_lib.lib().ctn_heff2_workspace_bytes(self._h, prec))
         ws = self._ws.get(prec)
@@ -87,7 +87,7 @@ class TwoSiteHeff(LinOp):
             self._ws[prec] = ws
         _lib.check(_lib.lib().ctn_heff2_set_env(self._h, self.L._data.data_ptr(), self.R._data.data_ptr(),
                                                 ws.data_ptr(), prec, _lib.stream_ptr()), "TwoSiteHeff.set_env")
-        self._bound = prec
+        self._bound.add(prec)
 
     # ---------------------------------------------------------------- matvec
     def apply_flat(self, x: torch.Tensor, y: torch.Tensor, precision: Optional[str] = None) -> None:
@@ -105,6 +105,50 @@ class TwoSiteHeff(LinOp):
         self.apply_flat(x, y)
         out = UniTensor._new_block(self.out_bonds, lbl, v.rowrank(), self.out_layout, [0, 1, 2, 3], y)
         return out
+
+    # ---------------------------------------------------------------- tile autotuner
+    def set_tiles(self, bn_step1: int, bn_step4: int, precision: Optional[str] = None) -> None:
+        prec = _lib.PRECISIONS[(precision or self.precision).lower()]
+        _lib.check(_lib.lib().ctn_heff2_set_tiles(self._h, prec, int(bn_step1), int(bn_step4)), "set_tiles")
+        self._ws.pop(prec, None)
+        self._bound.discard(prec)
+
+    def autotune(self, precision: Optional[str] = None, step1=(128, 160, 192, 256), step4=(96, 128, 144, 160, 256),
+                 reps: int = 5) -> dict:
+        """Pick the tensor-core tile widths of steps 1 and 4 by timing them on this plan.
+
+        The two GEMMs are independent kernels, so each is tuned with the other fixed:
+        every candidate re-packs the operand panels (they depend on the width), runs
+        the matvec and reads the per-phase CUDA-event times (ctn_heff2_profile)."""
+        import ctypes as ct
+
+        precision = (precision or self.precision).lower()
+        if precision not in ("3xtf32", "bf16x3"):
+            return {}
+        prec = _lib.PRECISIONS[precision]
+        x = self.psi_t.flat_view()
+        y = torch.empty_like(x)
+
+        def phase_ms(b1, b4):
+            self.set_tiles(b1, b4, precision)
+            self.bind(precision)
+            ms = (ct.c_double * 4)()
+            nl = ct.c_int()
+            _lib.check(_lib.lib().ctn_heff2_profile(self._h, x.data_ptr(), y.data_ptr(), prec, reps, ms, ct.byref(nl),
+                                                   _lib.stream_ptr()), "autotune")
+            return [ms[i] for i in range(4)]
+
+        table = {"step1": {}, "step4": {}}
+        b4_fixed = 128
+        for b1 in step1:
+            table["step1"][b1] = phase_ms(b1, b4_fixed)[1]
+        best1 = min(table["step1"], key=table["step1"].get)
+        for b4 in step4:
+            table["step4"][b4] = phase_ms(best1, b4)[3]
+        best4 = min(table["step4"], key=table["step4"].get)
+        self.set_tiles(best1, best4, precision)
+        self.bind(precision)
+        return {"step1": best1, "step4": best4, "ms_step1": table["step1"], "ms_step4": table["step4"]}
 
     # ---------------------------------------------------------------- Lanczos without Python callbacks
     def lanczos(self, psi0: UniTensor, maxiter: int = 40, cvgcrit: float = 1e-14,

@@ -237,6 +237,11 @@ double ctn_heff2_gemm_flops(const ctn_heff2_plan *plan, int step);
 /* the same for the stacked tensor-core GEMMs of a split precision (one product counted) */
 double ctn_heff2_split_gemm_flops(ctn_heff2_plan *plan, int precision, int step);
 void ctn_heff2_plan_destroy(ctn_heff2_plan *plan);
+/* tile widths (N of the UMMA tiles: 64, 96, 128, 144, 160, 192 or 256) of the step-1 and
+ * step-4 tensor-core GEMMs of a split precision; drops that precision's binding (the
+ * operand panels depend on the widths), so call ctn_heff2_set_env again.  Used by the
+ * autotuner (TwoSiteHeff.autotune). */
+ctn_status ctn_heff2_set_tiles(ctn_heff2_plan *plan, int precision, int bn_step1, int bn_step4);
 
 /* ---------------------------------------------------------------- Lanczos
  * Ground state by the Lanczos_Gnd_Ut recurrence on flat FP64 device vectors.

@@ -79,3 +79,20 @@ def test_heff_split_random_vectors_linear():
     H.apply_flat(x + y, hz, "3xtf32")
     lin = (torch.linalg.vector_norm(hz - hx - hy) / torch.linalg.vector_norm(hz)).item()
     assert lin < 1e-5
+
+
+@pytest.mark.parametrize("prec", ["3xtf32", "bf16x3"])
+def test_heff_split_tile_widths_agree(prec):
+    """Every compiled tile width gives the same matvec (to the split tolerance)."""
+    psi, H = _heff(512, seed=8)
+    x = psi.flat_view()
+    y64 = torch.empty_like(x)
+    H.apply_flat(x, y64, "fp64")
+    for b1, b4 in [(64, 96), (128, 144), (160, 160), (192, 256), (256, 64)]:
+        H.set_tiles(b1, b4, prec)
+        y = torch.empty_like(x)
+        H.apply_flat(x, y, prec)
+        err = (torch.linalg.vector_norm(y - y64) / torch.linalg.vector_norm(y64)).item()
+        assert err < (1e-5 if prec == "3xtf32" else 2e-3), (b1, b4, err)
+    tuned = H.autotune(prec, reps=2)
+    assert tuned["step1"] in (128, 160, 192, 256) and tuned["step4"] in (96, 128, 144, 160, 256)
