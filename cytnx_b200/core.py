@@ -427,6 +427,18 @@ class Tensor:
         out._storage = self._storage.to(Type.to_torch(dtype))
         return out
 
+    def __getitem__(self, key):
+        return Tensor.from_torch(self.to_torch()[key])
+
+    def __setitem__(self, key, value):
+        """Element/slice assignment on the logical tensor (writes through to storage)."""
+        if not self._contiguous:
+            self.contiguous_()
+        view = self._storage.view(*self._shape) if self._shape else self._storage.view(())
+        if isinstance(value, Tensor):
+            value = value.to_torch()
+        view[key] = value
+
     def item(self):
         if self._storage.numel() != 1:
             raise CytnxError("[ERROR] item() requires a tensor with exactly one element")

@@ -72,7 +72,20 @@ def layout_for(bonds: Sequence[Bond]) -> BlockLayout:
     return lay
 
 
-_PLANS: Dict[tuple, object] = {}
+class _LRU(dict):
+    """Plan cache bounded to `cap` entries (least recently inserted evicted first)."""
+
+    def __init__(self, cap: int):
+        super().__init__()
+        self.cap = cap
+
+    def __setitem__(self, k, v):
+        if k not in self and len(self) >= self.cap:
+            del self[next(iter(self))]
+        super().__setitem__(k, v)
+
+
+_PLANS: Dict[tuple, object] = _LRU(512)
 
 
 class _ContractPlan:

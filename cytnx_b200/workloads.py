@@ -131,6 +131,24 @@ def build_two_site(spec: Spec, mpo_vals, seed: int = 0, device=None, hermitian: 
     return psi, L, M, M2, R
 
 
+def xxz_mpo_unitensor(Jz: float = 1.0, Jxy: float = 1.0, h: float = 0.0, device=None):
+    """The XXZ MPO as a BlockUniTensor M[w_in (ket), w_out (bra), s (ket), s' (bra)] and its bonds."""
+    from .core import BD_KET, Bond
+    from .unitensor import UniTensor
+    import torch
+
+    phys = Bond(BD_KET, np.array(SPIN_PHYS_Q).reshape(-1, 1), [1, 1])
+    inner = Bond(BD_KET, np.array(XXZ_INNER_Q).reshape(-1, 1), [1] * 5)
+    M = UniTensor([inner, inner.redirect(), phys, phys.redirect()], labels=["w0", "w1", "s", "sp"], rowrank=2,
+                  device=device, name="MPO")
+    mv = np.zeros(M._layout.nelem)
+    idx = M._layout.index()
+    for key, val in xxz_mpo_values(Jz, Jxy, h).items():
+        mv[M._layout.offs[idx[key]]] = val
+    M._data.copy_(torch.from_numpy(mv))
+    return M, inner, phys
+
+
 def heff_network_lines() -> List[str]:
     """The two-site H_eff network of example/DMRG/dmrg_two_sites_U1.py:29-34."""
     return ["psi: -1,-2,-3,-4", "L: -5,-1,0", "R: -7,-4,3", "M1: -5,-6,-2,1", "M2: -6,-7,-3,2", "TOUT: 0,1;2,3"]
