@@ -10,6 +10,7 @@ from . import linalg  # noqa: F401
 from ._lib import CytnxError
 from .core import (BD_BRA, BD_IN, BD_KET, BD_NONE, BD_OUT, BD_REG, Bond, Device, Symmetry, Tensor, Type,
                    arange, bondType, zeros)
+from .batch import BatchedTwoSiteHeff
 from .heff import TwoSiteHeff
 from .network import LinOp, Network
 from .unitensor import Contract, UniTensor, UTenType
@@ -18,4 +19,4 @@ Qs = lambda *q: list(q)  # noqa: E731  (cytnx.Qs(...) helper of the reference te
 
 __all__ = ["Type", "Device", "Symmetry", "Bond", "BD_KET", "BD_BRA", "BD_IN", "BD_OUT", "BD_REG", "BD_NONE",
            "bondType", "Tensor", "UniTensor", "UTenType", "Contract", "Network", "LinOp", "linalg",
-           "TwoSiteHeff", "CytnxError", "arange", "zeros", "Qs"]
+           "TwoSiteHeff", "BatchedTwoSiteHeff", "CytnxError", "arange", "zeros", "Qs"]

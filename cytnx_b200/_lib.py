@@ -92,6 +92,14 @@ _SIGS = {
     "ctn_heff2_profile": (c_int, [c_vp, c_vp, c_vp, c_int, c_int, P_dbl, ctypes.POINTER(c_int), c_vp]),
     "ctn_heff2_gemm_flops": (c_dbl, [c_vp, c_int]),
     "ctn_heff2_split_gemm_flops": (c_dbl, [c_vp, c_int, c_int]),
+    "ctn_heff2_batch_create": (c_int, [ctypes.POINTER(c_vp), c_int, P_i64, P_i64, P_i64, c_int, c_int, c_int, c_int,
+                                       ctypes.POINTER(c_vp)]),
+    "ctn_heff2_batch_workspace_bytes": (c_size, [c_vp]),
+    "ctn_heff2_batch_gemm_flops": (c_dbl, [c_vp]),
+    "ctn_heff2_batch_set_env": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "ctn_heff2_batch_matvec": (c_int, [c_vp, c_vp, c_vp, c_vp]),
+    "ctn_heff2_batch_profile": (c_int, [c_vp, c_vp, c_vp, c_int, P_dbl, c_vp]),
+    "ctn_heff2_batch_destroy": (None, [c_vp]),
     "ctn_lanczos_gnd": (c_int, [MATVEC_FN, c_vp, c_vp, c_i64, c_int, c_dbl, c_vp, c_vp, c_vp, P_dbl,
                                 ctypes.POINTER(c_int), c_vp]),
     "ctn_heff2_lanczos_gnd": (c_int, [c_vp, c_int, c_vp, c_int, c_dbl, c_vp, c_vp, c_vp, P_dbl,

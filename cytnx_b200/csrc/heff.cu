@@ -418,7 +418,7 @@ extern "C" ctn_status ctn_heff2_set_tiles(ctn_heff2_plan *p, int precision, int 
   CTN_REQUIRE(p, "ctn_heff2_set_tiles: null plan");
   CTN_REQUIRE(precision == CTN_PREC_3XTF32 || precision == CTN_PREC_BF16X3, "ctn_heff2_set_tiles: split precision only");
   CTN_REQUIRE(ctn::tc_tile_width_supported(bn_step1) && ctn::tc_tile_width_supported(bn_step4),
-              "ctn_heff2_set_tiles: tile widths must be one of 64, 96, 128, 144, 160, 192, 256");
+              "ctn_heff2_set_tiles: tile widths must be one of 32, 48, 64, 96, 128, 144, 160, 192, 256");
   const int k = split_kind(precision);
   if (p->split_bn[k][0] == bn_step1 && p->split_bn[k][1] == bn_step4) return CTN_OK;
   p->split_bn[k][0] = bn_step1;

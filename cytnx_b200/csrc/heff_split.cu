@@ -41,8 +41,8 @@ struct MpoTermS {
 };
 
 struct WorkItem {
-  int32_t seg, pad_;
-  int64_t chunk0;
+  int32_t seg0, seg1;  // first and last segment overlapping the item's chunks
+  int64_t chunk0;      // global chunk index of the item's first chunk
 };
 
 struct HeffSplit {
@@ -61,6 +61,8 @@ struct HeffSplit {
   int64_t o_a1h, o_a1l, o_b1h, o_b1l, o_x1, o_a4h, o_a4l, o_b4h, o_b4l, o_err, total;
   std::vector<std::pair<int64_t, int64_t>> uncovered;  // out ranges no group writes (zero them)
   uint8_t *ws = nullptr;
+  int in_f32 = 0;   // psi / L / R given in FP32 (batched form) instead of FP64
+  int out_f32 = 0;  // out written in FP32 (step-4 groups in mode 2)
   ~HeffSplit() {
     if (d_mpo) cudaFree(d_mpo);
   }
@@ -73,6 +75,27 @@ constexpr int KALIGN = 8;
 
 int64_t up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
+// workspace layout (bytes): [A1 hi|lo][B1 hi|lo][X1 f32][A4 hi|lo][B4 hi|lo][error word]
+void split_layout(HeffSplit *s) {
+  int64_t o = 0;
+  auto take = [&](int64_t bytes) {
+    const int64_t at = o;
+    o = up(o + bytes, 1024);
+    return at;
+  };
+  s->o_a1h = take(s->g1.a_bytes);
+  s->o_a1l = take(s->g1.a_bytes);
+  s->o_b1h = take(s->g1.b_bytes);
+  s->o_b1l = take(s->g1.b_bytes);
+  s->o_x1 = take(s->x1_elems * 4);
+  s->o_a4h = take(s->g4.a_bytes);
+  s->o_a4l = take(s->g4.a_bytes);
+  s->o_b4h = take(s->g4.b_bytes);
+  s->o_b4l = take(s->g4.b_bytes);
+  s->o_err = take(256);
+  s->total = o;
+}
+
 __device__ __forceinline__ float to_tf32f(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
@@ -83,7 +106,8 @@ struct MpoSParams {
   const MpoSegS *segs;
   const MpoTermS *terms;
   const WorkItem *items;
-  int64_t nitems;
+  const int64_t *begin;  // chunk prefix sums per segment
+  int64_t nitems, nchunks;
   int kind;
   const float *x1;
   uint8_t *hi, *lo;
@@ -104,9 +128,11 @@ __device__ __forceinline__ uint32_t bf16_rne_bits(float x) {
   return (u + 0x7FFFu + ((u >> 16) & 1u)) >> 16;
 }
 
-// One CTA per work item (MPO_ITEM consecutive 16-byte chunks of one X3 block): the
-// block's term list is staged in shared memory once; every thread computes MPO_UNROLL
-// chunks in FP32 (X1 is FP32) and splits them into hi/lo panel chunks.
+// One CTA per work item of MPO_ITEM consecutive 16-byte chunks.  An item inside one X3
+// block stages the block's term list in shared memory; an item spanning several small
+// blocks lets each thread find its block by a binary search over the blocks the item
+// overlaps and reads the terms through the read-only cache.  Every thread computes
+// MPO_UNROLL chunks in FP32 (X1 is FP32) and splits them into hi/lo panel chunks.
 __global__ void __launch_bounds__(MPO_THREADS) k_mpo_split(MpoSParams p) {
   __shared__ MpoTermS sterm[MPO_MAXT];
   __shared__ float scoef[MPO_MAXT];
@@ -114,20 +140,33 @@ __global__ void __launch_bounds__(MPO_THREADS) k_mpo_split(MpoSParams p) {
   const int E = tf32 ? 4 : 8;
   for (int64_t it = blockIdx.x; it < p.nitems; it += gridDim.x) {
     const WorkItem wi = p.items[it];
-    const MpoSegS s = p.segs[wi.seg];
+    const bool single = wi.seg0 == wi.seg1;  // uniform over the CTA
     __syncthreads();
-    const int nt = s.term_count;
-    if (threadIdx.x < MPO_MAXT && threadIdx.x < nt) {
-      sterm[threadIdx.x] = p.terms[s.term_begin + threadIdx.x];
-      scoef[threadIdx.x] = (float)p.terms[s.term_begin + threadIdx.x].coef;
+    if (single) {
+      const MpoSegS s0 = p.segs[wi.seg0];
+      if (threadIdx.x < MPO_MAXT && threadIdx.x < s0.term_count) {
+        sterm[threadIdx.x] = p.terms[s0.term_begin + threadIdx.x];
+        scoef[threadIdx.x] = (float)p.terms[s0.term_begin + threadIdx.x].coef;
+      }
     }
     __syncthreads();
-    const int nkc = (s.cols + E - 1) / E;
-    const int total = s.rows * nkc;
 #pragma unroll
     for (int j = 0; j < MPO_UNROLL; ++j) {
-      const int cl = (int)wi.chunk0 + threadIdx.x + j * MPO_THREADS;
-      if (cl >= total) break;
+      const int64_t g = wi.chunk0 + threadIdx.x + j * MPO_THREADS;
+      if (g >= p.nchunks) break;
+      int si = wi.seg0;
+      if (!single) {
+        int hi_s = wi.seg1;  // last block with begin <= g
+        while (si < hi_s) {
+          const int mid = (si + hi_s + 1) >> 1;
+          if (__ldg(p.begin + mid) <= g) si = mid;
+          else hi_s = mid - 1;
+        }
+      }
+      const MpoSegS s = p.segs[si];
+      const int nt = s.term_count;
+      const int nkc = (s.cols + E - 1) / E;
+      const int cl = (int)(g - __ldg(p.begin + si));
       const int r = cl / nkc;
       const int kloc = (cl - r * nkc) * E;
       const int nvalid = min(E, s.cols - kloc);
@@ -135,8 +174,9 @@ __global__ void __launch_bounds__(MPO_THREADS) k_mpo_split(MpoSParams p) {
 #pragma unroll
       for (int e = 0; e < 8; ++e) x[e] = 0.f;
       for (int t = 0; t < nt; ++t) {
-        const MpoTermS tm = t < MPO_MAXT ? sterm[t] : p.terms[s.term_begin + t];
-        const float cf = t < MPO_MAXT ? scoef[t] : (float)tm.coef;
+        const bool st = single && t < MPO_MAXT;
+        const MpoTermS tm = st ? sterm[t] : p.terms[s.term_begin + t];
+        const float cf = st ? scoef[t] : (float)tm.coef;
         const float *src = p.x1 + tm.x1_off + (int64_t)r * tm.ld + kloc;
         if (nvalid == E && tf32 && ((reinterpret_cast<uintptr_t>(src) & 15) == 0)) {
           const float4 v = __ldg(reinterpret_cast<const float4 *>(src));
@@ -320,28 +360,8 @@ ctn_status heff_split_prepare(ctn_heff2_plan *p, int kind) {
     s->seg_begin.push_back(s->seg_begin.back() + (int64_t)xi.rows * ((xi.cols + E - 1) / E));
   }
   s->nchunks = s->seg_begin.back();
-  for (size_t i = 0; i < s->segs.size(); ++i) {
-    const int64_t n = s->seg_begin[i + 1] - s->seg_begin[i];
-    for (int64_t c = 0; c < n; c += MPO_ITEM) s->items.push_back(WorkItem{(int32_t)i, 0, c});
-  }
-  // ---------------- workspace layout
-  int64_t o = 0;
-  auto take = [&](int64_t bytes) {
-    const int64_t at = o;
-    o = up(o + bytes, 1024);
-    return at;
-  };
-  s->o_a1h = take(s->g1.a_bytes);
-  s->o_a1l = take(s->g1.a_bytes);
-  s->o_b1h = take(s->g1.b_bytes);
-  s->o_b1l = take(s->g1.b_bytes);
-  s->o_x1 = take(s->x1_elems * 4);
-  s->o_a4h = take(s->g4.a_bytes);
-  s->o_a4l = take(s->g4.a_bytes);
-  s->o_b4h = take(s->g4.b_bytes);
-  s->o_b4l = take(s->g4.b_bytes);
-  s->o_err = take(256);
-  s->total = o;
+  chunk_items(s->seg_begin, MPO_ITEM, s->items);
+  split_layout(s.get());
   p->split[kind] = s.release();
   return CTN_OK;
 }
@@ -356,21 +376,19 @@ size_t heff_split_ws_bytes(const ctn_heff2_plan *p, int kind) {
   return p->split[kind] ? (size_t)p->split[kind]->total : 0;
 }
 
-ctn_status heff_split_set_env(ctn_heff2_plan *p, int kind, const double *L, const double *R, void *ws,
-                              cudaStream_t st) {
-  HeffSplit *s = p->split[kind];
+ctn_status split_set_env(HeffSplit *s, const void *L, const void *R, void *ws, cudaStream_t st) {
   CTN_REQUIRE(s, "heff split: not prepared");
   s->ws = (uint8_t *)ws;
   CTN_CUDA(cudaMemsetAsync(ws, 0, s->total, st));
-  CTN_TRY(s->pk_L.run(L, 0, s->ws + s->o_a1h, s->ws + s->o_a1l, st));
-  CTN_TRY(s->pk_R.run(R, 0, s->ws + s->o_b4h, s->ws + s->o_b4l, st));
+  CTN_TRY(s->pk_L.run(L, s->in_f32, s->ws + s->o_a1h, s->ws + s->o_a1l, st));
+  CTN_TRY(s->pk_R.run(R, s->in_f32, s->ws + s->o_b4h, s->ws + s->o_b4l, st));
   // device copy of the MPO segment tables
   int dev = 0;
   CTN_CUDA(cudaGetDevice(&dev));
   if (!s->d_mpo || s->d_dev != dev) {
     if (s->d_mpo) cudaFree(s->d_mpo);
     const size_t bytes = s->segs.size() * sizeof(MpoSegS) + s->terms.size() * sizeof(MpoTermS) +
-                         s->items.size() * sizeof(WorkItem) + 64;
+                         s->items.size() * sizeof(WorkItem) + s->seg_begin.size() * sizeof(int64_t) + 64;
     CTN_CUDA(cudaMalloc(&s->d_mpo, bytes));
     s->d_dev = dev;
     char *q = (char *)s->d_mpo;
@@ -379,6 +397,9 @@ ctn_status heff_split_set_env(ctn_heff2_plan *p, int kind, const double *L, cons
     if (!s->terms.empty()) CTN_CUDA(cudaMemcpyAsync(q, s->terms.data(), s->terms.size() * sizeof(MpoTermS), cudaMemcpyHostToDevice, st));
     q += s->terms.size() * sizeof(MpoTermS);
     if (!s->items.empty()) CTN_CUDA(cudaMemcpyAsync(q, s->items.data(), s->items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, st));
+    q += s->items.size() * sizeof(WorkItem);
+    if (!s->seg_begin.empty())
+      CTN_CUDA(cudaMemcpyAsync(q, s->seg_begin.data(), s->seg_begin.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
     CTN_CUDA(cudaStreamSynchronize(st));
   }
   CTN_TRY(s->g1.upload(st));
@@ -387,17 +408,22 @@ ctn_status heff_split_set_env(ctn_heff2_plan *p, int kind, const double *L, cons
   return CTN_OK;
 }
 
-ctn_status heff_split_matvec(ctn_heff2_plan *p, int kind, const double *psi, double *out, cudaStream_t st,
-                             double *ms4) {
-  HeffSplit *s = p->split[kind];
+ctn_status heff_split_set_env(ctn_heff2_plan *p, int kind, const double *L, const double *R, void *ws,
+                              cudaStream_t st) {
+  return split_set_env(p->split[kind], L, R, ws, st);
+}
+
+ctn_status split_matvec(HeffSplit *s, const void *psi, void *out, cudaStream_t st, double *ms4) {
   CTN_REQUIRE(s && s->ws, "heff split: environments not bound");
+  const int kind = s->kind;
+  const size_t oes = s->out_f32 ? 4 : 8;
   uint8_t *w = s->ws;
   cudaEvent_t ev[5];
   if (ms4)
     for (auto &e : ev) CTN_CUDA(cudaEventCreate(&e));
   if (ms4) CTN_CUDA(cudaEventRecord(ev[0], st));
-  for (auto &u : s->uncovered) CTN_CUDA(cudaMemsetAsync(out + u.first, 0, u.second * sizeof(double), st));
-  CTN_TRY(s->pk_P.run(psi, 0, w + s->o_b1h, w + s->o_b1l, st));
+  for (auto &u : s->uncovered) CTN_CUDA(cudaMemsetAsync((char *)out + u.first * oes, 0, u.second * oes, st));
+  CTN_TRY(s->pk_P.run(psi, s->in_f32, w + s->o_b1h, w + s->o_b1l, st));
   if (ms4) CTN_CUDA(cudaEventRecord(ev[1], st));
   int *err = (int *)(w + s->o_err);
   CTN_TRY(s->g1.run(w + s->o_a1h, w + s->o_a1l, w + s->o_b1h, w + s->o_b1l, (float *)(w + s->o_x1), nullptr, err, st));
@@ -408,7 +434,10 @@ ctn_status heff_split_matvec(ctn_heff2_plan *p, int kind, const double *psi, dou
     prm.segs = (const MpoSegS *)q;
     prm.terms = (const MpoTermS *)(q + s->segs.size() * sizeof(MpoSegS));
     prm.items = (const WorkItem *)(q + s->segs.size() * sizeof(MpoSegS) + s->terms.size() * sizeof(MpoTermS));
+    prm.begin = (const int64_t *)(q + s->segs.size() * sizeof(MpoSegS) + s->terms.size() * sizeof(MpoTermS) +
+                                  s->items.size() * sizeof(WorkItem));
     prm.nitems = (int64_t)s->items.size();
+    prm.nchunks = s->nchunks;
     prm.kind = kind;
     prm.x1 = (const float *)(w + s->o_x1);
     prm.hi = w + s->o_a4h;
@@ -421,7 +450,10 @@ ctn_status heff_split_matvec(ctn_heff2_plan *p, int kind, const double *psi, dou
     CTN_CHECK_LAUNCH();
   }
   if (ms4) CTN_CUDA(cudaEventRecord(ev[3], st));
-  CTN_TRY(s->g4.run(w + s->o_a4h, w + s->o_a4l, w + s->o_b4h, w + s->o_b4l, nullptr, out, err, st));
+  if (s->out_f32)
+    CTN_TRY(s->g4.run(w + s->o_a4h, w + s->o_a4l, w + s->o_b4h, w + s->o_b4l, (float *)out, nullptr, err, st));
+  else
+    CTN_TRY(s->g4.run(w + s->o_a4h, w + s->o_a4l, w + s->o_b4h, w + s->o_b4l, nullptr, (double *)out, err, st));
   if (ms4) {
     CTN_CUDA(cudaEventRecord(ev[4], st));
     CTN_CUDA(cudaEventSynchronize(ev[4]));
@@ -435,4 +467,151 @@ ctn_status heff_split_matvec(ctn_heff2_plan *p, int kind, const double *psi, dou
   return CTN_OK;
 }
 
+ctn_status heff_split_matvec(ctn_heff2_plan *p, int kind, const double *psi, double *out, cudaStream_t st,
+                             double *ms4) {
+  return split_matvec(p->split[kind], psi, out, st, ms4);
+}
+
+// ---------------------------------------------------------------- batches of independent problems
+// The split tables of every problem are concatenated with their operand, panel, X1 and
+// output offsets shifted, so each phase of all problems is ONE launch (the tcgen05 GEMMs
+// schedule the union of all tiles, largest K first).
+HeffSplit *split_batch(std::vector<ctn_heff2_plan *> &plans, const int64_t *psi_offs, const int64_t *L_offs,
+                       const int64_t *R_offs, int kind, int bn1, int bn4, int fp32_io, ctn_status *st) {
+  *st = CTN_OK;
+  std::unique_ptr<HeffSplit> B(new HeffSplit());
+  B->kind = kind;
+  B->g1.kind = B->g4.kind = kind;
+  B->g1.bn = bn1;
+  B->g4.bn = bn4;
+  B->pk_L.kind = B->pk_P.kind = B->pk_R.kind = kind;
+  B->in_f32 = fp32_io;
+  B->out_f32 = fp32_io;
+  int64_t a1 = 0, b1 = 0, x1 = 0, a4 = 0, b4 = 0;
+  B->seg_begin.push_back(0);
+  for (size_t i = 0; i < plans.size(); ++i) {
+    ctn_heff2_plan *p = plans[i];
+    p->split_bn[kind][0] = bn1;
+    p->split_bn[kind][1] = bn4;
+    if (p->split[kind] && (p->split[kind]->g1.bn != bn1 || p->split[kind]->g4.bn != bn4)) {
+      delete p->split[kind];
+      p->split[kind] = nullptr;
+    }
+    *st = heff_split_prepare(p, kind);
+    if (*st != CTN_OK) return nullptr;
+    const HeffSplit *S = p->split[kind];
+    for (TcGroup g : S->g1.groups) {
+      g.a_off += a1;
+      g.b_off += b1;
+      g.c_off += x1;
+      B->g1.groups.push_back(g);
+    }
+    for (PackSeg sg : S->pk_L.segs) {
+      sg.src_off += L_offs[i];
+      sg.panel_off += a1;
+      B->pk_L.segs.push_back(sg);
+    }
+    for (PackSeg sg : S->pk_P.segs) {
+      sg.src_off += psi_offs[i];
+      sg.panel_off += b1;
+      B->pk_P.segs.push_back(sg);
+    }
+    const int64_t rm_base = (int64_t)B->g4.rowmap.size();
+    for (TcGroup g : S->g4.groups) {
+      g.a_off += a4;
+      g.b_off += b4;
+      g.rm_off += rm_base;
+      if (fp32_io) g.mode = 2;
+      B->g4.groups.push_back(g);
+    }
+    for (int64_t r : S->g4.rowmap) B->g4.rowmap.push_back(r + psi_offs[i]);
+    for (PackSeg sg : S->pk_R.segs) {
+      sg.src_off += R_offs[i];
+      sg.panel_off += b4;
+      B->pk_R.segs.push_back(sg);
+    }
+    const int32_t tbase = (int32_t)B->terms.size();
+    for (MpoSegS sg : S->segs) {
+      sg.panel_off += a4;
+      sg.term_begin += tbase;
+      B->segs.push_back(sg);
+    }
+    for (MpoTermS t : S->terms) {
+      t.x1_off += x1;
+      B->terms.push_back(t);
+    }
+    for (size_t k = 0; k + 1 < S->seg_begin.size(); ++k)
+      B->seg_begin.push_back(B->seg_begin.back() + (S->seg_begin[k + 1] - S->seg_begin[k]));
+    for (auto u : S->uncovered) B->uncovered.push_back({u.first + psi_offs[i], u.second});
+    a1 += S->g1.a_bytes;
+    b1 += S->g1.b_bytes;
+    x1 += S->x1_elems;
+    a4 += S->g4.a_bytes;
+    b4 += S->g4.b_bytes;
+    B->g1.flops += S->g1.flops;
+    B->g4.flops += S->g4.flops;
+  }
+  B->g1.a_bytes = a1;
+  B->g1.b_bytes = b1;
+  B->g4.a_bytes = a4;
+  B->g4.b_bytes = b4;
+  B->x1_elems = x1;
+  B->g1.finalize();
+  B->g4.finalize();
+  B->pk_L.finalize();
+  B->pk_P.finalize();
+  B->pk_R.finalize();
+  B->nchunks = B->seg_begin.back();
+  chunk_items(B->seg_begin, MPO_ITEM, B->items);
+  split_layout(B.get());
+  return B.release();
+}
+
 }  // namespace ctn
+
+struct ctn_heff2_batch {
+  ctn::HeffSplit *s = nullptr;
+  ~ctn_heff2_batch() { delete s; }
+};
+
+extern "C" ctn_status ctn_heff2_batch_create(ctn_heff2_plan *const *plans, int nprob, const int64_t *psi_offs,
+                                             const int64_t *L_offs, const int64_t *R_offs, int precision,
+                                             int bn_step1, int bn_step4, int fp32_io, ctn_heff2_batch **out) {
+  CTN_REQUIRE(plans && nprob > 0 && psi_offs && L_offs && R_offs && out, "ctn_heff2_batch_create: bad argument");
+  CTN_REQUIRE(precision == CTN_PREC_3XTF32 || precision == CTN_PREC_BF16X3,
+              "ctn_heff2_batch_create: split precisions only (3xTF32 or BF16x3)");
+  CTN_REQUIRE(ctn::tc_tile_width_supported(bn_step1) && ctn::tc_tile_width_supported(bn_step4),
+              "ctn_heff2_batch_create: unsupported tile width");
+  for (int i = 0; i < nprob; ++i) CTN_REQUIRE(plans[i], "ctn_heff2_batch_create: null plan");
+  std::vector<ctn_heff2_plan *> v(plans, plans + nprob);
+  ctn_status st = CTN_OK;
+  const int kind = precision == CTN_PREC_BF16X3 ? ctn::TC_BF16 : ctn::TC_TF32;
+  ctn::HeffSplit *s = ctn::split_batch(v, psi_offs, L_offs, R_offs, kind, bn_step1, bn_step4, fp32_io ? 1 : 0, &st);
+  if (!s) return st;
+  auto *b = new ctn_heff2_batch();
+  b->s = s;
+  *out = b;
+  return CTN_OK;
+}
+extern "C" size_t ctn_heff2_batch_workspace_bytes(const ctn_heff2_batch *b) { return b ? (size_t)b->s->total : 0; }
+extern "C" double ctn_heff2_batch_gemm_flops(const ctn_heff2_batch *b) {
+  return b ? b->s->g1.flops + b->s->g4.flops : 0.0;
+}
+extern "C" ctn_status ctn_heff2_batch_set_env(ctn_heff2_batch *b, const void *L_all, const void *R_all,
+                                              void *workspace, void *stream) {
+  CTN_REQUIRE(b && L_all && R_all && workspace, "ctn_heff2_batch_set_env: null argument");
+  return ctn::split_set_env(b->s, L_all, R_all, workspace, ctn::as_stream(stream));
+}
+extern "C" ctn_status ctn_heff2_batch_matvec(ctn_heff2_batch *b, const void *psi_all, void *out_all, void *stream) {
+  CTN_REQUIRE(b && psi_all && out_all, "ctn_heff2_batch_matvec: null argument");
+  return ctn::split_matvec(b->s, psi_all, out_all, ctn::as_stream(stream), nullptr);
+}
+extern "C" ctn_status ctn_heff2_batch_profile(ctn_heff2_batch *b, const void *psi_all, void *out_all, int reps,
+                                              double *ms4, void *stream) {
+  CTN_REQUIRE(b && psi_all && out_all && reps > 0 && ms4, "ctn_heff2_batch_profile: bad argument");
+  double acc[4] = {0, 0, 0, 0};
+  for (int r = 0; r < reps; ++r) CTN_TRY(ctn::split_matvec(b->s, psi_all, out_all, ctn::as_stream(stream), acc));
+  for (int i = 0; i < 4; ++i) ms4[i] = acc[i] / reps;
+  return CTN_OK;
+}
+extern "C" void ctn_heff2_batch_destroy(ctn_heff2_batch *b) { delete b; }

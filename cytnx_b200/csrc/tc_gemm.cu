@@ -268,9 +268,9 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
         const int cg0 = tl.nt * BN + c0;
         if (cg0 >= g.N || dst < 0) continue;
         const int ncol = min(min(32, BN - c0), g.N - cg0);  // a 32-column piece may pass the tile edge
-        if (g.mode == 0) {
+        if (g.mode != 1) {
           float *o = p.c32 + dst + cg0;
-          if (ncol == 32) {
+          if (ncol == 32 && ((reinterpret_cast<uintptr_t>(o) & 15) == 0)) {
 #pragma unroll
             for (int j = 0; j < 8; ++j)
               *reinterpret_cast<float4 *>(o + 4 * j) = make_float4(
@@ -384,25 +384,34 @@ constexpr int PACK_ITEM = PACK_THREADS * PACK_UNROLL;
 struct PackItemParams {
   const PackSeg *segs;
   const PackItem *items;
-  int64_t nitems;
+  const int64_t *begin;  // chunk prefix sums per segment (nseg + 1)
+  int64_t nitems, nchunks;
   int kind;
   int src_f32;
   const void *src;
   uint8_t *hi, *lo;
 };
 
-// One CTA per work item of PACK_ITEM chunks of one segment; rows fastest, so the
+// One CTA per work item of PACK_ITEM consecutive chunks; an item may span many small
+// segments (each thread finds its own segment by a binary search over the few the item
+// overlaps), so tiny blocks do not waste CTAs.  Rows fastest inside a segment, so the
 // source reads (rows are the contiguous axis of every operand packed here) coalesce.
 __global__ void __launch_bounds__(PACK_THREADS) k_pack_items(PackItemParams p) {
   const int E = p.kind == TC_TF32 ? 4 : 8;
   for (int64_t it = blockIdx.x; it < p.nitems; it += gridDim.x) {
     const PackItem wi = p.items[it];
-    const PackSeg s = p.segs[wi.seg];
-    const int64_t total = (int64_t)s.rows * ((s.cols + E - 1) / E);
 #pragma unroll
     for (int j = 0; j < PACK_UNROLL; ++j) {
-      const int64_t cl = wi.chunk0 + threadIdx.x + j * PACK_THREADS;
-      if (cl >= total) break;
+      const int64_t g = wi.chunk0 + threadIdx.x + j * PACK_THREADS;
+      if (g >= p.nchunks) break;
+      int lo_s = wi.seg0, hi_s = wi.seg1;  // last segment with begin <= g
+      while (lo_s < hi_s) {
+        const int mid = (lo_s + hi_s + 1) >> 1;
+        if (__ldg(p.begin + mid) <= g) lo_s = mid;
+        else hi_s = mid - 1;
+      }
+      const PackSeg s = p.segs[lo_s];
+      const int64_t cl = g - __ldg(p.begin + lo_s);
       const int r = (int)(cl % s.rows);
       const int kloc = (int)(cl / s.rows) * E;
       double x[8];
@@ -529,6 +538,8 @@ ctn_status launch_tc(const TcParams &prm, int64_t ntiles, cudaStream_t st) {
 template <int KIND>
 ctn_status launch_tc_kind(int bn, const TcParams &prm, cudaStream_t st) {
   switch (bn) {
+    case 32: return launch_tc<KIND, 32, 5>(prm, prm.ntiles, st);
+    case 48: return launch_tc<KIND, 48, 4>(prm, prm.ntiles, st);
     case 64: return launch_tc<KIND, 64, 4>(prm, prm.ntiles, st);
     case 96: return launch_tc<KIND, 96, 3>(prm, prm.ntiles, st);
     case 128: return launch_tc<KIND, 128, 3>(prm, prm.ntiles, st);
@@ -537,7 +548,7 @@ ctn_status launch_tc_kind(int bn, const TcParams &prm, cudaStream_t st) {
     case 192: return launch_tc<KIND, 192, 2>(prm, prm.ntiles, st);
     case 256: return launch_tc<KIND, 256, 2>(prm, prm.ntiles, st);
   }
-  set_error("tcgen05 GEMM: unsupported tile width %d (64, 96, 128, 144, 160, 192, 256)", bn);
+  set_error("tcgen05 GEMM: unsupported tile width %d (32, 48, 64, 96, 128, 144, 160, 192, 256)", bn);
   return CTN_ERR_UNSUPPORTED;
 }
 ctn_status launch_tc_any(int kind, int bn, const TcParams &prm, cudaStream_t st) {
@@ -547,7 +558,8 @@ ctn_status launch_tc_any(int kind, int bn, const TcParams &prm, cudaStream_t st)
 }  // namespace
 
 bool tc_tile_width_supported(int bn) {
-  return bn == 64 || bn == 96 || bn == 128 || bn == 144 || bn == 160 || bn == 192 || bn == 256;
+  return bn == 32 || bn == 48 || bn == 64 || bn == 96 || bn == 128 || bn == 144 || bn == 160 || bn == 192 ||
+         bn == 256;
 }
 
 int TcGemm::add_group(int M, int N, int K, int mode, int64_t c_off, int ldc, int64_t rm_off) {
@@ -675,21 +687,21 @@ void Packer::finalize() {
     seg_chunk_begin[i + 1] = seg_chunk_begin[i] + kc * segs[i].rows;
   }
   nchunks = seg_chunk_begin.back();
-  items.clear();
-  for (size_t i = 0; i < segs.size(); ++i) {
-    const int64_t n = seg_chunk_begin[i + 1] - seg_chunk_begin[i];
-    for (int64_t c = 0; c < n; c += PACK_ITEM) items.push_back(PackItem{(int32_t)i, 0, c});
-  }
+  chunk_items(seg_chunk_begin, PACK_ITEM, items);
   tile_items.clear();
-  transposing = !segs.empty();
-  for (const auto &sg : segs) transposing &= (sg.sr == 1);
-  if (transposing) {
+  bool all_rows = !segs.empty();
+  for (const auto &sg : segs) all_rows &= (sg.sr == 1);
+  if (all_rows) {
     for (size_t i = 0; i < segs.size(); ++i) {
       const int nkc = (segs[i].cols + E - 1) / E;
       for (int r0 = 0; r0 < segs[i].rows; r0 += 32)
         for (int kc = 0; kc < nkc; kc += 8) tile_items.push_back(PackTileItemH{(int32_t)i, r0, kc, 0});
     }
   }
+  // the transposing tile pack (32 rows x 8 chunks per item) pays off only when the
+  // blocks fill most of its tiles; small blocks use the flattened chunk items
+  transposing = all_rows && (double)nchunks >= 0.5 * 256.0 * (double)tile_items.size();
+  if (!transposing) tile_items.clear();
 }
 
 ctn_status Packer::upload(cudaStream_t st) {
@@ -699,16 +711,19 @@ ctn_status Packer::upload(cudaStream_t st) {
   if (d_mem) cudaFree(d_mem);
   d_mem = nullptr;
   const size_t bytes = segs.size() * sizeof(PackSeg) + items.size() * sizeof(PackItem) +
-                       tile_items.size() * sizeof(PackTileItem) + 64;
+                       tile_items.size() * sizeof(PackTileItem) + seg_chunk_begin.size() * sizeof(int64_t) + 64;
   CTN_CUDA(cudaMalloc(&d_mem, bytes));
   d_dev = dev;
-  if (!segs.empty()) CTN_CUDA(cudaMemcpyAsync(d_mem, segs.data(), segs.size() * sizeof(PackSeg), cudaMemcpyHostToDevice, st));
-  if (!items.empty())
-    CTN_CUDA(cudaMemcpyAsync((char *)d_mem + segs.size() * sizeof(PackSeg), items.data(), items.size() * sizeof(PackItem),
-                             cudaMemcpyHostToDevice, st));
+  char *q = (char *)d_mem;
+  if (!segs.empty()) CTN_CUDA(cudaMemcpyAsync(q, segs.data(), segs.size() * sizeof(PackSeg), cudaMemcpyHostToDevice, st));
+  q += segs.size() * sizeof(PackSeg);
+  if (!items.empty()) CTN_CUDA(cudaMemcpyAsync(q, items.data(), items.size() * sizeof(PackItem), cudaMemcpyHostToDevice, st));
+  q += items.size() * sizeof(PackItem);
   if (!tile_items.empty())
-    CTN_CUDA(cudaMemcpyAsync((char *)d_mem + segs.size() * sizeof(PackSeg) + items.size() * sizeof(PackItem),
-                             tile_items.data(), tile_items.size() * sizeof(PackTileItem), cudaMemcpyHostToDevice, st));
+    CTN_CUDA(cudaMemcpyAsync(q, tile_items.data(), tile_items.size() * sizeof(PackTileItem), cudaMemcpyHostToDevice, st));
+  q += tile_items.size() * sizeof(PackTileItem);
+  if (!seg_chunk_begin.empty())
+    CTN_CUDA(cudaMemcpyAsync(q, seg_chunk_begin.data(), seg_chunk_begin.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
   CTN_CUDA(cudaStreamSynchronize(st));
   return CTN_OK;
 }
@@ -732,9 +747,13 @@ ctn_status Packer::run(const void *src, int src_is_f32, uint8_t *hi, uint8_t *lo
     return CTN_OK;
   }
   PackItemParams prm;
-  prm.segs = (const PackSeg *)d_mem;
-  prm.items = (const PackItem *)((const char *)d_mem + segs.size() * sizeof(PackSeg));
+  const char *q = (const char *)d_mem;
+  prm.segs = (const PackSeg *)q;
+  prm.items = (const PackItem *)(q + segs.size() * sizeof(PackSeg));
+  prm.begin = (const int64_t *)(q + segs.size() * sizeof(PackSeg) + items.size() * sizeof(PackItem) +
+                                tile_items.size() * sizeof(PackTileItem));
   prm.nitems = (int64_t)items.size();
+  prm.nchunks = nchunks;
   prm.kind = kind;
   prm.src_f32 = src_is_f32;
   prm.src = src;

@@ -11,6 +11,7 @@
 // issues three MMAs lo*hi + hi*lo + hi*hi into one FP32 TMEM accumulator.
 #pragma once
 #include <cstdint>
+#include <algorithm>
 #include <vector>
 
 #include "ctn_common.h"
@@ -32,7 +33,7 @@ struct TcGroup {
   int64_t b_off;      // byte offset of tile (0,0) in the B panels
   int32_t M, N, K;    // logical sizes
   int32_t mt, nt, kb; // tile counts (128-row A tiles, BN-row B tiles, K slices)
-  int32_t mode;       // 0: C32[c_off + r*ldc + c] (FP32), 1: C64[rowmap[rm_off + r] + c] (FP64)
+  int32_t mode;       // 0: C32[c_off + r*ldc + c], 1: C64[rowmap[rm_off + r] + c], 2: C32[rowmap[rm_off + r] + c]
   int32_t ldc;
   int64_t c_off;
   int64_t rm_off;
@@ -97,8 +98,8 @@ struct PackSeg {
 };
 
 struct PackItem {
-  int32_t seg, pad_;
-  int64_t chunk0;  // first chunk of this CTA work item inside the segment
+  int32_t seg0, seg1;  // first and last segment overlapping the item's chunks
+  int64_t chunk0;      // first chunk of this CTA work item (global chunk index)
 };
 
 struct PackTileItemH {
@@ -111,7 +112,7 @@ struct Packer {
   bool transposing = false;
   std::vector<PackSeg> segs;
   std::vector<int64_t> seg_chunk_begin;  // prefix sums of 16-byte chunks per segment
-  std::vector<PackItem> items;           // CTA work items (one segment each, no search on device)
+  std::vector<PackItem> items;           // CTA work items: PACK_ITEM consecutive chunks (may span segments)
   int64_t nchunks = 0;
   void *d_mem = nullptr;
   int d_dev = -1;
@@ -124,6 +125,27 @@ struct Packer {
 
 
 bool tc_tile_width_supported(int bn);
+
+// Work items of `per_item` consecutive chunks over segments with chunk prefix sums
+// `begin`; each item records the first and last segment it overlaps (seg0, seg1).
+template <class Item>
+inline void chunk_items(const std::vector<int64_t> &begin, int64_t per_item, std::vector<Item> &items) {
+  items.clear();
+  const int64_t total = begin.back();
+  const int nseg = (int)begin.size() - 1;
+  int s = 0;
+  for (int64_t c0 = 0; c0 < total; c0 += per_item) {
+    while (s + 1 < nseg && begin[s + 1] <= c0) ++s;
+    int e = s;
+    const int64_t last = std::min(c0 + per_item, total) - 1;
+    while (e + 1 < nseg && begin[e + 1] <= last) ++e;
+    Item it{};
+    it.seg0 = s;
+    it.seg1 = e;
+    it.chunk0 = c0;
+    items.push_back(it);
+  }
+}
 
 // Launch helpers over device-resident tables (the caller owns every buffer).
 ctn_status tc_launch_tables(int kind, int bn, const TcGroup *d_groups, const TcTile *d_tiles, int64_t ntiles,

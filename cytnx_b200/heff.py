@@ -31,6 +31,31 @@ def _plain_desc(u: UniTensor, keep):
     return u, _desc(u._layout, None, u._layout.itoi, u._layout.shapes, keep)
 
 
+def plan_two_site(L: UniTensor, M1: UniTensor, M2: UniTensor, R: UniTensor, psi: UniTensor, keep: list):
+    """Plan the two-site matvec on the host from the operands' block structure and the
+    MPO values (no device data is read).  Returns (plan handle, contiguous operands,
+    output bonds, output layout); ``keep`` collects the host arrays the plan was built from."""
+    Lc, dL = _plain_desc(L, keep)
+    M1c, dM1 = _plain_desc(M1, keep)
+    M2c, dM2 = _plain_desc(M2, keep)
+    Rc, dR = _plain_desc(R, keep)
+    Pc, dP = _plain_desc(psi, keep)
+    out_bonds = [Lc.bonds()[2], M1c.bonds()[3], M2c.bonds()[3], Rc.bonds()[2]]
+    out_layout = layout_for(out_bonds)
+    if not np.array_equal(out_layout.itoi, Pc._layout.itoi) or \
+            not np.array_equal(out_layout.shapes, Pc._layout.shapes):
+        raise CytnxError("[TwoSiteHeff] the output block structure differs from psi's")
+    dO = _desc(out_layout, None, out_layout.itoi, out_layout.shapes, keep)
+    m1h = M1c._data.detach().cpu().numpy().astype(np.float64)
+    m2h = M2c._data.detach().cpu().numpy().astype(np.float64)
+    keep += [m1h, m2h]
+    desc = Heff2Desc(ctypes.pointer(dP), ctypes.pointer(dL), ctypes.pointer(dR), ctypes.pointer(dM1),
+                     ctypes.pointer(dM2), ctypes.pointer(dO), m1h.ctypes.data, m2h.ctypes.data)
+    h = ctypes.c_void_p()
+    _lib.check(_lib.lib().ctn_heff2_plan_create(ctypes.byref(desc), ctypes.byref(h)), "TwoSiteHeff")
+    return h.value, (Lc, M1c, M2c, Rc, Pc), out_bonds, out_layout
+
+
 class TwoSiteHeff(LinOp):
     def __init__(self, L: UniTensor, M1: UniTensor, M2: UniTensor, R: UniTensor, psi: UniTensor,
                  precision: str = "fp64"):
@@ -39,28 +64,10 @@ class TwoSiteHeff(LinOp):
         for t, nm in ((L, "L"), (M1, "M1"), (M2, "M2"), (R, "R"), (psi, "psi")):
             if t.dtype() != Type.Double:
                 raise CytnxError(f"[TwoSiteHeff] {nm} must be float64")
+        require_cuda(L._data, "TwoSiteHeff")
         keep: list = []
-        self.L, dL = _plain_desc(L, keep)
-        self.M1, dM1 = _plain_desc(M1, keep)
-        self.M2, dM2 = _plain_desc(M2, keep)
-        self.R, dR = _plain_desc(R, keep)
-        self.psi_t, dP = _plain_desc(psi, keep)
-        require_cuda(self.L._data, "TwoSiteHeff")
-        out_bonds = [self.L.bonds()[2], self.M1.bonds()[3], self.M2.bonds()[3], self.R.bonds()[2]]
-        self.out_layout = layout_for(out_bonds)
-        if not np.array_equal(self.out_layout.itoi, self.psi_t._layout.itoi) or \
-                not np.array_equal(self.out_layout.shapes, self.psi_t._layout.shapes):
-            raise CytnxError("[TwoSiteHeff] the output block structure differs from psi's")
-        self.out_bonds = out_bonds
-        dO = _desc(self.out_layout, None, self.out_layout.itoi, self.out_layout.shapes, keep)
-        m1h = self.M1._data.detach().cpu().numpy().astype(np.float64)
-        m2h = self.M2._data.detach().cpu().numpy().astype(np.float64)
-        keep += [m1h, m2h]
-        desc = Heff2Desc(ctypes.pointer(dP), ctypes.pointer(dL), ctypes.pointer(dR), ctypes.pointer(dM1),
-                         ctypes.pointer(dM2), ctypes.pointer(dO), m1h.ctypes.data, m2h.ctypes.data)
-        h = ctypes.c_void_p()
-        _lib.check(_lib.lib().ctn_heff2_plan_create(ctypes.byref(desc), ctypes.byref(h)), "TwoSiteHeff")
-        self._h = h.value
+        self._h, (self.L, self.M1, self.M2, self.R, self.psi_t), self.out_bonds, self.out_layout = \
+            plan_two_site(L, M1, M2, R, psi, keep)
         self._keep = keep
         self.n = int(_lib.lib().ctn_heff2_psi_elems(self._h))
         self.plan_flops = float(_lib.lib().ctn_heff2_flops(self._h))

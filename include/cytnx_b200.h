@@ -237,11 +237,40 @@ double ctn_heff2_gemm_flops(const ctn_heff2_plan *plan, int step);
 /* the same for the stacked tensor-core GEMMs of a split precision (one product counted) */
 double ctn_heff2_split_gemm_flops(ctn_heff2_plan *plan, int precision, int step);
 void ctn_heff2_plan_destroy(ctn_heff2_plan *plan);
-/* tile widths (N of the UMMA tiles: 64, 96, 128, 144, 160, 192 or 256) of the step-1 and
+/* tile widths (N of the UMMA tiles: 32, 48, 64, 96, 128, 144, 160, 192 or 256) of the step-1 and
  * step-4 tensor-core GEMMs of a split precision; drops that precision's binding (the
  * operand panels depend on the widths), so call ctn_heff2_set_env again.  Used by the
  * autotuner (TwoSiteHeff.autotune). */
 ctn_status ctn_heff2_set_tiles(ctn_heff2_plan *plan, int precision, int bn_step1, int bn_step4);
+
+/* ---------------------------------------------------------------- batched H_eff
+ * Many independent two-site problems (uneven block structures) applied together: the
+ * split-precision tables of every plan are concatenated, so each phase (pack, step-1
+ * GEMM, MPO fold, step-4 GEMM) of all problems is one launch; the two tcgen05 GEMMs are
+ * persistent grouped launches over the union of all problems' tiles.  The vectors and
+ * environments of problem i live at element offsets psi_offs[i] / L_offs[i] / R_offs[i]
+ * of shared flat buffers (the output uses psi's offsets).  fp32_io != 0: psi, L, R and
+ * out are FP32 (else FP64).  ctn_heff2_batch_matvec issues no host synchronisation once
+ * ctn_heff2_batch_set_env has run, so it may be recorded in a CUDA graph.  Creating a
+ * batch (re)prepares each plan's split tables for the given tile widths.
+ * No counterpart in the reference, which contracts one network at a time through
+ * Network::Launch (src/RegularNetwork.cpp:901-1007); this batches the two-site matvec
+ * of example/DMRG/dmrg_two_sites_U1.py:18-23 over many problems. */
+typedef struct ctn_heff2_batch ctn_heff2_batch;
+ctn_status ctn_heff2_batch_create(ctn_heff2_plan *const *plans, int nprob, const int64_t *psi_offs,
+                                  const int64_t *L_offs, const int64_t *R_offs, int precision,
+                                  int bn_step1, int bn_step4, int fp32_io, ctn_heff2_batch **batch);
+size_t ctn_heff2_batch_workspace_bytes(const ctn_heff2_batch *batch);
+/* useful flops of one batched matvec (2*M*N*K over the GEMM groups, one product) */
+double ctn_heff2_batch_gemm_flops(const ctn_heff2_batch *batch);
+ctn_status ctn_heff2_batch_set_env(ctn_heff2_batch *batch, const void *L_all, const void *R_all,
+                                   void *workspace, void *stream);
+ctn_status ctn_heff2_batch_matvec(ctn_heff2_batch *batch, const void *psi_all, void *out_all,
+                                  void *stream);
+/* average phase times over `reps` matvecs: ms[0..3] = pack, step-1 GEMM, MPO fold, step-4 GEMM */
+ctn_status ctn_heff2_batch_profile(ctn_heff2_batch *batch, const void *psi_all, void *out_all,
+                                   int reps, double *ms, void *stream);
+void ctn_heff2_batch_destroy(ctn_heff2_batch *batch);
 
 /* ---------------------------------------------------------------- Lanczos
  * Ground state by the Lanczos_Gnd_Ut recurrence on flat FP64 device vectors.
