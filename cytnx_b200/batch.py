@@ -247,3 +247,19 @@ class BatchedTwoSiteHeff:
         self._create(best1, best4)
         self.set_env(L_all, R_all)
         return {"step1": best1, "step4": best4, "ms_step1": t1, "ms_step4": t4}
+
+
+def shard_problems(costs: Sequence[float], nshards: int) -> List[List[int]]:
+    """Split problems over ``nshards`` ranks by longest-processing-time-first: problems in
+    decreasing cost go to the currently lightest shard (ties: lowest rank).  Deterministic,
+    so every rank computes the same assignment without communicating."""
+    if nshards < 1:
+        raise CytnxError("[shard_problems] nshards must be >= 1")
+    order = sorted(range(len(costs)), key=lambda i: (-float(costs[i]), i))
+    load = [0.0] * nshards
+    shards: List[List[int]] = [[] for _ in range(nshards)]
+    for i in order:
+        r = min(range(nshards), key=lambda k: (load[k], k))
+        shards[r].append(i)
+        load[r] += float(costs[i])
+    return [sorted(s) for s in shards]
