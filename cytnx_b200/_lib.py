@@ -102,6 +102,10 @@ _SIGS = {
     "ctn_heff2_batch_destroy": (None, [c_vp]),
     "ctn_lanczos_gnd": (c_int, [MATVEC_FN, c_vp, c_vp, c_i64, c_int, c_dbl, c_vp, c_vp, c_vp, P_dbl,
                                 ctypes.POINTER(c_int), c_vp]),
+    "ctn_lanczos_refined": (c_int, [MATVEC_FN, c_vp, MATVEC_FN, c_vp, c_vp, c_i64, c_int, c_int, c_dbl, c_vp, c_vp,
+                                    c_vp, P_dbl, P_dbl, ctypes.POINTER(c_int), P_i64, c_vp]),
+    "ctn_heff2_lanczos_refined": (c_int, [c_vp, c_int, c_vp, c_int, c_int, c_dbl, c_vp, c_vp, c_vp, P_dbl, P_dbl,
+                                          ctypes.POINTER(c_int), P_i64, c_vp]),
     "ctn_heff2_lanczos_gnd": (c_int, [c_vp, c_int, c_vp, c_int, c_dbl, c_vp, c_vp, c_vp, P_dbl,
                                       ctypes.POINTER(c_int), c_vp]),
 }

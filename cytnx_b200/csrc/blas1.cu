@@ -120,6 +120,28 @@ __global__ void __launch_bounds__(RT) k_lanczos_update(double *__restrict__ w, c
   finish(s, partials, ticket, nrm, 1);
 }
 
+// w -= alpha*p1 + beta*p0 + gamma*q, ||w|| to *nrm (p0 / q may be null)
+__global__ void __launch_bounds__(RT) k_lanczos_update3(double *__restrict__ w, const double *__restrict__ p1,
+                                                       const double *__restrict__ p0, const double *__restrict__ q,
+                                                       int64_t n, const double *alpha, const double *beta,
+                                                       const double *gamma, double *partials, unsigned *ticket,
+                                                       double *nrm) {
+  const double a = *alpha;
+  const double b = p0 ? *beta : 0.0;
+  const double c = q ? *gamma : 0.0;
+  double s = 0.0;
+  const int64_t step = (int64_t)gridDim.x * RT;
+  for (int64_t i = (int64_t)blockIdx.x * RT + threadIdx.x; i < n; i += step) {
+    double v = w[i] - a * p1[i];
+    if (p0) v -= b * p0[i];
+    if (q) v -= c * q[i];
+    w[i] = v;
+    s = fma(v, v, s);
+  }
+  s = block_sum(s);
+  finish(s, partials, ticket, nrm, 1);
+}
+
 // y = x / *a
 __global__ void __launch_bounds__(RT) k_div_copy(const double *__restrict__ x, double *__restrict__ y,
                                                 int64_t n, const double *a) {
@@ -181,6 +203,15 @@ ctn_status lanczos_update_f64(double *w, const double *p1, const double *p0, int
                               const double *beta, double *nrm, double *ws, cudaStream_t st) {
   int g = grid_for(n);
   k_lanczos_update<<<g, RT, 0, st>>>(w, p1, p0, n, alpha, beta, ws, reinterpret_cast<unsigned *>(ws + MAXCTA), nrm);
+  CTN_CHECK_LAUNCH();
+  return CTN_OK;
+}
+ctn_status lanczos_update3_f64(double *w, const double *p1, const double *p0, const double *q, int64_t n,
+                               const double *alpha, const double *beta, const double *gamma, double *nrm, double *ws,
+                               cudaStream_t st) {
+  const int g = std::min(grid_for(n), MAXCTA);
+  k_lanczos_update3<<<g, RT, 0, st>>>(w, p1, p0, q, n, alpha, beta, gamma, ws,
+                                      reinterpret_cast<unsigned *>(ws + MAXCTA), nrm);
   CTN_CHECK_LAUNCH();
   return CTN_OK;
 }

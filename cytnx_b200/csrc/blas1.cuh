@@ -11,6 +11,9 @@ ctn_status axpy_f64(const double *x, double *y, int64_t n, const double *a, doub
 ctn_status scal_f64(double *x, int64_t n, const double *a, int invert, cudaStream_t st);
 ctn_status lanczos_update_f64(double *w, const double *p1, const double *p0, int64_t n, const double *alpha,
                               const double *beta, double *nrm, double *ws, cudaStream_t st);
+ctn_status lanczos_update3_f64(double *w, const double *p1, const double *p0, const double *q, int64_t n,
+                               const double *alpha, const double *beta, const double *gamma, double *nrm, double *ws,
+                               cudaStream_t st);
 ctn_status div_copy_f64(const double *x, double *y, int64_t n, const double *a, cudaStream_t st);
 ctn_status combine_f64(const double *K, int64_t n, int m, const double *c, double *out, cudaStream_t st);
 }  // namespace ctn

@@ -241,6 +241,109 @@ ctn_status lanczos_gnd(int (*mv)(void *, const double *, double *, void *), void
 }
 }  // namespace ctn
 
+namespace ctn {
+// Restarted ground-state Lanczos with a low-precision matvec and one FP64 refinement
+// matvec per restart.  Each cycle starts from the current unit vector q0 = v:
+//   w = H_hi q0 (FP64): theta = <q0, w>, r = w - theta q0, rho = |r|  -- the FP64
+//   Rayleigh quotient and eigen-residual of v; stop when rho <= tol * |theta|;
+//   q1 = r / rho, then q_{j+1} from w = H_lo q_j with the three-term recurrence and an
+//   FP64 re-orthogonalisation of w against q0 at every step;
+//   the (krydim x krydim) tridiagonal T is solved in FP64 and v <- normalised sum y_j q_j.
+// The low-precision products only ever act on the correction directions q_j (j >= 1),
+// whose weight in v shrinks with rho, so the FP64 residual keeps falling below the
+// matvec error.  Returned energy and residual are the FP64 Rayleigh quotient and |r| of
+// the returned vector (measured by the last FP64 matvec).
+ctn_status lanczos_refined(int (*mv_lo)(void *, const double *, double *, void *), void *u_lo,
+                           int (*mv_hi)(void *, const double *, double *, void *), void *u_hi, const double *psi0,
+                           int64_t n, int krydim, int max_restarts, double tol, double *krylov, double *work,
+                           double *eigvec, double *energy, double *residual, int *restarts, int64_t *counts,
+                           cudaStream_t st) {
+  CTN_REQUIRE(krydim >= 2 && max_restarts >= 1 && n > 0 && tol >= 0, "[Lanczos refined] bad argument");
+  double *w = work;
+  double *scal = work + n;  // [1] alpha [2] beta_prev [3] |w| [4] gamma (overlap with q0) [0] norm
+  double *ws = work + n + 8;
+  double *cdev = ws + reduce_ws_bytes() / sizeof(double);
+  CTN_CUDA(cudaMemsetAsync(ws, 0, reduce_ws_bytes(), st));
+  double host = 0.0;
+  auto fetch = [&](int idx, double *dst) -> ctn_status {
+    CTN_CUDA(cudaMemcpyAsync(dst, scal + idx, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CTN_CUDA(cudaStreamSynchronize(st));
+    return CTN_OK;
+  };
+  int64_t n_lo = 0, n_hi = 0;
+  CTN_TRY(nrm2_f64(psi0, n, scal + 0, ws, st));
+  CTN_TRY(fetch(0, &host));
+  CTN_REQUIRE(host > 0 && std::isfinite(host), "[Lanczos refined] initial vector has zero or non-finite norm");
+  CTN_TRY(div_copy_f64(psi0, krylov, n, scal + 0, st));
+  double theta = 0.0, rho = 0.0;
+  int c = 0;
+  std::vector<double> As, Bs, evals, evecs;
+  for (c = 0; c < max_restarts; ++c) {
+    double *q0 = krylov;
+    if (mv_hi(u_hi, q0, w, st) != 0) return CTN_ERR_CUDA;
+    ++n_hi;
+    CTN_TRY(dot_f64(w, q0, n, scal + 1, ws, st));
+    CTN_TRY(lanczos_update_f64(w, q0, nullptr, n, scal + 1, scal + 2, scal + 3, ws, st));
+    CTN_TRY(fetch(1, &theta));
+    CTN_TRY(fetch(3, &rho));
+    CTN_REQUIRE(std::isfinite(theta) && std::isfinite(rho), "[Lanczos refined] non-finite Rayleigh quotient");
+    if (rho <= tol * std::fabs(theta) || rho == 0.0 || c == max_restarts - 1) break;
+    As.assign(1, theta);
+    Bs.assign(1, rho);
+    CTN_CUDA(cudaMemcpyAsync(scal + 2, &rho, sizeof(double), cudaMemcpyHostToDevice, st));
+    CTN_TRY(div_copy_f64(w, krylov + n, n, scal + 3, st));
+    for (int j = 1; j < krydim; ++j) {
+      const double *qj = krylov + (int64_t)j * n;
+      const double *qp = krylov + (int64_t)(j - 1) * n;
+      if (mv_lo(u_lo, qj, w, st) != 0) return CTN_ERR_CUDA;
+      ++n_lo;
+      CTN_TRY(dot_f64(w, qj, n, scal + 1, ws, st));
+      CTN_TRY(dot_f64(w, q0, n, scal + 4, ws, st));
+      if (j == 1)  // q_{j-1} is q0: its measured overlap replaces beta
+        CTN_TRY(lanczos_update3_f64(w, qj, q0, nullptr, n, scal + 1, scal + 4, nullptr, scal + 3, ws, st));
+      else
+        CTN_TRY(lanczos_update3_f64(w, qj, qp, q0, n, scal + 1, scal + 2, scal + 4, scal + 3, ws, st));
+      double alpha = 0.0, beta = 0.0;
+      CTN_TRY(fetch(1, &alpha));
+      CTN_TRY(fetch(3, &beta));
+      As.push_back(alpha);
+      if (j == krydim - 1 || beta == 0.0 || !std::isfinite(beta)) break;
+      Bs.push_back(beta);
+      CTN_CUDA(cudaMemcpyAsync(scal + 2, &beta, sizeof(double), cudaMemcpyHostToDevice, st));
+      CTN_TRY(div_copy_f64(w, krylov + (int64_t)(j + 1) * n, n, scal + 3, st));
+    }
+    const int m = (int)As.size();
+    evals.assign(m, 0.0);
+    evecs.assign((size_t)m * m, 0.0);
+    CTN_TRY(tql(m, As.data(), Bs.data(), evals.data(), evecs.data()));
+    CTN_CUDA(cudaMemcpyAsync(cdev, evecs.data(), sizeof(double) * m, cudaMemcpyHostToDevice, st));
+    CTN_TRY(combine_f64(krylov, n, m, cdev, w, st));
+    CTN_TRY(nrm2_f64(w, n, scal + 0, ws, st));
+    CTN_TRY(div_copy_f64(w, krylov, n, scal + 0, st));
+  }
+  CTN_CUDA(cudaMemcpyAsync(eigvec, krylov, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  CTN_CUDA(cudaStreamSynchronize(st));
+  *energy = theta;
+  if (residual) *residual = rho;
+  if (restarts) *restarts = c;
+  if (counts) {
+    counts[0] = n_lo;
+    counts[1] = n_hi;
+  }
+  return CTN_OK;
+}
+}  // namespace ctn
+
+extern "C" ctn_status ctn_lanczos_refined(ctn_matvec_fn matvec_lo, void *user_lo, ctn_matvec_fn matvec_hi,
+                                          void *user_hi, const double *psi0, int64_t n, int krydim, int max_restarts,
+                                          double tol, double *krylov, double *work, double *eigvec, double *energy,
+                                          double *residual, int *restarts, int64_t *matvecs, void *stream) {
+  CTN_REQUIRE(matvec_lo && matvec_hi && psi0 && krylov && work && eigvec && energy,
+              "ctn_lanczos_refined: null argument");
+  return ctn::lanczos_refined(matvec_lo, user_lo, matvec_hi, user_hi, psi0, n, krydim, max_restarts, tol, krylov,
+                              work, eigvec, energy, residual, restarts, matvecs, ctn::as_stream(stream));
+}
+
 extern "C" ctn_status ctn_lanczos_gnd(ctn_matvec_fn matvec, void *user, const double *psi0, int64_t n, int maxiter,
                                       double cvgcrit, double *krylov, double *work, double *eigvec, double *energy,
                                       int *iters, void *stream) {

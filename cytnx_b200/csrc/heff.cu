@@ -448,6 +448,17 @@ extern "C" ctn_status ctn_heff2_lanczos_gnd(ctn_heff2_plan *plan, int precision,
                          iters, stream);
 }
 
+extern "C" ctn_status ctn_heff2_lanczos_refined(ctn_heff2_plan *plan, int precision, const double *psi0, int krydim,
+                                                int max_restarts, double tol, double *krylov, double *work,
+                                                double *eigvec, double *energy, double *residual, int *restarts,
+                                                int64_t *matvecs, void *stream) {
+  CTN_REQUIRE(plan && plan->bound, "ctn_heff2_lanczos_refined: the FP64 environments must be bound (ctn_heff2_set_env "
+                                   "with CTN_PREC_F64) for the refinement matvecs");
+  HeffUser lo{plan, precision}, hi{plan, CTN_PREC_F64};
+  return ctn_lanczos_refined(heff_mv, &lo, heff_mv, &hi, psi0, plan->psi_elems, krydim, max_restarts, tol, krylov,
+                             work, eigvec, energy, residual, restarts, matvecs, stream);
+}
+
 extern "C" ctn_status ctn_heff2_profile(ctn_heff2_plan *p, const double *psi, double *out, int precision, int reps,
                                         double *ms_out, int *launches_out, void *stream) {
   CTN_REQUIRE(p && reps > 0 && ms_out, "ctn_heff2_profile: bad argument");

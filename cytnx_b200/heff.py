@@ -176,6 +176,33 @@ class TwoSiteHeff(LinOp):
         vec = UniTensor._new_block(self.out_bonds, psi0.labels(), psi0.rowrank(), self.out_layout, [0, 1, 2, 3], eig)
         return e.value, vec, it.value
 
+    def lanczos_refined(self, psi0: UniTensor, precision: Optional[str] = None, krylov_dim: int = 20,
+                        max_restarts: int = 200, tol: float = 1e-12) -> dict:
+        """Restarted Lanczos: Krylov steps in ``precision``, one FP64 refinement matvec per
+        restart (ctn_heff2_lanczos_refined).  Returns the FP64 Rayleigh quotient
+        ``energy`` of the returned unit vector ``vec``, its FP64 eigen-residual
+        ``residual`` = |H v - E v|, and the numbers of restarts and matvecs."""
+        prec = _lib.PRECISIONS[(precision or self.precision).lower()]
+        self.bind(precision)
+        self.bind("fp64")
+        x0 = psi0.contiguous().flat_view()
+        n = self.n
+        krylov = torch.empty(krylov_dim * n, dtype=torch.float64, device=x0.device)
+        work = torch.empty(n + 8 + 1032 + krylov_dim + 64, dtype=torch.float64, device=x0.device)
+        eig = torch.empty(n, dtype=torch.float64, device=x0.device)
+        e, r = ctypes.c_double(), ctypes.c_double()
+        rs = ctypes.c_int()
+        cnt = np.zeros(2, dtype=np.int64)
+        _lib.check(_lib.lib().ctn_heff2_lanczos_refined(self._h, prec, x0.data_ptr(), int(krylov_dim),
+                                                        int(max_restarts), float(tol), krylov.data_ptr(),
+                                                        work.data_ptr(), eig.data_ptr(), ctypes.byref(e),
+                                                        ctypes.byref(r), ctypes.byref(rs),
+                                                        cnt.ctypes.data_as(_lib.P_i64), _lib.stream_ptr()),
+                   "TwoSiteHeff.lanczos_refined")
+        vec = UniTensor._new_block(self.out_bonds, psi0.labels(), psi0.rowrank(), self.out_layout, [0, 1, 2, 3], eig)
+        return {"energy": e.value, "vec": vec, "residual": r.value, "restarts": rs.value,
+                "matvecs_lo": int(cnt[0]), "matvecs_fp64": int(cnt[1])}
+
     # ---------------------------------------------------------------- accounting
     def algorithmic_flops(self) -> float:
         """Flops of the reference's block-pair GEMMs for one matvec in the order

@@ -283,6 +283,26 @@ typedef int (*ctn_matvec_fn)(void *user, const double *x, double *y, void *strea
 ctn_status ctn_lanczos_gnd(ctn_matvec_fn matvec, void *user, const double *psi0, int64_t n,
                            int maxiter, double cvgcrit, double *krylov, double *work,
                            double *eigvec, double *energy, int *iters, void *stream);
+/* Restarted ground-state Lanczos with two matvecs: matvec_lo (e.g. split precision) builds
+ * the Krylov space of each cycle, matvec_hi (FP64) is applied once per restart to the
+ * current vector to give its FP64 Rayleigh quotient and eigen-residual r = Hv - Ev.  Each
+ * cycle: q0 = v, q1 = r/|r|, krydim - 1 low-precision steps with three-term recurrence and
+ * an FP64 re-orthogonalisation against q0, FP64 tridiagonal solve, v <- Ritz vector.  Stops
+ * when |r| <= tol * |E| or after max_restarts FP64 matvecs.  krylov: krydim * n doubles;
+ * work >= n + 8 + 1032 + krydim + 64 doubles.  *energy / *residual: FP64 Rayleigh quotient
+ * and |r| of the returned unit vector; matvecs[0..1] = low / FP64 products used.
+ * No direct counterpart in the reference (its Lanczos_ER restarts in one precision,
+ * src/linalg/Lanczos_ER.cpp); the recurrence is that of Lanczos_Gnd_Ut. */
+ctn_status ctn_lanczos_refined(ctn_matvec_fn matvec_lo, void *user_lo, ctn_matvec_fn matvec_hi,
+                               void *user_hi, const double *psi0, int64_t n, int krydim, int max_restarts,
+                               double tol, double *krylov, double *work, double *eigvec, double *energy,
+                               double *residual, int *restarts, int64_t *matvecs, void *stream);
+/* the same on a planned H_eff: `precision` for the Krylov steps, FP64 for the refinement
+ * (both must be bound with ctn_heff2_set_env) */
+ctn_status ctn_heff2_lanczos_refined(ctn_heff2_plan *plan, int precision, const double *psi0, int krydim,
+                                     int max_restarts, double tol, double *krylov, double *work,
+                                     double *eigvec, double *energy, double *residual, int *restarts,
+                                     int64_t *matvecs, void *stream);
 /* the same driver on a planned H_eff (no callback) */
 ctn_status ctn_heff2_lanczos_gnd(ctn_heff2_plan *plan, int precision, const double *psi0,
                                  int maxiter, double cvgcrit, double *krylov, double *work,

@@ -167,3 +167,26 @@ def test_lanczos_dense_arange_golden():
 
     E, v = c.linalg.Lanczos(Op("mv", 27), c.arange(27, device=0), "Gnd", 9.999999999999999988e-15, 10000)
     assert abs(E.item() - (-1628.9964650426593)) < 1e-5
+
+
+@pytest.mark.parametrize("form", ["bf16x3", "3xtf32"])
+def test_refined_lanczos_reaches_fp64_energy(form):
+    """Split-precision Krylov steps with one FP64 refinement matvec per restart converge to
+    the FP64 ground-state energy (same driver run in FP64) far below the matvec error."""
+    import cytnx_b200 as c
+
+    psi, L, M1, M2, R = build(128, seed=2)
+    H = c.TwoSiteHeff(L, M1, M2, R, psi)
+    ref = H.lanczos_refined(psi, precision="fp64", krylov_dim=24, max_restarts=400, tol=1e-11)
+    got = H.lanczos_refined(psi, precision=form, krylov_dim=24, max_restarts=400, tol=1e-11)
+    E64, E = ref["energy"], got["energy"]
+    assert ref["residual"] <= 1e-11 * abs(E64)
+    assert got["residual"] <= 1e-11 * abs(E)  # FP64 eigen-residual of the split-form vector
+    assert abs(E - E64) / abs(E64) < 1e-10
+    assert got["matvecs_fp64"] == got["restarts"] + 1
+    # the returned energy is the FP64 Rayleigh quotient of the returned vector
+    v = got["vec"].flat_view()
+    hv = torch.empty_like(v)
+    H.apply_flat(v, hv, "fp64")
+    assert abs(float(torch.dot(v, hv)) - E) < 1e-12 * abs(E)
+    assert abs(float(torch.linalg.vector_norm(hv - E * v)) - got["residual"]) < 1e-9 * abs(E)
