@@ -123,3 +123,29 @@ def test_batch_planning_host_only(prec):
     # tile widths are validated before any table is built
     with pytest.raises(Exception):
         B._create(100, 64)
+
+
+def test_mps_bond_sectors():
+    from cytnx_b200.autodiff import mps_bond_sectors
+
+    for L, Dmax in ((32, 512), (10, 16), (8, 1000)):
+        for k in range(L + 1):
+            q, d = mps_bond_sectors(L, k, Dmax)
+            assert d.sum() <= Dmax and (d > 0).all()
+            assert ((q + k) % 2 == 0).all() and (np.abs(q) <= min(k, L - k)).all()
+        q0, d0 = mps_bond_sectors(L, 0, Dmax)
+        qL, dL = mps_bond_sectors(L, L, Dmax)
+        assert q0.tolist() == [0] and d0.tolist() == [1] and qL.tolist() == [0] and dL.tolist() == [1]
+    # no cap binds: exact Schmidt dimensions
+    q, d = mps_bond_sectors(8, 4, 1000)
+    assert dict(zip(q.tolist(), d.tolist())) == {-4: 1, -2: 4, 0: 6, 2: 4, 4: 1}
+
+
+def test_redirected_bonds_keep_the_block_layout():
+    from cytnx_b200.unitensor import layout_for
+
+    spec = W.xxz_spec(64)
+    Vl, Vr, phys, inner = W.spec_bonds(spec)
+    bonds = [inner.redirect(), Vl.redirect(), Vl]
+    a, b = layout_for(bonds), layout_for([x.redirect() for x in bonds])
+    assert np.array_equal(a.itoi, b.itoi) and np.array_equal(a.offs, b.offs)
