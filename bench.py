@@ -49,6 +49,13 @@ def parse():
     ap.add_argument("--lanczos-iters", type=int, default=40)
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--precision", default="bf16x3", help="headline arithmetic form: bf16x3, 3xtf32 or fp64")
+    ap.add_argument("--matvec-only", action="store_true",
+                    help="profiling driver: bind the headline form with --tiles, run warmup + steps matvecs, exit")
+    ap.add_argument("--tiles", default="", help="step-1,step-4 tile widths for --matvec-only (e.g. 192,128)")
+    ap.add_argument("--batch-only", type=int, default=0,
+                    help="profiling driver: the first N batched Hubbard problems, headline form, --tiles, eager matvecs")
+    ap.add_argument("--mps-lbfgs-steps", type=int, default=200,
+                    help="differentiable U(1) MPS section (L=32, D=512): L-BFGS steps (0 skips it)")
     ap.add_argument("--batch-problems", type=int, default=256,
                     help="batched Hubbard section: number of two-site problems (0 skips it)")
     return ap.parse_args()
@@ -170,6 +177,24 @@ def main():
 
     from cytnx_b200 import workloads as W
 
+    if args.batch_only > 0:  # small fixed launch sequence of the batched path for ncu
+        from cytnx_b200.batch import BatchedTwoSiteHeff
+
+        dims = W.hubbard_batch_dims(256, seed=0)[: args.batch_only]
+        probs = W.hubbard_batch(dims)
+        data = [W.problem_data(p, 1000 + i) for i, p in enumerate(probs)]
+        tiles = tuple(int(t) for t in args.tiles.split(",")) if args.tiles else (128, 48)
+        B = BatchedTwoSiteHeff(probs, args.precision, tiles=tiles)
+        B.set_env(B.gather([d[0] for d in data], "L"), B.gather([d[1] for d in data], "R"))
+        x = B.gather([d[2] for d in data], "psi")
+        y = torch.zeros_like(x)
+        for _ in range(args.warmup + args.steps):
+            B.matvec(x, y)
+        torch.cuda.synchronize()
+        print(json.dumps({"batch_only": args.batch_only, "precision": args.precision, "tiles": list(tiles),
+                          "workspace_gb": B.workspace_bytes() / 1e9, "out_norm": float(y.norm())}), flush=True)
+        return
+
     spec = W.xxz_spec(args.D)
     mpo_vals = W.xxz_mpo_values(1.0, 1.0, 0.0)
     workload = f"u1_xxz_two_site_heff_D{args.D}"
@@ -208,6 +233,21 @@ def main():
     st = torch.cuda.current_stream()
     psi, L, M1, M2, R = W.build_two_site(spec, mpo_vals, seed=0, device=local)
     H = c.TwoSiteHeff(L, M1, M2, R, psi, precision=args.precision)
+    if args.matvec_only:  # small fixed launch sequence for ncu: no autotuning, no other sections
+        if args.tiles and args.precision != "fp64":
+            b1, b4 = (int(t) for t in args.tiles.split(","))
+            H.set_tiles(b1, b4, args.precision)
+        x = psi.flat_view()
+        y = torch.empty_like(x)
+        for _ in range(args.warmup + args.steps):
+            H.apply_flat(x, y, args.precision)
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"matvec_only": True, "precision": args.precision, "D": args.D, "tiles": args.tiles,
+                              "matvecs": args.warmup + args.steps, "out_norm": float(y.norm())}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
     flops = H.algorithmic_flops()
     tiles = {f: H.autotune(f) for f in ("bf16x3", "3xtf32")}
     x = psi.flat_view()
@@ -361,6 +401,7 @@ def main():
                  "kernel_flops_per_matvec": g_flops, "kernel_ms_per_matvec": g_ms})
     clocks = sampler.summary()
     batched = run_batched(args, world, rank, dev, st) if args.batch_problems > 0 else None
+    mps_ad = run_mps_autograd(args, dev) if args.mps_lbfgs_steps > 0 else None
     if rank == 0:
         cpu = None
         if world == 1 and os.environ.get("CTN_BENCH_NO_CPU") != "1":
@@ -395,6 +436,7 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cpu,
             "batched_hubbard": batched,
+            "autograd_mps": mps_ad,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -476,6 +518,78 @@ def run_batched(args, world, rank, dev, st):
         rec["rel_err_vs_fp64_median_rank0"] = float(e.median().item())
         del rec["_B"], rec["_y"]
     out["setup_s"] = time.perf_counter() - t_setup
+    return out
+
+
+def run_mps_autograd(args, dev):
+    """Differentiation variant: finite U(1) MPS, L=32, D=512, d=2, XXZ MPO; energy
+    <A|H|A>/<A|A> through block-sparse contractions with the hand-written adjoint,
+    environments checkpointed every 4 sites; gradient checks, then L-BFGS."""
+    import torch
+
+    from cytnx_b200.autodiff import U1MPS
+
+    L, D = 32, 512
+    t_setup = time.perf_counter()
+    mps = U1MPS(L, D, seed=0, device=dev)
+    out = {"L": L, "D": D, "d": 2, "model": "XXZ Jz=1 Jxy=1 h=0", "params": mps.numel(), "checkpoint_every": 4}
+    for ce in (4, 0):  # warm both forms, then time one energy + gradient each and record peak memory
+        E = mps.energy(checkpoint_every=ce)
+        torch.autograd.grad(E, mps.params)
+        torch.cuda.synchronize()
+        torch.cuda.reset_peak_memory_stats(dev)
+        t0 = time.perf_counter()
+        E = mps.energy(checkpoint_every=ce)
+        g = torch.autograd.grad(E, mps.params)
+        torch.cuda.synchronize()
+        out[f"eval_grad_s_ckpt{ce}"] = time.perf_counter() - t0
+        out[f"peak_mem_mb_ckpt{ce}"] = torch.cuda.max_memory_allocated(dev) / 1e6
+    flat_g = torch.cat([x.reshape(-1) for x in g])
+    sizes = [p.numel() for p in mps.params]
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    rng = np.random.default_rng(7)
+    h, worst = 1e-6, 0.0
+    for gi in rng.choice(int(offs[-1]), 64, replace=False):
+        k = int(np.searchsorted(offs, gi, side="right") - 1)
+        i = int(gi - offs[k])
+        with torch.no_grad():
+            ps = [p.detach() for p in mps.params]
+            xp, xm = ps[k].clone(), ps[k].clone()
+            xp[i] += h
+            xm[i] -= h
+            fd = float((mps.energy([*ps[:k], xp, *ps[k + 1:]], checkpoint_every=0) -
+                        mps.energy([*ps[:k], xm, *ps[k + 1:]], checkpoint_every=0)) / (2 * h))
+        worst = max(worst, abs(fd - float(flat_g[gi])))
+    out["fd_check"] = {"entries": 64, "h": h, "max_abs_err": worst, "max_abs_grad": float(flat_g.abs().max())}
+    num = mps.energy(checkpoint_every=4, numerator_only=True)
+    gnum = torch.autograd.grad(num, mps.params)
+    errs = []
+    for k in (0, L // 2, L - 1):
+        ref = 2.0 * mps.heff_times_site(k)
+        errs.append(float(torch.linalg.vector_norm(gnum[k] - ref) / torch.linalg.vector_norm(ref)))
+    out["grad_vs_2HeffA_rel_err_max"] = max(errs)
+    if args.mps_lbfgs_steps > 0:
+        x = torch.cat([p.detach().reshape(-1) for p in mps.params]).clone().requires_grad_(True)
+        opt = torch.optim.LBFGS([x], lr=1.0, max_iter=args.mps_lbfgs_steps, history_size=30,
+                                line_search_fn="strong_wolfe", tolerance_grad=1e-14, tolerance_change=1e-16)
+        hist = []
+
+        def closure():
+            opt.zero_grad()
+            e = mps.energy(list(torch.split(x, sizes)), checkpoint_every=4)
+            e.backward()
+            hist.append(float(e.detach()))
+            return e
+
+        t0 = time.perf_counter()
+        opt.step(closure)
+        torch.cuda.synchronize()
+        st = opt.state[opt._params[0]]
+        out["lbfgs"] = {"steps": int(st.get("n_iter", 0)), "energy_evals": int(st.get("func_evals", len(hist))),
+                        "seconds": time.perf_counter() - t0, "energy_initial": hist[0], "energy_final": hist[-1],
+                        "energy_per_site_final": hist[-1] / L,
+                        "trace_every_20": hist[::20]}
+    out["setup_and_checks_s"] = time.perf_counter() - t_setup
     return out
 
 
