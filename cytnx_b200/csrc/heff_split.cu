@@ -52,7 +52,7 @@ struct HeffSplit {
   Packer pk_L, pk_P, pk_R;
   std::vector<MpoSegS> segs;
   std::vector<MpoTermS> terms;
-  std::vector<int64_t> seg_begin;
+  std::vector<int64_t> seg_begin;  // chunk prefix sums per segment
   int64_t nchunks = 0;
   void *d_mpo = nullptr;
   int d_dev = -1;
@@ -114,9 +114,8 @@ struct MpoSParams {
 };
 
 constexpr int MPO_THREADS = 256;
-constexpr int MPO_UNROLL = 2;
+constexpr int MPO_UNROLL = 1;
 constexpr int MPO_ITEM = MPO_THREADS * MPO_UNROLL;  // chunks per work item
-constexpr int MPO_MAXT = 32;                        // terms staged in shared memory
 
 // round-to-nearest (ties away) to TF32 / round-to-nearest-even to BF16 with integer ops
 // (ALU pipe; the conversion unit is the bottleneck of a cvt-based version)
@@ -128,96 +127,105 @@ __device__ __forceinline__ uint32_t bf16_rne_bits(float x) {
   return (u + 0x7FFFu + ((u >> 16) & 1u)) >> 16;
 }
 
-// One CTA per work item of MPO_ITEM consecutive 16-byte chunks.  An item inside one X3
-// block stages the block's term list in shared memory; an item spanning several small
-// blocks lets each thread find its block by a binary search over the blocks the item
-// overlaps and reads the terms through the read-only cache.  Every thread computes
-// MPO_UNROLL chunks in FP32 (X1 is FP32) and splits them into hi/lo panel chunks.
+// One CTA per work item of MPO_ITEM consecutive chunks (E = 4 TF32 / 8 BF16 elements of
+// one row) of the flattened X3 blocks; an item may span several small blocks (each
+// thread finds its block by a binary search over the blocks the item overlaps).  Blocks
+// are ordered by (a', b), so the blocks that read the same X1 inputs run together and
+// share them in L2.  X1 block rows start on 16-byte boundaries (padded step-1 columns),
+// so full chunks load as float4, four terms per round.
 __global__ void __launch_bounds__(MPO_THREADS) k_mpo_split(MpoSParams p) {
-  __shared__ MpoTermS sterm[MPO_MAXT];
-  __shared__ float scoef[MPO_MAXT];
   const bool tf32 = p.kind == TC_TF32;
   const int E = tf32 ? 4 : 8;
   for (int64_t it = blockIdx.x; it < p.nitems; it += gridDim.x) {
     const WorkItem wi = p.items[it];
-    const bool single = wi.seg0 == wi.seg1;  // uniform over the CTA
-    __syncthreads();
-    if (single) {
-      const MpoSegS s0 = p.segs[wi.seg0];
-      if (threadIdx.x < MPO_MAXT && threadIdx.x < s0.term_count) {
-        sterm[threadIdx.x] = p.terms[s0.term_begin + threadIdx.x];
-        scoef[threadIdx.x] = (float)p.terms[s0.term_begin + threadIdx.x].coef;
-      }
-    }
-    __syncthreads();
-#pragma unroll
+#pragma unroll 1
     for (int j = 0; j < MPO_UNROLL; ++j) {
       const int64_t g = wi.chunk0 + threadIdx.x + j * MPO_THREADS;
       if (g >= p.nchunks) break;
-      int si = wi.seg0;
-      if (!single) {
-        int hi_s = wi.seg1;  // last block with begin <= g
-        while (si < hi_s) {
-          const int mid = (si + hi_s + 1) >> 1;
-          if (__ldg(p.begin + mid) <= g) si = mid;
-          else hi_s = mid - 1;
-        }
+      int si = wi.seg0, hi_s = wi.seg1;  // last block with begin <= g
+      while (si < hi_s) {
+        const int mid = (si + hi_s + 1) >> 1;
+        if (__ldg(p.begin + mid) <= g) si = mid;
+        else hi_s = mid - 1;
       }
       const MpoSegS s = p.segs[si];
-      const int nt = s.term_count;
       const int nkc = (s.cols + E - 1) / E;
       const int cl = (int)(g - __ldg(p.begin + si));
       const int r = cl / nkc;
       const int kloc = (cl - r * nkc) * E;
       const int nvalid = min(E, s.cols - kloc);
-      float x[8];
+      {
+        float x[8];
 #pragma unroll
-      for (int e = 0; e < 8; ++e) x[e] = 0.f;
-      for (int t = 0; t < nt; ++t) {
-        const bool st = single && t < MPO_MAXT;
-        const MpoTermS tm = st ? sterm[t] : p.terms[s.term_begin + t];
-        const float cf = st ? scoef[t] : (float)tm.coef;
-        const float *src = p.x1 + tm.x1_off + (int64_t)r * tm.ld + kloc;
-        if (nvalid == E && tf32 && ((reinterpret_cast<uintptr_t>(src) & 15) == 0)) {
-          const float4 v = __ldg(reinterpret_cast<const float4 *>(src));
-          x[0] = fmaf(cf, v.x, x[0]);
-          x[1] = fmaf(cf, v.y, x[1]);
-          x[2] = fmaf(cf, v.z, x[2]);
-          x[3] = fmaf(cf, v.w, x[3]);
+        for (int e = 0; e < 8; ++e) x[e] = 0.f;
+        if (nvalid == E) {
+          // four terms per round: their loads are issued together (memory-level parallelism)
+          for (int t0 = 0; t0 < s.term_count; t0 += 4) {
+            float4 v[4], w[4];
+            float cf[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              v[u] = w[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+              cf[u] = 0.f;
+              if (t0 + u < s.term_count) {
+                const MpoTermS tm = p.terms[s.term_begin + t0 + u];
+                cf[u] = (float)tm.coef;
+                const float4 *src = reinterpret_cast<const float4 *>(p.x1 + tm.x1_off + (int64_t)r * tm.ld + kloc);
+                v[u] = __ldg(src);
+                if (!tf32) w[u] = __ldg(src + 1);
+              }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              x[0] = fmaf(cf[u], v[u].x, x[0]);
+              x[1] = fmaf(cf[u], v[u].y, x[1]);
+              x[2] = fmaf(cf[u], v[u].z, x[2]);
+              x[3] = fmaf(cf[u], v[u].w, x[3]);
+              x[4] = fmaf(cf[u], w[u].x, x[4]);
+              x[5] = fmaf(cf[u], w[u].y, x[5]);
+              x[6] = fmaf(cf[u], w[u].z, x[6]);
+              x[7] = fmaf(cf[u], w[u].w, x[7]);
+            }
+          }
         } else {
+          for (int t = 0; t < s.term_count; ++t) {
+            const MpoTermS tm = p.terms[s.term_begin + t];
+            const float cf = (float)tm.coef;
+            const float *src = p.x1 + tm.x1_off + (int64_t)r * tm.ld + kloc;
 #pragma unroll
-          for (int e = 0; e < 8; ++e)
-            if (e < nvalid) x[e] = fmaf(cf, __ldg(src + e), x[e]);
+            for (int e = 0; e < 8; ++e)
+              if (e < nvalid) x[e] = fmaf(cf, __ldg(src + e), x[e]);
+          }
         }
+        // panel offset (32-bit index math except the final byte offset)
+        const int row = s.row0 + r, kabs = s.k0 + kloc;
+        const int rr = row & (TC_BM - 1);
+        const int kslice = tf32 ? (kabs >> 5) : (kabs >> 6);
+        const int byte = tf32 ? ((kabs & 31) << 2) : ((kabs & 63) << 1);
+        const int64_t off = s.panel_off + ((int64_t)(row >> 7) * s.kb + kslice) * TC_A_TILE + (rr >> 3) * 1024 +
+                            (rr & 7) * 128 + (((byte >> 4) ^ (rr & 7)) << 4);
+        if (tf32) {
+          float h[4], l[4];
+  #pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            h[e] = tf32_rna(x[e]);
+            l[e] = tf32_rna(x[e] - h[e]);  // exact in FP32
+          }
+          *(float4 *)(p.hi + off) = make_float4(h[0], h[1], h[2], h[3]);
+          *(float4 *)(p.lo + off) = make_float4(l[0], l[1], l[2], l[3]);
+        } else {
+          uint32_t hw[4], lw[4];
+  #pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const uint32_t h0 = bf16_rne_bits(x[2 * e]), h1 = bf16_rne_bits(x[2 * e + 1]);
+            const uint32_t l0 = bf16_rne_bits(x[2 * e] - __uint_as_float(h0 << 16));
+            const uint32_t l1 = bf16_rne_bits(x[2 * e + 1] - __uint_as_float(h1 << 16));
+            hw[e] = h0 | (h1 << 16);
+            lw[e] = l0 | (l1 << 16);
+          }
+          *(uint4 *)(p.hi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+          *(uint4 *)(p.lo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
       }
-      // panel offset (32-bit index math except the final byte offset)
-      const int row = s.row0 + r, kabs = s.k0 + kloc;
-      const int rr = row & (TC_BM - 1);
-      const int kslice = tf32 ? (kabs >> 5) : (kabs >> 6);
-      const int byte = tf32 ? ((kabs & 31) << 2) : ((kabs & 63) << 1);
-      const int64_t off = s.panel_off + ((int64_t)(row >> 7) * s.kb + kslice) * TC_A_TILE + (rr >> 3) * 1024 +
-                          (rr & 7) * 128 + (((byte >> 4) ^ (rr & 7)) << 4);
-      if (tf32) {
-        float h[4], l[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          h[e] = tf32_rna(x[e]);
-          l[e] = tf32_rna(x[e] - h[e]);  // exact in FP32
-        }
-        *(float4 *)(p.hi + off) = make_float4(h[0], h[1], h[2], h[3]);
-        *(float4 *)(p.lo + off) = make_float4(l[0], l[1], l[2], l[3]);
-      } else {
-        uint32_t hw[4], lw[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const uint32_t h0 = bf16_rne_bits(x[2 * e]), h1 = bf16_rne_bits(x[2 * e + 1]);
-          const uint32_t l0 = bf16_rne_bits(x[2 * e] - __uint_as_float(h0 << 16));
-          const uint32_t l1 = bf16_rne_bits(x[2 * e + 1] - __uint_as_float(h1 << 16));
-          hw[e] = h0 | (h1 << 16);
-          lw[e] = l0 | (l1 << 16);
-        }
-        *(uint4 *)(p.hi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-        *(uint4 *)(p.lo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
       }
     }
   }
@@ -250,9 +258,9 @@ ctn_status heff_split_prepare(ctn_heff2_plan *p, int kind) {
       l_row[l] = M;
       M += p->Lb[l].d[0] * p->Lb[l].d[2];
     }
-    for (int64_t q : jt->second) {
+    for (int64_t q : jt->second) {  // each psi block's X1 columns start on a 16-byte boundary
       p_col[q] = N;
-      N += p->Pb[q].d[1] * p->Pb[q].d[2] * p->Pb[q].d[3];
+      N = up(N + p->Pb[q].d[1] * p->Pb[q].d[2] * p->Pb[q].d[3], 4);
     }
     if (M == 0 || N == 0 || K == 0) continue;
     const int64_t ldc = up(N, 4);  // FP32 rows start on 16-byte boundaries (TMA bulk stores)
@@ -324,40 +332,49 @@ ctn_status heff_split_prepare(ctn_heff2_plan *p, int kind) {
       const BlkInfo &b = p->Ob[o];
       s->uncovered.push_back({b.off, b.d[0] * b.d[1] * b.d[2] * b.d[3]});
     }
-  // ---------------- MPO segments: X3 blocks into the step-4 A panels
+  // ---------------- MPO segments: X3 blocks into the step-4 A panels, ordered by (a', b)
+  // (the blocks of one (a', b) read the same X1 blocks)
   const int E = kind == TC_TF32 ? 4 : 8;
+  std::map<std::pair<int64_t, int64_t>, std::vector<size_t>> by_ab;
+  for (size_t i = 0; i < p->x3.size(); ++i) {
+    const X3Info &xi = p->x3[i];
+    by_ab[{p->Ob[xi.o].q[0], p->Rb[xi.r].q[1]}].push_back(i);
+  }
   s->seg_begin.push_back(0);
-  for (const X3Info &xi : p->x3) {
-    if (o_group[xi.o] < 0 || r_group[xi.r] < 0 || o_group[xi.o] != r_group[xi.r]) {
-      set_error("heff split plan: inconsistent step-4 grouping");
-      return CTN_ERR_INVALID;
-    }
-    const TcGroup &g = s->g4.groups[o_group[xi.o]];
-    MpoSegS sg;
-    sg.rows = (int32_t)xi.rows;
-    sg.cols = (int32_t)xi.cols;
-    sg.row0 = (int32_t)o_row[xi.o];
-    sg.k0 = (int32_t)r_k[xi.r];
-    sg.panel_off = g.a_off;
-    sg.kb = g.kb;
-    sg.pad_ = 0;
-    sg.term_begin = (int32_t)s->terms.size();
-    sg.term_count = (int32_t)xi.terms.size();
-    for (auto &tm : xi.terms) {
-      const int64_t l = p->x1_lp[tm.first].first, q = p->x1_lp[tm.first].second;
-      const int64_t gi = l_group[l];
-      if (gi < 0 || p_group[q] != gi) {
-        set_error("heff split plan: X1 block outside the step-1 groups");
+  for (auto &kv : by_ab) {
+    for (size_t i : kv.second) {
+      const X3Info &xi = p->x3[i];
+      if (o_group[xi.o] < 0 || r_group[xi.r] < 0 || o_group[xi.o] != r_group[xi.r]) {
+        set_error("heff split plan: inconsistent step-4 grouping");
         return CTN_ERR_INVALID;
       }
-      MpoTermS t;
-      t.ld = g1_ldc[gi];
-      t.x1_off = g1_coff[gi] + l_row[l] * t.ld + p_col[q];
-      t.coef = tm.second;
-      s->terms.push_back(t);
+      const TcGroup &g = s->g4.groups[o_group[xi.o]];
+      MpoSegS sg;
+      sg.rows = (int32_t)xi.rows;
+      sg.cols = (int32_t)xi.cols;
+      sg.row0 = (int32_t)o_row[xi.o];
+      sg.k0 = (int32_t)r_k[xi.r];
+      sg.panel_off = g.a_off;
+      sg.kb = g.kb;
+      sg.pad_ = 0;
+      sg.term_begin = (int32_t)s->terms.size();
+      sg.term_count = (int32_t)xi.terms.size();
+      for (auto &tm : xi.terms) {
+        const int64_t l = p->x1_lp[tm.first].first, q = p->x1_lp[tm.first].second;
+        const int64_t gi = l_group[l];
+        if (gi < 0 || p_group[q] != gi) {
+          set_error("heff split plan: X1 block outside the step-1 groups");
+          return CTN_ERR_INVALID;
+        }
+        MpoTermS t;
+        t.ld = g1_ldc[gi];
+        t.x1_off = g1_coff[gi] + l_row[l] * t.ld + p_col[q];
+        t.coef = tm.second;
+        s->terms.push_back(t);
+      }
+      s->segs.push_back(sg);
+      s->seg_begin.push_back(s->seg_begin.back() + (int64_t)xi.rows * ((xi.cols + E - 1) / E));
     }
-    s->segs.push_back(sg);
-    s->seg_begin.push_back(s->seg_begin.back() + (int64_t)xi.rows * ((xi.cols + E - 1) / E));
   }
   s->nchunks = s->seg_begin.back();
   chunk_items(s->seg_begin, MPO_ITEM, s->items);
@@ -433,9 +450,9 @@ ctn_status split_matvec(HeffSplit *s, const void *psi, void *out, cudaStream_t s
     const char *q = (const char *)s->d_mpo;
     prm.segs = (const MpoSegS *)q;
     prm.terms = (const MpoTermS *)(q + s->segs.size() * sizeof(MpoSegS));
-    prm.items = (const WorkItem *)(q + s->segs.size() * sizeof(MpoSegS) + s->terms.size() * sizeof(MpoTermS));
-    prm.begin = (const int64_t *)(q + s->segs.size() * sizeof(MpoSegS) + s->terms.size() * sizeof(MpoTermS) +
-                                  s->items.size() * sizeof(WorkItem));
+    const size_t o_items = s->segs.size() * sizeof(MpoSegS) + s->terms.size() * sizeof(MpoTermS);
+    prm.items = (const WorkItem *)(q + o_items);
+    prm.begin = (const int64_t *)(q + o_items + s->items.size() * sizeof(WorkItem));
     prm.nitems = (int64_t)s->items.size();
     prm.nchunks = s->nchunks;
     prm.kind = kind;
