@@ -392,12 +392,42 @@ struct PackItemParams {
   uint8_t *hi, *lo;
 };
 
+// hi/lo split of one chunk (E elements) and its two 16-byte stores
+template <int KIND>
+__device__ __forceinline__ void store_split(const double (&x)[8], uint8_t *hi, uint8_t *lo, int64_t off) {
+  if (KIND == TC_TF32) {
+    float h[4], l[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      h[e] = to_tf32((float)x[e]);
+      l[e] = to_tf32((float)(x[e] - (double)h[e]));
+    }
+    *(float4 *)(hi + off) = make_float4(h[0], h[1], h[2], h[3]);
+    *(float4 *)(lo + off) = make_float4(l[0], l[1], l[2], l[3]);
+  } else {
+    __nv_bfloat16 h[8], l[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      h[e] = __double2bfloat16(x[e]);
+      l[e] = __double2bfloat16(x[e] - (double)__bfloat162float(h[e]));
+    }
+    *(uint4 *)(hi + off) = *(uint4 *)h;
+    *(uint4 *)(lo + off) = *(uint4 *)l;
+  }
+}
+
+template <bool F32>
+__device__ __forceinline__ double load_src(const void *src, int64_t idx) {
+  return F32 ? (double)__ldg((const float *)src + idx) : __ldg((const double *)src + idx);
+}
+
 // One CTA per work item of PACK_ITEM consecutive chunks; an item may span many small
 // segments (each thread finds its own segment by a binary search over the few the item
 // overlaps), so tiny blocks do not waste CTAs.  Rows fastest inside a segment, so the
 // source reads (rows are the contiguous axis of every operand packed here) coalesce.
+template <int KIND, bool F32>
 __global__ void __launch_bounds__(PACK_THREADS) k_pack_items(PackItemParams p) {
-  const int E = p.kind == TC_TF32 ? 4 : 8;
+  constexpr int E = KIND == TC_TF32 ? 4 : 8;
   for (int64_t it = blockIdx.x; it < p.nitems; it += gridDim.x) {
     const PackItem wi = p.items[it];
 #pragma unroll
@@ -418,39 +448,20 @@ __global__ void __launch_bounds__(PACK_THREADS) k_pack_items(PackItemParams p) {
 #pragma unroll
       for (int e = 0; e < 8; ++e) {
         x[e] = 0.0;
-        if (e < E && kloc + e < s.cols) {
-          const int64_t idx = s.src_off + (int64_t)r * s.sr + (int64_t)(kloc + e) * s.sk;
-          x[e] = p.src_f32 ? (double)__ldg((const float *)p.src + idx) : __ldg((const double *)p.src + idx);
-        }
+        if (e < E && kloc + e < s.cols)
+          x[e] = load_src<F32>(p.src, s.src_off + (int64_t)r * s.sr + (int64_t)(kloc + e) * s.sk);
       }
-      const int64_t off = s.panel_off + tc_panel_offset(s.row0 + r, s.k0 + kloc, s.tile_rows, s.kb, p.kind);
-      if (p.kind == TC_TF32) {
-        float h[4], l[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          h[e] = to_tf32((float)x[e]);
-          l[e] = to_tf32((float)(x[e] - (double)h[e]));
-        }
-        *(float4 *)(p.hi + off) = make_float4(h[0], h[1], h[2], h[3]);
-        *(float4 *)(p.lo + off) = make_float4(l[0], l[1], l[2], l[3]);
-      } else {
-        __nv_bfloat16 h[8], l[8];
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          h[e] = __double2bfloat16(x[e]);
-          l[e] = __double2bfloat16(x[e] - (double)__bfloat162float(h[e]));
-        }
-        *(uint4 *)(p.hi + off) = *(uint4 *)h;
-        *(uint4 *)(p.lo + off) = *(uint4 *)l;
-      }
+      const int64_t off = s.panel_off + tc_panel_offset(s.row0 + r, s.k0 + kloc, s.tile_rows, s.kb, KIND);
+      store_split<KIND>(x, p.hi, p.lo, off);
     }
   }
 }
 
 // Transposing pack for segments whose rows are the contiguous source axis (sr == 1):
 // a CTA loads a 32-row x 32-k (TF32) or 32 x 64 (BF16) tile with coalesced reads along
-// the rows into shared memory, then each thread writes one 16-byte chunk with the 8
-// chunks of a panel row on 8 consecutive threads (whole 128-byte rows per 8 threads).
+// the rows (all of a thread's loads issued together), stages it in shared memory, then
+// each thread writes one 16-byte chunk with the 8 chunks of a panel row on 8 consecutive
+// threads (whole 128-byte rows per 8 threads).
 using PackTileItem = PackTileItemH;  // rows r0..r0+31, local k chunks kc0..kc0+7
 struct PackTileParams {
   const PackSeg *segs;
@@ -462,50 +473,40 @@ struct PackTileParams {
   uint8_t *hi, *lo;
 };
 
+template <int KIND, bool F32>
 __global__ void __launch_bounds__(256) k_pack_tile(PackTileParams p) {
-  __shared__ double T[64][33];
-  const int E = p.kind == TC_TF32 ? 4 : 8;
-  const int KT = 8 * E;  // k values per item: 8 chunks
+  constexpr int E = KIND == TC_TF32 ? 4 : 8;
+  constexpr int KT = 8 * E;             // k values per item: 8 chunks
+  constexpr int PER = 32 * KT / 256;    // source elements per thread
+  __shared__ double T[KT][33];
   for (int64_t it = blockIdx.x; it < p.nitems; it += gridDim.x) {
     const PackTileItem wi = p.items[it];
     const PackSeg s = p.segs[wi.seg];
     const int k0 = wi.kc0 * E;
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < 32 * KT; idx += 256) {
+    double v[PER];
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int idx = threadIdx.x + u * 256;
       const int r = idx & 31, k = idx >> 5;
-      double v = 0.0;
-      if (wi.r0 + r < s.rows && k0 + k < s.cols) {
-        const int64_t src = s.src_off + (int64_t)(wi.r0 + r) * s.sr + (int64_t)(k0 + k) * s.sk;
-        v = p.src_f32 ? (double)__ldg((const float *)p.src + src) : __ldg((const double *)p.src + src);
-      }
-      T[k][r] = v;
+      v[u] = 0.0;
+      if (wi.r0 + r < s.rows && k0 + k < s.cols)
+        v[u] = load_src<F32>(p.src, s.src_off + (int64_t)(wi.r0 + r) * s.sr + (int64_t)(k0 + k) * s.sk);
+    }
+    __syncthreads();  // the previous item's readers are done with T
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int idx = threadIdx.x + u * 256;
+      T[idx >> 5][idx & 31] = v[u];
     }
     __syncthreads();
     const int r = threadIdx.x >> 3, c = threadIdx.x & 7;
     const int kl = k0 + c * E;  // local k of this chunk
     if (wi.r0 + r >= s.rows || kl >= s.cols) continue;
-    const int64_t off = s.panel_off + tc_panel_offset(s.row0 + wi.r0 + r, s.k0 + kl, s.tile_rows, s.kb, p.kind);
-    if (p.kind == TC_TF32) {
-      float h[4], l[4];
+    const int64_t off = s.panel_off + tc_panel_offset(s.row0 + wi.r0 + r, s.k0 + kl, s.tile_rows, s.kb, KIND);
+    double x[8];
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const double x = T[c * 4 + e][r];
-        h[e] = to_tf32((float)x);
-        l[e] = to_tf32((float)(x - (double)h[e]));
-      }
-      *(float4 *)(p.hi + off) = make_float4(h[0], h[1], h[2], h[3]);
-      *(float4 *)(p.lo + off) = make_float4(l[0], l[1], l[2], l[3]);
-    } else {
-      __nv_bfloat16 h[8], l[8];
-#pragma unroll
-      for (int e = 0; e < 8; ++e) {
-        const double x = T[c * 8 + e][r];
-        h[e] = __double2bfloat16(x);
-        l[e] = __double2bfloat16(x - (double)__bfloat162float(h[e]));
-      }
-      *(uint4 *)(p.hi + off) = *(uint4 *)h;
-      *(uint4 *)(p.lo + off) = *(uint4 *)l;
-    }
+    for (int e = 0; e < 8; ++e) x[e] = e < E ? T[c * E + e][r] : 0.0;
+    store_split<KIND>(x, p.hi, p.lo, off);
   }
 }
 
@@ -742,7 +743,13 @@ ctn_status Packer::run(const void *src, int src_is_f32, uint8_t *hi, uint8_t *lo
     tp.hi = hi;
     tp.lo = lo;
     const int64_t g2 = std::min<int64_t>(tp.nitems, (int64_t)nsm_count() * 8);
-    k_pack_tile<<<(unsigned)g2, 256, 0, st>>>(tp);
+    if (kind == TC_TF32) {
+      if (src_is_f32) k_pack_tile<TC_TF32, true><<<(unsigned)g2, 256, 0, st>>>(tp);
+      else k_pack_tile<TC_TF32, false><<<(unsigned)g2, 256, 0, st>>>(tp);
+    } else {
+      if (src_is_f32) k_pack_tile<TC_BF16, true><<<(unsigned)g2, 256, 0, st>>>(tp);
+      else k_pack_tile<TC_BF16, false><<<(unsigned)g2, 256, 0, st>>>(tp);
+    }
     CTN_CHECK_LAUNCH();
     return CTN_OK;
   }
@@ -760,7 +767,13 @@ ctn_status Packer::run(const void *src, int src_is_f32, uint8_t *hi, uint8_t *lo
   prm.hi = hi;
   prm.lo = lo;
   const int64_t grid = std::min<int64_t>(prm.nitems, (int64_t)nsm_count() * 8);
-  k_pack_items<<<(unsigned)grid, PACK_THREADS, 0, st>>>(prm);
+  if (kind == TC_TF32) {
+    if (src_is_f32) k_pack_items<TC_TF32, true><<<(unsigned)grid, PACK_THREADS, 0, st>>>(prm);
+    else k_pack_items<TC_TF32, false><<<(unsigned)grid, PACK_THREADS, 0, st>>>(prm);
+  } else {
+    if (src_is_f32) k_pack_items<TC_BF16, true><<<(unsigned)grid, PACK_THREADS, 0, st>>>(prm);
+    else k_pack_items<TC_BF16, false><<<(unsigned)grid, PACK_THREADS, 0, st>>>(prm);
+  }
   CTN_CHECK_LAUNCH();
   return CTN_OK;
 }
