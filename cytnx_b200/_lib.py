@@ -89,6 +89,7 @@ _SIGS = {
     "ctn_heff2_matvec": (c_int, [c_vp, c_vp, c_vp, c_int, c_vp]),
     "ctn_heff2_plan_destroy": (None, [c_vp]),
     "ctn_heff2_set_tiles": (c_int, [c_vp, c_int, c_int, c_int]),
+    "ctn_heff2_set_epilogue": (c_int, [c_vp, c_int, c_int, c_int]),
     "ctn_heff2_profile": (c_int, [c_vp, c_vp, c_vp, c_int, c_int, P_dbl, ctypes.POINTER(c_int), c_vp]),
     "ctn_heff2_gemm_flops": (c_dbl, [c_vp, c_int]),
     "ctn_heff2_split_gemm_flops": (c_dbl, [c_vp, c_int, c_int]),

@@ -418,7 +418,8 @@ extern "C" ctn_status ctn_heff2_set_tiles(ctn_heff2_plan *p, int precision, int 
   CTN_REQUIRE(p, "ctn_heff2_set_tiles: null plan");
   CTN_REQUIRE(precision == CTN_PREC_3XTF32 || precision == CTN_PREC_BF16X3, "ctn_heff2_set_tiles: split precision only");
   CTN_REQUIRE(ctn::tc_tile_width_supported(bn_step1) && ctn::tc_tile_width_supported(bn_step4),
-              "ctn_heff2_set_tiles: tile widths must be one of 32, 48, 64, 96, 128, 144, 160, 192, 256");
+              "ctn_heff2_set_tiles: tile widths must be one of 32, 48, 64, 96, 128, 144, 160, 192, 256 "
+              "or -128, -192, -256 (2-CTA tiles)");
   const int k = split_kind(precision);
   if (p->split_bn[k][0] == bn_step1 && p->split_bn[k][1] == bn_step4) return CTN_OK;
   p->split_bn[k][0] = bn_step1;
@@ -426,6 +427,19 @@ extern "C" ctn_status ctn_heff2_set_tiles(ctn_heff2_plan *p, int precision, int 
   ctn::heff_split_free(p->split[k]);
   p->split[k] = nullptr;
   p->split_bound[k] = false;  // the panels depend on the tile widths: bind again
+  return CTN_OK;
+}
+
+extern "C" ctn_status ctn_heff2_set_epilogue(ctn_heff2_plan *p, int precision, int epi_step1, int epi_step4) {
+  CTN_REQUIRE(p, "ctn_heff2_set_epilogue: null plan");
+  CTN_REQUIRE(precision == CTN_PREC_3XTF32 || precision == CTN_PREC_BF16X3,
+              "ctn_heff2_set_epilogue: split precision only");
+  CTN_REQUIRE(epi_step1 >= -1 && epi_step1 <= 1 && epi_step4 >= -1 && epi_step4 <= 1,
+              "ctn_heff2_set_epilogue: -1 (automatic), 0 (direct) or 1 (staged)");
+  const int k = split_kind(precision);
+  p->split_epi[k][0] = epi_step1;
+  p->split_epi[k][1] = epi_step4;
+  ctn::heff_split_apply_epilogue(p, k);  // the panels do not depend on it: no rebind
   return CTN_OK;
 }
 

@@ -57,6 +57,7 @@ ctn_status heff_split_matvec(struct ::ctn_heff2_plan *p, int kind, const double 
                              double *ms3);
 void heff_split_free(HeffSplit *s);
 double heff_split_gemm_flops(const struct ::ctn_heff2_plan *p, int kind, int step);
+void heff_split_apply_epilogue(struct ::ctn_heff2_plan *p, int kind);
 }  // namespace ctn
 
 struct ctn_heff2_plan {
@@ -80,6 +81,7 @@ struct ctn_heff2_plan {
   // split-precision state per kind (0: 3xTF32, 1: BF16x3)
   ctn::HeffSplit *split[2] = {nullptr, nullptr};
   int split_bn[2][2] = {{128, 128}, {128, 128}};  // tile widths of steps 1 and 4 per split kind
+  int split_epi[2][2] = {{-1, -1}, {-1, -1}};     // epilogue form per GEMM: -1 automatic, 0 direct, 1 staged
   bool split_bound[2] = {false, false};
   ~ctn_heff2_plan() {
     for (auto *s : split) ctn::heff_split_free(s);

@@ -237,8 +237,8 @@ ctn_status heff_split_prepare(ctn_heff2_plan *p, int kind) {
   std::unique_ptr<HeffSplit> s(new HeffSplit());
   s->kind = kind;
   s->g1.kind = s->g4.kind = kind;
-  s->g1.bn = p->split_bn[kind][0];
-  s->g4.bn = p->split_bn[kind][1];
+  s->g1.set_width(p->split_bn[kind][0]);
+  s->g4.set_width(p->split_bn[kind][1]);
   s->pk_L.kind = s->pk_P.kind = s->pk_R.kind = kind;
   const int bn = s->g1.bn;
   // ---------------- step 1 groups: one per left sector a
@@ -380,7 +380,15 @@ ctn_status heff_split_prepare(ctn_heff2_plan *p, int kind) {
   chunk_items(s->seg_begin, MPO_ITEM, s->items);
   split_layout(s.get());
   p->split[kind] = s.release();
+  heff_split_apply_epilogue(p, kind);
   return CTN_OK;
+}
+
+void heff_split_apply_epilogue(ctn_heff2_plan *p, int kind) {
+  HeffSplit *s = p->split[kind];
+  if (!s) return;
+  s->g1.epi_staged = p->split_epi[kind][0] < 0 ? s->g1.epi_auto : p->split_epi[kind][0] != 0;
+  s->g4.epi_staged = p->split_epi[kind][1] < 0 ? s->g4.epi_auto : p->split_epi[kind][1] != 0;
 }
 
 double heff_split_gemm_flops(const ctn_heff2_plan *p, int kind, int step) {
@@ -499,8 +507,8 @@ HeffSplit *split_batch(std::vector<ctn_heff2_plan *> &plans, const int64_t *psi_
   std::unique_ptr<HeffSplit> B(new HeffSplit());
   B->kind = kind;
   B->g1.kind = B->g4.kind = kind;
-  B->g1.bn = bn1;
-  B->g4.bn = bn4;
+  B->g1.set_width(bn1);
+  B->g4.set_width(bn4);
   B->pk_L.kind = B->pk_P.kind = B->pk_R.kind = kind;
   B->in_f32 = fp32_io;
   B->out_f32 = fp32_io;
@@ -510,7 +518,7 @@ HeffSplit *split_batch(std::vector<ctn_heff2_plan *> &plans, const int64_t *psi_
     ctn_heff2_plan *p = plans[i];
     p->split_bn[kind][0] = bn1;
     p->split_bn[kind][1] = bn4;
-    if (p->split[kind] && (p->split[kind]->g1.bn != bn1 || p->split[kind]->g4.bn != bn4)) {
+    if (p->split[kind] && (p->split[kind]->g1.width() != bn1 || p->split[kind]->g4.width() != bn4)) {
       delete p->split[kind];
       p->split[kind] = nullptr;
     }

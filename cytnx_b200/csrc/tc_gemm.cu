@@ -101,6 +101,95 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// Epilogue store of one 32-column piece of a warp's 32 accumulator rows.  Each lane holds
+// its row's 32 FP32 values (TMEM lane = row); they are staged in the warp's padded
+// shared-memory slab (row stride 36 floats: 16-byte aligned, 4-way bank spread) and
+// written back 8 lanes per row, so every store instruction covers 4 whole 128-byte
+// FP32 row segments (or 4 x 256-byte FP64 segments) instead of 32 scattered 16-byte
+// pieces of 32 different rows.
+constexpr int EPI_LD = 36;                        // floats per staged row
+constexpr int EPI_WARP_FLOATS = 32 * EPI_LD;      // one warp's slab
+constexpr int EPI_BYTES = 4 * EPI_WARP_FLOATS * 4;  // four epilogue warps
+
+__device__ __forceinline__ void epi_store_piece(const uint32_t (&v)[32], float *slab, int lane, int64_t dst,
+                                                int cg0, int ncol_tile, int mode, float *c32, double *c64) {
+  // stage: lane = row
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+    *reinterpret_cast<float4 *>(slab + lane * EPI_LD + 4 * j) =
+        make_float4(__uint_as_float(v[4 * j]), __uint_as_float(v[4 * j + 1]), __uint_as_float(v[4 * j + 2]),
+                    __uint_as_float(v[4 * j + 3]));
+  __syncwarp();
+  const int sub = lane >> 3, ch = lane & 7;  // 4 rows per round, 8 chunks of 4 columns per row
+  const int c = ch * 4;                      // first column of this lane's chunk inside the piece
+  int64_t rdst[8];
+  float4 x[8];
+#pragma unroll
+  for (int it = 0; it < 8; ++it) rdst[it] = __shfl_sync(0xffffffffu, dst, it * 4 + sub);
+#pragma unroll
+  for (int it = 0; it < 8; ++it) x[it] = *reinterpret_cast<const float4 *>(slab + (it * 4 + sub) * EPI_LD + c);
+  const int nv = min(4, ncol_tile - c);
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    if (rdst[it] < 0 || nv <= 0) continue;
+    if (mode != 1) {
+      float *o = c32 + rdst[it] + cg0 + c;
+      if (nv == 4 && ((reinterpret_cast<uintptr_t>(o) & 15) == 0)) {
+        *reinterpret_cast<float4 *>(o) = x[it];
+      } else {
+        const float xs[4] = {x[it].x, x[it].y, x[it].z, x[it].w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (e < nv) o[e] = xs[e];
+      }
+    } else {
+      double *o = c64 + rdst[it] + cg0 + c;
+      if (nv == 4 && ((reinterpret_cast<uintptr_t>(o) & 15) == 0)) {
+        reinterpret_cast<double2 *>(o)[0] = make_double2((double)x[it].x, (double)x[it].y);
+        reinterpret_cast<double2 *>(o)[1] = make_double2((double)x[it].z, (double)x[it].w);
+      } else {
+        const float xs[4] = {x[it].x, x[it].y, x[it].z, x[it].w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (e < nv) o[e] = (double)xs[e];
+      }
+    }
+  }
+  __syncwarp();  // the slab is reused by the next piece
+}
+
+// Direct form: each lane stores its own row's piece (16-byte vector stores when aligned).
+// Cheaper than staging when the tiles are mostly empty (small blocks) or the rows are
+// scattered FP64 rows.
+__device__ __forceinline__ void epi_store_direct(const uint32_t (&v)[32], int64_t dst, int cg0, int ncol, int mode,
+                                                 float *c32, double *c64) {
+  if (mode != 1) {
+    float *o = c32 + dst + cg0;
+    if (ncol == 32 && ((reinterpret_cast<uintptr_t>(o) & 15) == 0)) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        *reinterpret_cast<float4 *>(o + 4 * j) = make_float4(__uint_as_float(v[4 * j]), __uint_as_float(v[4 * j + 1]),
+                                                             __uint_as_float(v[4 * j + 2]), __uint_as_float(v[4 * j + 3]));
+    } else {
+#pragma unroll
+      for (int e = 0; e < 32; ++e)
+        if (e < ncol) o[e] = __uint_as_float(v[e]);
+    }
+  } else {
+    double *o = c64 + dst + cg0;
+    if (ncol == 32 && ((reinterpret_cast<uintptr_t>(o) & 15) == 0)) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j)
+        *reinterpret_cast<double2 *>(o + 2 * j) =
+            make_double2((double)__uint_as_float(v[2 * j]), (double)__uint_as_float(v[2 * j + 1]));
+    } else {
+#pragma unroll
+      for (int e = 0; e < 32; ++e)
+        if (e < ncol) o[e] = (double)__uint_as_float(v[e]);
+    }
+  }
+}
+
 template <int KIND, int BN, int STAGES>
 struct TcSmem {
   static constexpr int A_BYTES = TC_A_TILE;
@@ -108,8 +197,8 @@ struct TcSmem {
   static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
   static constexpr int RING = STAGES * STAGE_BYTES;
   static constexpr int BAR_OFF = RING;                 // full[S], empty[S], tfull[2], tempty[2], drain
-  static constexpr int BAR_BYTES = 8 * (2 * STAGES + 5) + 16;
-  static constexpr int TOTAL = RING + 256;
+  static constexpr int EPI_OFF = RING + 256;  // four warps' epilogue slabs
+  static constexpr int TOTAL = EPI_OFF + EPI_BYTES;
 };
 
 template <int KIND, int BN, int STAGES>
@@ -238,6 +327,7 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
   } else if (warp >= 2) {
     // ---------------------------------------------------------------- epilogue
     const int q = warp & 3;  // TMEM lane quarter this warp may access
+    float *slab = reinterpret_cast<float *>(smem + SM::EPI_OFF) + (warp - 2) * EPI_WARP_FLOATS;
     int acc = 0;
     uint32_t acc_phase = 0;
     for (int64_t t = blockIdx.x; t < p.ntiles; t += gridDim.x) {
@@ -254,45 +344,25 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
       const uint32_t base = tmem_base + (uint32_t)(acc * BN) + ((uint32_t)(q * 32) << 16);
       int64_t dst = -1;  // this lane's row start in the output (-1: row beyond M)
       if (r < g.M) dst = g.mode == 0 ? g.c_off + (int64_t)r * g.ldc : p.rowmap[g.rm_off + r];
-      // Each lane owns one accumulator row (TMEM lane = row) and stores its 32-column
-      // pieces straight from registers with 16-byte vector stores (FP32 rows are padded to
-      // 16-byte boundaries; FP64 rows use 16-byte stores when aligned, 8-byte otherwise).
-      // A shared-memory transpose for coalesced row stores measured ~2x slower: its
-      // shuffle/ld.shared/st.global chains serialise the four epilogue warps.
+      // Each lane owns one accumulator row (TMEM lane = row); every 32-column piece goes
+      // through the warp's shared-memory slab so that the global stores cover whole row
+      // segments (epi_store_piece).  Storing straight from registers (one row per lane)
+      // made every store instruction touch 32 rows and kept the epilogue of a 128 x 192
+      // FP32 tile at ~4 us, longer than the next tile's MMAs.
+      const bool any_row = __any_sync(0xffffffffu, dst >= 0);  // warp-uniform: rows of this quarter inside M
 #pragma unroll 1
-      for (int c0 = 0; c0 < BN; c0 += 32) {
+      for (int c0 = 0; c0 < BN && any_row; c0 += 32) {
         uint32_t v[32];
         tmem_ld16(base + c0, *reinterpret_cast<uint32_t(*)[16]>(&v[0]));
         tmem_ld16(base + c0 + 16, *reinterpret_cast<uint32_t(*)[16]>(&v[16]));
         tmem_wait_ld();
         const int cg0 = tl.nt * BN + c0;
-        if (cg0 >= g.N || dst < 0) continue;
+        if (cg0 >= g.N) continue;  // warp-uniform: the whole piece is past the tile edge
         const int ncol = min(min(32, BN - c0), g.N - cg0);  // a 32-column piece may pass the tile edge
-        if (g.mode != 1) {
-          float *o = p.c32 + dst + cg0;
-          if (ncol == 32 && ((reinterpret_cast<uintptr_t>(o) & 15) == 0)) {
-#pragma unroll
-            for (int j = 0; j < 8; ++j)
-              *reinterpret_cast<float4 *>(o + 4 * j) = make_float4(
-                  __uint_as_float(v[4 * j]), __uint_as_float(v[4 * j + 1]), __uint_as_float(v[4 * j + 2]),
-                  __uint_as_float(v[4 * j + 3]));
-          } else {
-#pragma unroll
-            for (int e = 0; e < 32; ++e)
-              if (e < ncol) o[e] = __uint_as_float(v[e]);
-          }
-        } else {
-          double *o = p.c64 + dst + cg0;
-          if (ncol == 32 && ((reinterpret_cast<uintptr_t>(o) & 15) == 0)) {
-#pragma unroll
-            for (int j = 0; j < 16; ++j)
-              *reinterpret_cast<double2 *>(o + 2 * j) =
-                  make_double2((double)__uint_as_float(v[2 * j]), (double)__uint_as_float(v[2 * j + 1]));
-          } else {
-#pragma unroll
-            for (int e = 0; e < 32; ++e)
-              if (e < ncol) o[e] = (double)__uint_as_float(v[e]);
-          }
+        if (p.epi_staged) {
+          epi_store_piece(v, slab, lane, dst, cg0, ncol, g.mode, p.c32, p.c64);
+        } else if (dst >= 0) {
+          epi_store_direct(v, dst, cg0, ncol, g.mode, p.c32, p.c64);
         }
       }
       tc_fence_before();
@@ -309,6 +379,273 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
   if (warp == 1) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
+  }
+}
+
+// ------------------------------------------------------------------ 2-CTA (cta_group::2) form
+// A pair of CTAs (a cluster of 2) computes one 256 x BN tile: each CTA stages its own
+// 128 rows of A and half (BN/2 rows) of B per K slice, the leader (cluster rank 0) issues
+// tcgen05.mma.cta_group::2 with M = 256, which reads A from both CTAs and B from both
+// halves, and each CTA's TMEM receives the accumulator rows of its own 128 rows.  Per SM
+// this moves half of B per tile, so the operand ingest per flop drops by a third (BN=128)
+// to a half (BN=256) against the 1-CTA form.
+// Synchronisation: the follower's bulk copies complete on its own full barrier and its
+// relay thread (warp 1) forwards each completion to the leader's full barrier with a
+// remote arrive; the leader's MMA commits are multicast to both CTAs' empty / tfull
+// barriers; the follower's epilogue warps arrive on the leader's tempty barriers.  Every
+// wait is bounded; both CTAs meet at a cluster barrier before TMEM is released.
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// shared::cluster address of the same shared variable in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t peer_addr(const void *p, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
+__device__ __forceinline__ void tc_mma2(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accum, int kind) {
+  if (kind == TC_TF32) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum));
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum));
+  }
+}
+// arrive on the barrier at this offset in both CTAs of the pair once the MMAs complete
+__device__ __forceinline__ void tc_commit2_both(uint64_t *bar) {
+  asm volatile(
+      "{\n\t.reg .b16 m;\n\tmov.b16 m, 3;\n\t"
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], m;\n\t}" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tc_commit2_local(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+template <int KIND, int BN, int STAGES>
+struct TcSmem2 {
+  static constexpr int A_BYTES = TC_A_TILE;              // this CTA's 128 rows
+  static constexpr int B_BYTES = (BN / 2) * TC_ROW_BYTES;  // this CTA's half of B
+  static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+  static constexpr int RING = STAGES * STAGE_BYTES;
+  static constexpr int BAR_OFF = RING;  // full[S], empty[S], tfull[2], tempty[2], drain
+  static constexpr int EPI_OFF = RING + 256;
+  static constexpr int TOTAL = EPI_OFF + EPI_BYTES;
+};
+
+template <int KIND, int BN, int STAGES>
+__global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p) {
+  using SM = TcSmem2<KIND, BN, STAGES>;
+  static_assert(BN % 16 == 0 && BN >= 32 && BN <= 256, "2-CTA tile width");
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t *full = (uint64_t *)(smem + SM::BAR_OFF);
+  uint64_t *empty = full + STAGES;
+  uint64_t *tfull = empty + STAGES;
+  uint64_t *tempty = tfull + 2;
+  uint64_t *drain = tempty + 2;
+  uint32_t *tmem_holder = (uint32_t *)(drain + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();  // 0: leader (issues the MMAs), 1: follower
+  const int64_t pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+  constexpr uint32_t TMEM_COLS = 2 * BN <= 64 ? 64 : 2 * BN <= 128 ? 128 : 2 * BN <= 256 ? 256 : 512;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], rank == 0 ? 2 : 1);  // leader: own copies + the follower's relay
+      mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&tfull[a], 1);
+      mbar_init(&tempty[a], 8);  // leader: 4 own + 4 follower epilogue warps
+    }
+    mbar_init(drain, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_holder)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+  }
+  tc_fence_before();
+  cluster_sync_all();  // both CTAs' barriers initialised and TMEM allocated
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_holder;
+
+  constexpr uint32_t FMT = KIND == TC_TF32 ? 2u : 1u;
+  constexpr uint32_t IDESC =
+      (1u << 4) | (FMT << 7) | (FMT << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(256 >> 4) << 24);
+  constexpr int KSTEPS = 4;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------------------------------------------------------- producer (both CTAs)
+    int stage = 0;
+    uint32_t phase = 0;
+    uint32_t filled[STAGES];
+    for (int s = 0; s < STAGES; ++s) filled[s] = 0;
+    bool ok = true;
+    for (int64_t t = pair; t < p.ntiles && ok; t += npairs) {
+      const TcTile tl = p.tiles[t];
+      const TcGroup g = p.groups[tl.group];
+      const int mt128 = 2 * tl.mt + (int)rank;  // this CTA's 128-row A tile (panels hold an even count)
+      for (int kb = 0; kb < g.kb; ++kb) {
+        if (!mbar_wait(&empty[stage], phase ^ 1, p.err, 1)) {
+          ok = false;
+          break;
+        }
+        uint8_t *st = smem + stage * SM::STAGE_BYTES;
+        mbar_expect_tx(&full[stage], SM::STAGE_BYTES);
+        const int64_t ao = g.a_off + ((int64_t)mt128 * g.kb + kb) * SM::A_BYTES;
+        const int64_t bo = g.b_off + ((int64_t)tl.nt * g.kb + kb) * (2 * SM::B_BYTES) + (int64_t)rank * SM::B_BYTES;
+        bulk_g2s(st, p.a_hi + ao, SM::A_BYTES, &full[stage]);
+        bulk_g2s(st + SM::A_BYTES, p.a_lo + ao, SM::A_BYTES, &full[stage]);
+        bulk_g2s(st + 2 * SM::A_BYTES, p.b_hi + bo, SM::B_BYTES, &full[stage]);
+        bulk_g2s(st + 2 * SM::A_BYTES + SM::B_BYTES, p.b_lo + bo, SM::B_BYTES, &full[stage]);
+        filled[stage]++;
+        if (++stage == STAGES) {
+          stage = 0;
+          phase ^= 1;
+        }
+      }
+    }
+    // drain: every issued fill must have landed before the CTA may exit (bounded)
+    for (int s = 0; s < STAGES; ++s)
+      if (filled[s]) mbar_wait(&full[s], (filled[s] - 1) & 1, p.err, 5);
+  } else if (warp == 1 && lane == 0 && rank == 1) {
+    // ---------------------------------------------------------------- relay (follower)
+    int stage = 0;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int64_t t = pair; t < p.ntiles && ok; t += npairs) {
+      const TcGroup g = p.groups[p.tiles[t].group];
+      for (int kb = 0; kb < g.kb; ++kb) {
+        if (!mbar_wait(&full[stage], phase, p.err, 7)) {
+          ok = false;
+          break;
+        }
+        mbar_arrive_remote(peer_addr(&full[stage], 0));
+        if (++stage == STAGES) {
+          stage = 0;
+          phase ^= 1;
+        }
+      }
+    }
+  } else if (warp == 1 && lane == 0 && rank == 0) {
+    // ---------------------------------------------------------------- MMA issuer (leader)
+    int stage = 0;
+    uint32_t phase = 0;
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    bool ok = true;
+    bool issued = false;
+    for (int64_t t = pair; t < p.ntiles && ok; t += npairs) {
+      const TcGroup g = p.groups[p.tiles[t].group];
+      if (!mbar_wait(&tempty[acc], acc_phase ^ 1, p.err, 2)) break;
+      tc_fence_after();
+      const uint32_t d = tmem_base + (uint32_t)(acc * BN);
+      for (int kb = 0; kb < g.kb; ++kb) {
+        if (!mbar_wait(&full[stage], phase, p.err, 3)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        uint8_t *st = smem + stage * SM::STAGE_BYTES;
+        const uint64_t ahi = smem_desc(st), alo = smem_desc(st + SM::A_BYTES);
+        const uint64_t bhi = smem_desc(st + 2 * SM::A_BYTES), blo = smem_desc(st + 2 * SM::A_BYTES + SM::B_BYTES);
+#pragma unroll
+        for (int j = 0; j < KSTEPS; ++j) {
+          const uint64_t adv = (uint64_t)(j * 32) >> 4;
+          tc_mma2(d, alo + adv, bhi + adv, IDESC, (kb | j) != 0, KIND);
+          tc_mma2(d, ahi + adv, blo + adv, IDESC, 1u, KIND);
+          tc_mma2(d, ahi + adv, bhi + adv, IDESC, 1u, KIND);
+        }
+        issued = true;
+        tc_commit2_both(&empty[stage]);
+        if (++stage == STAGES) {
+          stage = 0;
+          phase ^= 1;
+        }
+      }
+      if (!ok) break;
+      tc_commit2_both(&tfull[acc]);
+      if (++acc == 2) {
+        acc = 0;
+        acc_phase ^= 1;
+      }
+    }
+    if (issued) {
+      tc_commit2_local(drain);
+      mbar_wait(drain, 0, p.err, 6);
+    }
+  } else if (warp >= 2) {
+    // ---------------------------------------------------------------- epilogue (both CTAs)
+    const int q = warp & 3;
+    float *slab = reinterpret_cast<float *>(smem + SM::EPI_OFF) + (warp - 2) * EPI_WARP_FLOATS;
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    const uint32_t leader_tempty0 = peer_addr(&tempty[0], 0), leader_tempty1 = peer_addr(&tempty[1], 0);
+    for (int64_t t = pair; t < p.ntiles; t += npairs) {
+      const TcTile tl = p.tiles[t];
+      const TcGroup g = p.groups[tl.group];
+      int okw = 0;
+      if (lane == 0) okw = mbar_wait(&tfull[acc], acc_phase, p.err, 4) ? 1 : 0;
+      okw = __shfl_sync(0xffffffffu, okw, 0);
+      __syncwarp();
+      if (!okw) break;
+      tc_fence_after();
+      const int r = (2 * tl.mt + (int)rank) * TC_BM + q * 32 + lane;
+      const uint32_t base = tmem_base + (uint32_t)(acc * BN) + ((uint32_t)(q * 32) << 16);
+      int64_t dst = -1;
+      if (r < g.M) dst = g.mode == 0 ? g.c_off + (int64_t)r * g.ldc : p.rowmap[g.rm_off + r];
+      const bool any_row = __any_sync(0xffffffffu, dst >= 0);  // warp-uniform: rows of this quarter inside M
+#pragma unroll 1
+      for (int c0 = 0; c0 < BN && any_row; c0 += 32) {
+        uint32_t v[32];
+        tmem_ld16(base + c0, *reinterpret_cast<uint32_t(*)[16]>(&v[0]));
+        tmem_ld16(base + c0 + 16, *reinterpret_cast<uint32_t(*)[16]>(&v[16]));
+        tmem_wait_ld();
+        const int cg0 = tl.nt * BN + c0;
+        if (cg0 >= g.N) continue;  // warp-uniform: the whole piece is past the tile edge
+        const int ncol = min(min(32, BN - c0), g.N - cg0);  // a 32-column piece may pass the tile edge
+        if (p.epi_staged) {
+          epi_store_piece(v, slab, lane, dst, cg0, ncol, g.mode, p.c32, p.c64);
+        } else if (dst >= 0) {
+          epi_store_direct(v, dst, cg0, ncol, g.mode, p.c32, p.c64);
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) {
+        if (rank == 0) mbar_arrive(&tempty[acc]);
+        else mbar_arrive_remote(acc == 0 ? leader_tempty0 : leader_tempty1);
+      }
+      if (++acc == 2) {
+        acc = 0;
+        acc_phase ^= 1;
+      }
+    }
+  }
+  tc_fence_before();
+  cluster_sync_all();  // no CTA leaves while its peer may still touch its shared memory or TMEM
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
   }
 }
 
@@ -534,6 +871,46 @@ ctn_status launch_tc(const TcParams &prm, int64_t ntiles, cudaStream_t st) {
   return CTN_OK;
 }
 
+template <int KIND, int BN, int STAGES>
+ctn_status launch_tc_pair(const TcParams &prm, int64_t ntiles, cudaStream_t st) {
+  using SM = TcSmem2<KIND, BN, STAGES>;
+  const int smem = SM::TOTAL + 1024;
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_set[dev & 63]) {
+    CTN_CUDA(cudaFuncSetAttribute(k_tc_gemm_pair<KIND, BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  smem));
+    attr_set[dev & 63] = true;
+  }
+  const int pairs = (int)std::min<int64_t>(ntiles, nsm_count() / 2);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2 * pairs, 1, 1);
+  cfg.blockDim = dim3(NTHREADS_TC, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  CTN_CUDA(cudaLaunchKernelEx(&cfg, k_tc_gemm_pair<KIND, BN, STAGES>, prm));
+  return CTN_OK;
+}
+
+template <int KIND>
+ctn_status launch_tc_pair_kind(int bn, const TcParams &prm, cudaStream_t st) {
+  switch (bn) {
+    case 128: return launch_tc_pair<KIND, 128, 4>(prm, prm.ntiles, st);
+    case 192: return launch_tc_pair<KIND, 192, 3>(prm, prm.ntiles, st);
+    case 256: return launch_tc_pair<KIND, 256, 3>(prm, prm.ntiles, st);
+  }
+  set_error("tcgen05 2-CTA GEMM: unsupported tile width %d (128, 192, 256)", bn);
+  return CTN_ERR_UNSUPPORTED;
+}
+
 // tile widths compiled (UMMA M=128 allows N = 16..256 in steps of 16); the ring depth is
 // the largest that fits next to 2 x 16 KiB A tiles and 2 x BN x 128 B B tiles per stage
 template <int KIND>
@@ -545,20 +922,24 @@ ctn_status launch_tc_kind(int bn, const TcParams &prm, cudaStream_t st) {
     case 96: return launch_tc<KIND, 96, 3>(prm, prm.ntiles, st);
     case 128: return launch_tc<KIND, 128, 3>(prm, prm.ntiles, st);
     case 144: return launch_tc<KIND, 144, 3>(prm, prm.ntiles, st);
-    case 160: return launch_tc<KIND, 160, 3>(prm, prm.ntiles, st);
+    case 160: return launch_tc<KIND, 160, 2>(prm, prm.ntiles, st);
     case 192: return launch_tc<KIND, 192, 2>(prm, prm.ntiles, st);
     case 256: return launch_tc<KIND, 256, 2>(prm, prm.ntiles, st);
   }
   set_error("tcgen05 GEMM: unsupported tile width %d (32, 48, 64, 96, 128, 144, 160, 192, 256)", bn);
   return CTN_ERR_UNSUPPORTED;
 }
-ctn_status launch_tc_any(int kind, int bn, const TcParams &prm, cudaStream_t st) {
+ctn_status launch_tc_any(int kind, int bn, bool pair, const TcParams &prm, cudaStream_t st) {
+  if (pair)
+    return kind == TC_TF32 ? launch_tc_pair_kind<TC_TF32>(bn, prm, st) : launch_tc_pair_kind<TC_BF16>(bn, prm, st);
   return kind == TC_TF32 ? launch_tc_kind<TC_TF32>(bn, prm, st) : launch_tc_kind<TC_BF16>(bn, prm, st);
 }
 
 }  // namespace
 
-bool tc_tile_width_supported(int bn) {
+bool tc_tile_width_supported(int w) {
+  if (w < 0) return w == -128 || w == -192 || w == -256;  // 2-CTA (256-row) tiles
+  const int bn = w;
   return bn == 32 || bn == 48 || bn == 64 || bn == 96 || bn == 128 || bn == 144 || bn == 160 || bn == 192 ||
          bn == 256;
 }
@@ -572,13 +953,14 @@ int TcGemm::add_group(int M, int N, int K, int mode, int64_t c_off, int ldc, int
   g.mt = (M + TC_BM - 1) / TC_BM;
   g.nt = (N + bn - 1) / bn;
   g.kb = (K + ks - 1) / ks;
+  const int mt_alloc = pair ? (g.mt + 1) / 2 * 2 : g.mt;  // 2-CTA tiles read 128-row A tiles in pairs
   g.mode = mode;
   g.c_off = c_off;
   g.ldc = ldc;
   g.rm_off = rm_off;
   g.a_off = a_bytes;
   g.b_off = b_bytes;
-  a_bytes += (int64_t)g.mt * g.kb * TC_A_TILE;
+  a_bytes += (int64_t)mt_alloc * g.kb * TC_A_TILE;
   b_bytes += (int64_t)g.nt * g.kb * bn * TC_ROW_BYTES;
   groups.push_back(g);
   flops += 2.0 * M * (double)N * K;
@@ -586,11 +968,20 @@ int TcGemm::add_group(int M, int N, int K, int mode, int64_t c_off, int ldc, int
 }
 
 void TcGemm::finalize() {
+  // staged epilogue when the tiles are mostly filled (whole row segments pay off); direct
+  // when most of every tile lies outside its group (small blocks)
+  double used = 0.0, cover = 0.0;
+  for (const TcGroup &g : groups) {
+    used += (double)g.M * g.N;
+    cover += (double)(pair ? (g.mt + 1) / 2 * 2 : g.mt) * TC_BM * (double)g.nt * bn;
+  }
+  epi_staged = epi_auto = cover > 0.0 && used >= 0.5 * cover;
   std::vector<std::pair<int, TcTile>> tmp;
   for (size_t i = 0; i < groups.size(); ++i) {
     const TcGroup &g = groups[i];
     if (g.kb == 0) continue;
-    for (int m = 0; m < g.mt; ++m)
+    const int mtiles = pair ? (g.mt + 1) / 2 : g.mt;  // 2-CTA: m counts 256-row tiles
+    for (int m = 0; m < mtiles; ++m)
       for (int n = 0; n < g.nt; ++n) tmp.push_back({g.kb, TcTile{(int32_t)i, m, n, 0}});
   }
   std::stable_sort(tmp.begin(), tmp.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
@@ -628,6 +1019,7 @@ ctn_status TcGemm::run(const uint8_t *a_hi, const uint8_t *a_lo, const uint8_t *
   prm.tiles = (const TcTile *)(q + groups.size() * sizeof(TcGroup));
   prm.rowmap = (const int64_t *)(q + groups.size() * sizeof(TcGroup) + tiles.size() * sizeof(TcTile));
   prm.ntiles = (int64_t)tiles.size();
+  prm.epi_staged = epi_staged ? 1 : 0;
   prm.a_hi = a_hi;
   prm.a_lo = a_lo;
   prm.b_hi = b_hi;
@@ -635,7 +1027,7 @@ ctn_status TcGemm::run(const uint8_t *a_hi, const uint8_t *a_lo, const uint8_t *
   prm.c32 = c32;
   prm.c64 = c64;
   prm.err = err;
-  return launch_tc_any(kind, bn, prm, st);
+  return launch_tc_any(kind, bn, pair, prm, st);
 }
 
 ctn_status tc_launch_tables(int kind, int bn, const TcGroup *d_groups, const TcTile *d_tiles, int64_t ntiles,
@@ -647,6 +1039,7 @@ ctn_status tc_launch_tables(int kind, int bn, const TcGroup *d_groups, const TcT
   prm.tiles = d_tiles;
   prm.rowmap = d_rowmap;
   prm.ntiles = ntiles;
+  prm.epi_staged = 0;
   prm.a_hi = a_hi;
   prm.a_lo = a_lo;
   prm.b_hi = b_hi;
@@ -654,7 +1047,7 @@ ctn_status tc_launch_tables(int kind, int bn, const TcGroup *d_groups, const TcT
   prm.c32 = c32;
   prm.c64 = c64;
   prm.err = err;
-  return launch_tc_any(kind, bn, prm, st);
+  return launch_tc_any(kind, bn, false, prm, st);
 }
 
 ctn_status pack_launch_tables(int kind, const PackSeg *d_segs, const int64_t *d_begin, int nseg, int64_t nchunks,

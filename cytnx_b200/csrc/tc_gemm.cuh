@@ -51,6 +51,7 @@ struct TcParams {
   double *c64;
   const int64_t *rowmap;
   int *err;  // device error word: 0 ok, else the code of the wait that gave up
+  int epi_staged;  // 1: epilogue through the shared-memory slab (whole row segments), 0: direct
 };
 
 // byte offset of element (r, k) inside a panel of tiles with `rows` rows per tile
@@ -69,6 +70,15 @@ __host__ __device__ inline int64_t tc_panel_offset(int64_t r, int64_t k, int row
 struct TcGemm {
   int kind = TC_TF32;
   int bn = 128;
+  bool pair = false;  // 2-CTA (cta_group::2) tiles of 256 rows
+  // signed width: bn for 1-CTA tiles, -bn for 2-CTA tiles
+  void set_width(int w) {
+    pair = w < 0;
+    bn = w < 0 ? -w : w;
+  }
+  int width() const { return pair ? -bn : bn; }
+  bool epi_staged = false;  // chosen in finalize from the output mode and the tile fill
+  bool epi_auto = false;    // finalize's choice (restored by an automatic setting)
   std::vector<TcGroup> groups;
   std::vector<TcTile> tiles;
   std::vector<int64_t> rowmap;
@@ -124,7 +134,8 @@ struct Packer {
 };
 
 
-bool tc_tile_width_supported(int bn);
+// compiled tile widths: positive = 1-CTA tile of 128 x bn, negative = 2-CTA tile of 256 x |bn|
+bool tc_tile_width_supported(int width);
 
 // Work items of `per_item` consecutive chunks over segments with chunk prefix sums
 // `begin`; each item records the first and last segment it overlaps (seg0, seg1).

@@ -121,12 +121,14 @@ class TwoSiteHeff(LinOp):
         self._bound.discard(prec)
 
     def autotune(self, precision: Optional[str] = None, step1=(128, 160, 192, 256), step4=(96, 128, 144, 160, 256),
-                 reps: int = 5) -> dict:
-        """Pick the tensor-core tile widths of steps 1 and 4 by timing them on this plan.
+                 reps: int = 5, epilogues=(0, 1)) -> dict:
+        """Pick the tensor-core tile width and epilogue form of steps 1 and 4 by timing them.
 
         The two GEMMs are independent kernels, so each is tuned with the other fixed:
-        every candidate re-packs the operand panels (they depend on the width), runs
-        the matvec and reads the per-phase CUDA-event times (ctn_heff2_profile)."""
+        every width re-packs the operand panels (they depend on the width); for each
+        width both epilogue forms (0 direct, 1 staged through shared memory) are timed
+        with the per-phase CUDA-event profile (ctn_heff2_profile).  Negative widths
+        (2-CTA tiles) may be passed as candidates too."""
         import ctypes as ct
 
         precision = (precision or self.precision).lower()
@@ -136,9 +138,10 @@ class TwoSiteHeff(LinOp):
         x = self.psi_t.flat_view()
         y = torch.empty_like(x)
 
-        def phase_ms(b1, b4):
+        def phase_ms(b1, b4, e1, e4):
             self.set_tiles(b1, b4, precision)
             self.bind(precision)
+            _lib.check(_lib.lib().ctn_heff2_set_epilogue(self._h, prec, int(e1), int(e4)), "autotune")
             ms = (ct.c_double * 4)()
             nl = ct.c_int()
             _lib.check(_lib.lib().ctn_heff2_profile(self._h, x.data_ptr(), y.data_ptr(), prec, reps, ms, ct.byref(nl),
@@ -146,16 +149,20 @@ class TwoSiteHeff(LinOp):
             return [ms[i] for i in range(4)]
 
         table = {"step1": {}, "step4": {}}
-        b4_fixed = 128
         for b1 in step1:
-            table["step1"][b1] = phase_ms(b1, b4_fixed)[1]
+            for e in epilogues:
+                table["step1"][(b1, e)] = phase_ms(b1, 128, e, -1)[1]
         best1 = min(table["step1"], key=table["step1"].get)
         for b4 in step4:
-            table["step4"][b4] = phase_ms(best1, b4)[3]
+            for e in epilogues:
+                table["step4"][(b4, e)] = phase_ms(best1[0], b4, best1[1], e)[3]
         best4 = min(table["step4"], key=table["step4"].get)
-        self.set_tiles(best1, best4, precision)
+        self.set_tiles(best1[0], best4[0], precision)
         self.bind(precision)
-        return {"step1": best1, "step4": best4, "ms_step1": table["step1"], "ms_step4": table["step4"]}
+        _lib.check(_lib.lib().ctn_heff2_set_epilogue(self._h, prec, best1[1], best4[1]), "autotune")
+        return {"step1": best1[0], "step4": best4[0], "epilogue": [best1[1], best4[1]],
+                "ms_step1": {f"{k[0]}/{'staged' if k[1] else 'direct'}": v for k, v in table["step1"].items()},
+                "ms_step4": {f"{k[0]}/{'staged' if k[1] else 'direct'}": v for k, v in table["step4"].items()}}
 
     # ---------------------------------------------------------------- Lanczos without Python callbacks
     def lanczos(self, psi0: UniTensor, maxiter: int = 40, cvgcrit: float = 1e-14,

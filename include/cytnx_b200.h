@@ -237,11 +237,17 @@ double ctn_heff2_gemm_flops(const ctn_heff2_plan *plan, int step);
 /* the same for the stacked tensor-core GEMMs of a split precision (one product counted) */
 double ctn_heff2_split_gemm_flops(ctn_heff2_plan *plan, int precision, int step);
 void ctn_heff2_plan_destroy(ctn_heff2_plan *plan);
-/* tile widths (N of the UMMA tiles: 32, 48, 64, 96, 128, 144, 160, 192 or 256) of the step-1 and
+/* tile widths (N of the UMMA tiles: 32, 48, 64, 96, 128, 144, 160, 192 or 256; negative -128, -192,
+ * -256 select 2-CTA cta_group::2 tiles of 256 rows) of the step-1 and
  * step-4 tensor-core GEMMs of a split precision; drops that precision's binding (the
  * operand panels depend on the widths), so call ctn_heff2_set_env again.  Used by the
  * autotuner (TwoSiteHeff.autotune). */
 ctn_status ctn_heff2_set_tiles(ctn_heff2_plan *plan, int precision, int bn_step1, int bn_step4);
+/* epilogue form of the step-1 / step-4 tensor-core GEMMs: -1 automatic (staged through
+ * shared memory when the tiles are at least half filled), 0 direct
+ * (each lane stores its own accumulator row), 1 staged (whole row segments per store).
+ * Takes effect on the next matvec; used by the autotuner. */
+ctn_status ctn_heff2_set_epilogue(ctn_heff2_plan *plan, int precision, int epi_step1, int epi_step4);
 
 /* ---------------------------------------------------------------- batched H_eff
  * Many independent two-site problems (uneven block structures) applied together: the

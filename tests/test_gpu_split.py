@@ -96,3 +96,41 @@ def test_heff_split_tile_widths_agree(prec):
         assert err < (1e-5 if prec == "3xtf32" else 2e-3), (b1, b4, err)
     tuned = H.autotune(prec, reps=2)
     assert tuned["step1"] in (128, 160, 192, 256) and tuned["step4"] in (96, 128, 144, 160, 256)
+
+
+@pytest.mark.parametrize("prec", ["3xtf32", "bf16x3"])
+def test_heff_split_pair_tiles_match_single_cta(prec):
+    """2-CTA (cta_group::2, 256-row) tiles give the 1-CTA result: same products, same
+    K order; the FP32 accumulators agree to rounding."""
+    psi, H = _heff(512, seed=9)
+    x = psi.flat_view()
+    y64 = torch.empty_like(x)
+    H.apply_flat(x, y64, "fp64")
+    H.set_tiles(128, 128, prec)
+    y1 = torch.empty_like(x)
+    H.apply_flat(x, y1, prec)
+    for b1, b4 in [(-128, -128), (-256, -192), (-192, -256), (-128, 128), (160, -128)]:
+        H.set_tiles(b1, b4, prec)
+        y = torch.empty_like(x)
+        H.apply_flat(x, y, prec)
+        d = (torch.linalg.vector_norm(y - y1) / torch.linalg.vector_norm(y1)).item()
+        e = (torch.linalg.vector_norm(y - y64) / torch.linalg.vector_norm(y64)).item()
+        assert d < 1e-6 and e < 2e-5, (b1, b4, d, e)
+
+
+@pytest.mark.parametrize("prec", ["3xtf32", "bf16x3"])
+def test_epilogue_forms_are_bitwise_equal(prec):
+    """The direct and the shared-memory-staged epilogues store the same accumulators."""
+    from cytnx_b200 import _lib
+
+    psi, H = _heff(384, seed=10)
+    x = psi.flat_view()
+    H.set_tiles(160, 144, prec)
+    out = []
+    for e1, e4 in [(0, 0), (1, 1), (0, 1), (-1, -1)]:
+        _lib.check(_lib.lib().ctn_heff2_set_epilogue(H._h, _lib.PRECISIONS[prec], e1, e4))
+        y = torch.zeros_like(x)
+        H.apply_flat(x, y, prec)
+        out.append(y)
+    for y in out[1:]:
+        assert torch.equal(y, out[0])
