@@ -142,12 +142,50 @@ __global__ void __launch_bounds__(RT) k_lanczos_update3(double *__restrict__ w, 
   finish(s, partials, ticket, nrm, 1);
 }
 
-// y = x / *a
+// y = x / *a (y = 0 when *a is zero: a Lanczos breakdown leaves the next vector empty)
 __global__ void __launch_bounds__(RT) k_div_copy(const double *__restrict__ x, double *__restrict__ y,
                                                 int64_t n, const double *a) {
   const double al = *a;
+  const bool zero = al == 0.0;
   const int64_t step = (int64_t)gridDim.x * RT;
-  for (int64_t i = (int64_t)blockIdx.x * RT + threadIdx.x; i < n; i += step) y[i] = x[i] / al;
+  for (int64_t i = (int64_t)blockIdx.x * RT + threadIdx.x; i < n; i += step) y[i] = zero ? 0.0 : x[i] / al;
+}
+
+// <w, a> and <w, b> in one pass over w (two reductions, partials side by side)
+__global__ void __launch_bounds__(RT) k_dot2(const double *__restrict__ w, const double *__restrict__ a,
+                                            const double *__restrict__ b, int64_t n, double *partials,
+                                            unsigned *ticket, double *out_a, double *out_b) {
+  double sa = 0.0, sb = 0.0;
+  const int64_t step = (int64_t)gridDim.x * RT;
+  for (int64_t i = (int64_t)blockIdx.x * RT + threadIdx.x; i < n; i += step) {
+    const double x = w[i];
+    sa = fma(x, a[i], sa);
+    sb = fma(x, b[i], sb);
+  }
+  sa = block_sum(sa);
+  sb = block_sum(sb);
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = sa;
+    partials[2 * blockIdx.x + 1] = sb;
+    __threadfence();
+    const unsigned t = atomicAdd(ticket, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  double va = 0.0, vb = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += RT) {
+    va += ((volatile double *)partials)[2 * i];
+    vb += ((volatile double *)partials)[2 * i + 1];
+  }
+  va = block_sum(va);
+  vb = block_sum(vb);
+  if (threadIdx.x == 0) {
+    *out_a = va;
+    *out_b = vb;
+    *ticket = 0u;
+  }
 }
 
 // out = sum_j c[j] * K[j]  (Krylov combination), c on device
@@ -175,6 +213,16 @@ int grid_for(int64_t n) {
 }  // namespace
 
 size_t reduce_ws_bytes() { return (MAXCTA + 8) * sizeof(double); }
+size_t reduce2_ws_bytes() { return (2 * MAXCTA + 8) * sizeof(double); }
+
+// ws2 layout: [2 * MAXCTA partials][ticket]
+ctn_status dot2_f64(const double *w, const double *a, const double *b, int64_t n, double *out_a, double *out_b,
+                    double *ws2, cudaStream_t st) {
+  const int g = grid_for(n);
+  k_dot2<<<g, RT, 0, st>>>(w, a, b, n, ws2, reinterpret_cast<unsigned *>(ws2 + 2 * MAXCTA), out_a, out_b);
+  CTN_CHECK_LAUNCH();
+  return CTN_OK;
+}
 
 // ws layout: [partials MAXCTA doubles][ticket (8 bytes)]
 ctn_status dot_f64(const double *x, const double *y, int64_t n, double *out, double *ws, cudaStream_t st) {

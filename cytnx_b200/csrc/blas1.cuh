@@ -5,6 +5,10 @@
 namespace ctn {
 // bytes of the reduction workspace (partials + ticket); must be zeroed once before first use
 size_t reduce_ws_bytes();
+// the same for dot2_f64 (two reductions in one pass)
+size_t reduce2_ws_bytes();
+ctn_status dot2_f64(const double *w, const double *a, const double *b, int64_t n, double *out_a, double *out_b,
+                    double *ws2, cudaStream_t st);
 ctn_status dot_f64(const double *x, const double *y, int64_t n, double *out, double *ws, cudaStream_t st);
 ctn_status nrm2_f64(const double *x, int64_t n, double *out, double *ws, cudaStream_t st);
 ctn_status axpy_f64(const double *x, double *y, int64_t n, const double *a, double a_scale, cudaStream_t st);

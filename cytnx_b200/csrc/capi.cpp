@@ -259,60 +259,66 @@ ctn_status lanczos_refined(int (*mv_lo)(void *, const double *, double *, void *
                            double *eigvec, double *energy, double *residual, int *restarts, int64_t *counts,
                            cudaStream_t st) {
   CTN_REQUIRE(krydim >= 2 && max_restarts >= 1 && n > 0 && tol >= 0, "[Lanczos refined] bad argument");
+  // work: [w n][scalars 8][reduction ws][two-sum ws][Ritz coefficients m][alpha m][beta m]
   double *w = work;
-  double *scal = work + n;  // [1] alpha [2] beta_prev [3] |w| [4] gamma (overlap with q0) [0] norm
+  double *scal = work + n;  // [0] norm [1] theta [3] rho [4] gamma (overlap with q0)
   double *ws = work + n + 8;
-  double *cdev = ws + reduce_ws_bytes() / sizeof(double);
-  CTN_CUDA(cudaMemsetAsync(ws, 0, reduce_ws_bytes(), st));
+  double *ws2 = ws + reduce_ws_bytes() / sizeof(double);
+  double *cdev = ws2 + reduce2_ws_bytes() / sizeof(double);
+  double *alpha = cdev + krydim;
+  double *beta = alpha + krydim;
+  CTN_CUDA(cudaMemsetAsync(ws, 0, reduce_ws_bytes() + reduce2_ws_bytes(), st));
   double host = 0.0;
-  auto fetch = [&](int idx, double *dst) -> ctn_status {
-    CTN_CUDA(cudaMemcpyAsync(dst, scal + idx, sizeof(double), cudaMemcpyDeviceToHost, st));
-    CTN_CUDA(cudaStreamSynchronize(st));
-    return CTN_OK;
-  };
   int64_t n_lo = 0, n_hi = 0;
   CTN_TRY(nrm2_f64(psi0, n, scal + 0, ws, st));
-  CTN_TRY(fetch(0, &host));
+  CTN_CUDA(cudaMemcpyAsync(&host, scal + 0, sizeof(double), cudaMemcpyDeviceToHost, st));
+  CTN_CUDA(cudaStreamSynchronize(st));
   CTN_REQUIRE(host > 0 && std::isfinite(host), "[Lanczos refined] initial vector has zero or non-finite norm");
   CTN_TRY(div_copy_f64(psi0, krylov, n, scal + 0, st));
   double theta = 0.0, rho = 0.0;
   int c = 0;
-  std::vector<double> As, Bs, evals, evecs;
+  std::vector<double> As(krydim), Bs(krydim), evals, evecs;
   for (c = 0; c < max_restarts; ++c) {
     double *q0 = krylov;
+    // FP64 refinement: theta = <q0, H q0>, r = H q0 - theta q0, rho = |r|  (alpha[0], beta[0])
     if (mv_hi(u_hi, q0, w, st) != 0) return CTN_ERR_CUDA;
     ++n_hi;
-    CTN_TRY(dot_f64(w, q0, n, scal + 1, ws, st));
-    CTN_TRY(lanczos_update_f64(w, q0, nullptr, n, scal + 1, scal + 2, scal + 3, ws, st));
-    CTN_TRY(fetch(1, &theta));
-    CTN_TRY(fetch(3, &rho));
+    CTN_TRY(dot_f64(w, q0, n, alpha + 0, ws, st));
+    CTN_TRY(lanczos_update_f64(w, q0, nullptr, n, alpha + 0, nullptr, beta + 0, ws, st));
+    double tr[2];
+    CTN_CUDA(cudaMemcpyAsync(&tr[0], alpha + 0, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CTN_CUDA(cudaMemcpyAsync(&tr[1], beta + 0, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CTN_CUDA(cudaStreamSynchronize(st));  // the one host synchronisation of a cycle
+    theta = tr[0];
+    rho = tr[1];
     CTN_REQUIRE(std::isfinite(theta) && std::isfinite(rho), "[Lanczos refined] non-finite Rayleigh quotient");
     if (rho <= tol * std::fabs(theta) || rho == 0.0 || c == max_restarts - 1) break;
-    As.assign(1, theta);
-    Bs.assign(1, rho);
-    CTN_CUDA(cudaMemcpyAsync(scal + 2, &rho, sizeof(double), cudaMemcpyHostToDevice, st));
-    CTN_TRY(div_copy_f64(w, krylov + n, n, scal + 3, st));
+    CTN_TRY(div_copy_f64(w, krylov + n, n, beta + 0, st));
+    // low-precision Krylov steps, all scalars kept on the device (no host round trip)
     for (int j = 1; j < krydim; ++j) {
       const double *qj = krylov + (int64_t)j * n;
       const double *qp = krylov + (int64_t)(j - 1) * n;
       if (mv_lo(u_lo, qj, w, st) != 0) return CTN_ERR_CUDA;
       ++n_lo;
-      CTN_TRY(dot_f64(w, qj, n, scal + 1, ws, st));
-      CTN_TRY(dot_f64(w, q0, n, scal + 4, ws, st));
+      CTN_TRY(dot2_f64(w, qj, q0, n, alpha + j, scal + 4, ws2, st));
       if (j == 1)  // q_{j-1} is q0: its measured overlap replaces beta
-        CTN_TRY(lanczos_update3_f64(w, qj, q0, nullptr, n, scal + 1, scal + 4, nullptr, scal + 3, ws, st));
+        CTN_TRY(lanczos_update3_f64(w, qj, q0, nullptr, n, alpha + j, scal + 4, nullptr, beta + j, ws, st));
       else
-        CTN_TRY(lanczos_update3_f64(w, qj, qp, q0, n, scal + 1, scal + 2, scal + 4, scal + 3, ws, st));
-      double alpha = 0.0, beta = 0.0;
-      CTN_TRY(fetch(1, &alpha));
-      CTN_TRY(fetch(3, &beta));
-      As.push_back(alpha);
-      if (j == krydim - 1 || beta == 0.0 || !std::isfinite(beta)) break;
-      Bs.push_back(beta);
-      CTN_CUDA(cudaMemcpyAsync(scal + 2, &beta, sizeof(double), cudaMemcpyHostToDevice, st));
-      CTN_TRY(div_copy_f64(w, krylov + (int64_t)(j + 1) * n, n, scal + 3, st));
+        CTN_TRY(lanczos_update3_f64(w, qj, qp, q0, n, alpha + j, beta + j - 1, scal + 4, beta + j, ws, st));
+      if (j + 1 < krydim) CTN_TRY(div_copy_f64(w, krylov + (int64_t)(j + 1) * n, n, beta + j, st));
     }
-    const int m = (int)As.size();
+    CTN_CUDA(cudaMemcpyAsync(As.data(), alpha, sizeof(double) * krydim, cudaMemcpyDeviceToHost, st));
+    CTN_CUDA(cudaMemcpyAsync(Bs.data(), beta, sizeof(double) * krydim, cudaMemcpyDeviceToHost, st));
+    CTN_CUDA(cudaStreamSynchronize(st));
+    // a zero beta (breakdown) ends the Krylov space there
+    int m = krydim;
+    for (int j = 0; j + 1 < krydim; ++j)
+      if (!(Bs[j] > 0.0) || !std::isfinite(Bs[j])) {
+        m = j + 1;
+        break;
+      }
+    for (int j = 0; j < m; ++j)
+      CTN_REQUIRE(std::isfinite(As[j]), "[Lanczos refined] non-finite recurrence coefficient");
     evals.assign(m, 0.0);
     evecs.assign((size_t)m * m, 0.0);
     CTN_TRY(tql(m, As.data(), Bs.data(), evals.data(), evecs.data()));

@@ -195,7 +195,7 @@ class TwoSiteHeff(LinOp):
         x0 = psi0.contiguous().flat_view()
         n = self.n
         krylov = torch.empty(krylov_dim * n, dtype=torch.float64, device=x0.device)
-        work = torch.empty(n + 8 + 1032 + krylov_dim + 64, dtype=torch.float64, device=x0.device)
+        work = torch.empty(n + 3200 + 3 * krylov_dim, dtype=torch.float64, device=x0.device)
         eig = torch.empty(n, dtype=torch.float64, device=x0.device)
         e, r = ctypes.c_double(), ctypes.c_double()
         rs = ctypes.c_int()

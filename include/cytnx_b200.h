@@ -295,7 +295,8 @@ ctn_status ctn_lanczos_gnd(ctn_matvec_fn matvec, void *user, const double *psi0,
  * cycle: q0 = v, q1 = r/|r|, krydim - 1 low-precision steps with three-term recurrence and
  * an FP64 re-orthogonalisation against q0, FP64 tridiagonal solve, v <- Ritz vector.  Stops
  * when |r| <= tol * |E| or after max_restarts FP64 matvecs.  krylov: krydim * n doubles;
- * work >= n + 8 + 1032 + krydim + 64 doubles.  *energy / *residual: FP64 Rayleigh quotient
+ * work >= n + 3200 + 3 * krydim doubles.  The Krylov steps keep alpha / beta on the device
+ * (one host synchronisation per restart).  *energy / *residual: FP64 Rayleigh quotient
  * and |r| of the returned unit vector; matvecs[0..1] = low / FP64 products used.
  * No direct counterpart in the reference (its Lanczos_ER restarts in one precision,
  * src/linalg/Lanczos_ER.cpp); the recurrence is that of Lanczos_Gnd_Ut. */
