@@ -127,106 +127,131 @@ __device__ __forceinline__ uint32_t bf16_rne_bits(float x) {
   return (u + 0x7FFFu + ((u >> 16) & 1u)) >> 16;
 }
 
+// split of one X3 chunk into its hi/lo panel chunks (integer rounding on the ALU pipe)
+template <int KIND>
+__device__ __forceinline__ void mpo_store(const float (&x)[8], const MpoSegS &s, int r, int kloc, uint8_t *hi,
+                                          uint8_t *lo) {
+  constexpr bool TF = KIND == TC_TF32;
+  // panel offset (32-bit index math except the final byte offset)
+  const int row = s.row0 + r, kabs = s.k0 + kloc;
+  const int rr = row & (TC_BM - 1);
+  const int kslice = TF ? (kabs >> 5) : (kabs >> 6);
+  const int byte = TF ? ((kabs & 31) << 2) : ((kabs & 63) << 1);
+  const int64_t off = s.panel_off + ((int64_t)(row >> 7) * s.kb + kslice) * TC_A_TILE + (rr >> 3) * 1024 +
+                      (rr & 7) * 128 + (((byte >> 4) ^ (rr & 7)) << 4);
+  if (TF) {
+    float h[4], l[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      h[e] = tf32_rna(x[e]);
+      l[e] = tf32_rna(x[e] - h[e]);  // exact in FP32
+    }
+    *(float4 *)(hi + off) = make_float4(h[0], h[1], h[2], h[3]);
+    *(float4 *)(lo + off) = make_float4(l[0], l[1], l[2], l[3]);
+  } else {
+    uint32_t hw[4], lw[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const uint32_t h0 = bf16_rne_bits(x[2 * e]), h1 = bf16_rne_bits(x[2 * e + 1]);
+      const uint32_t l0 = bf16_rne_bits(x[2 * e] - __uint_as_float(h0 << 16));
+      const uint32_t l1 = bf16_rne_bits(x[2 * e + 1] - __uint_as_float(h1 << 16));
+      hw[e] = h0 | (h1 << 16);
+      lw[e] = l0 | (l1 << 16);
+    }
+    *(uint4 *)(hi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+    *(uint4 *)(lo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+  }
+}
+
 // One CTA per work item of MPO_ITEM consecutive chunks (E = 4 TF32 / 8 BF16 elements of
 // one row) of the flattened X3 blocks; an item may span several small blocks (each
 // thread finds its block by a binary search over the blocks the item overlaps).  Blocks
 // are ordered by (a', b), so the blocks that read the same X1 inputs run together and
 // share them in L2.  X1 block rows start on 16-byte boundaries (padded step-1 columns),
-// so full chunks load as float4, four terms per round.
+// so full chunks load as float4.  Each thread computes MPO_UNROLL chunks together, four
+// terms per round: up to 2 x 4 x 2 independent 16-byte loads are in flight per thread.
+template <int KIND>
 __global__ void __launch_bounds__(MPO_THREADS) k_mpo_split(MpoSParams p) {
-  const bool tf32 = p.kind == TC_TF32;
-  const int E = tf32 ? 4 : 8;
+  constexpr bool TF = KIND == TC_TF32;
+  constexpr int E = TF ? 4 : 8;
+  constexpr int U = MPO_UNROLL;
   for (int64_t it = blockIdx.x; it < p.nitems; it += gridDim.x) {
     const WorkItem wi = p.items[it];
-#pragma unroll 1
-    for (int j = 0; j < MPO_UNROLL; ++j) {
+    MpoSegS sg[U];
+    int r[U], kloc[U], nv[U], nt[U];
+#pragma unroll
+    for (int j = 0; j < U; ++j) {
       const int64_t g = wi.chunk0 + threadIdx.x + j * MPO_THREADS;
-      if (g >= p.nchunks) break;
+      const bool ok = g < p.nchunks;
       int si = wi.seg0, hi_s = wi.seg1;  // last block with begin <= g
-      while (si < hi_s) {
+      while (ok && si < hi_s) {
         const int mid = (si + hi_s + 1) >> 1;
         if (__ldg(p.begin + mid) <= g) si = mid;
         else hi_s = mid - 1;
       }
-      const MpoSegS s = p.segs[si];
-      const int nkc = (s.cols + E - 1) / E;
-      const int cl = (int)(g - __ldg(p.begin + si));
-      const int r = cl / nkc;
-      const int kloc = (cl - r * nkc) * E;
-      const int nvalid = min(E, s.cols - kloc);
-      {
-        float x[8];
+      sg[j] = p.segs[si];
+      const int nkc = (sg[j].cols + E - 1) / E;
+      const int cl = ok ? (int)(g - __ldg(p.begin + si)) : 0;
+      r[j] = cl / nkc;
+      kloc[j] = (cl - r[j] * nkc) * E;
+      nv[j] = ok ? min(E, sg[j].cols - kloc[j]) : 0;
+      nt[j] = ok ? sg[j].term_count : 0;
+    }
+    float x[U][8];
 #pragma unroll
-        for (int e = 0; e < 8; ++e) x[e] = 0.f;
-        if (nvalid == E) {
-          // four terms per round: their loads are issued together (memory-level parallelism)
-          for (int t0 = 0; t0 < s.term_count; t0 += 4) {
-            float4 v[4], w[4];
-            float cf[4];
+    for (int j = 0; j < U; ++j)
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              v[u] = w[u] = make_float4(0.f, 0.f, 0.f, 0.f);
-              cf[u] = 0.f;
-              if (t0 + u < s.term_count) {
-                const MpoTermS tm = p.terms[s.term_begin + t0 + u];
-                cf[u] = (float)tm.coef;
-                const float4 *src = reinterpret_cast<const float4 *>(p.x1 + tm.x1_off + (int64_t)r * tm.ld + kloc);
-                v[u] = __ldg(src);
-                if (!tf32) w[u] = __ldg(src + 1);
-              }
-            }
+      for (int e = 0; e < 8; ++e) x[j][e] = 0.f;
+    int tmax = 0;
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              x[0] = fmaf(cf[u], v[u].x, x[0]);
-              x[1] = fmaf(cf[u], v[u].y, x[1]);
-              x[2] = fmaf(cf[u], v[u].z, x[2]);
-              x[3] = fmaf(cf[u], v[u].w, x[3]);
-              x[4] = fmaf(cf[u], w[u].x, x[4]);
-              x[5] = fmaf(cf[u], w[u].y, x[5]);
-              x[6] = fmaf(cf[u], w[u].z, x[6]);
-              x[7] = fmaf(cf[u], w[u].w, x[7]);
-            }
-          }
-        } else {
-          for (int t = 0; t < s.term_count; ++t) {
-            const MpoTermS tm = p.terms[s.term_begin + t];
-            const float cf = (float)tm.coef;
-            const float *src = p.x1 + tm.x1_off + (int64_t)r * tm.ld + kloc;
+    for (int j = 0; j < U; ++j) tmax = max(tmax, nv[j] == E ? nt[j] : 0);
+    for (int t0 = 0; t0 < tmax; t0 += 4) {
+      float4 v[U][4], w[U][4];
+      float cf[U][4];
 #pragma unroll
-            for (int e = 0; e < 8; ++e)
-              if (e < nvalid) x[e] = fmaf(cf, __ldg(src + e), x[e]);
+      for (int j = 0; j < U; ++j)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          v[j][u] = w[j][u] = make_float4(0.f, 0.f, 0.f, 0.f);
+          cf[j][u] = 0.f;
+          if (nv[j] == E && t0 + u < nt[j]) {
+            const MpoTermS tm = p.terms[sg[j].term_begin + t0 + u];
+            cf[j][u] = (float)tm.coef;
+            const float4 *src = reinterpret_cast<const float4 *>(p.x1 + tm.x1_off + (int64_t)r[j] * tm.ld + kloc[j]);
+            v[j][u] = __ldg(src);
+            if (!TF) w[j][u] = __ldg(src + 1);
           }
         }
-        // panel offset (32-bit index math except the final byte offset)
-        const int row = s.row0 + r, kabs = s.k0 + kloc;
-        const int rr = row & (TC_BM - 1);
-        const int kslice = tf32 ? (kabs >> 5) : (kabs >> 6);
-        const int byte = tf32 ? ((kabs & 31) << 2) : ((kabs & 63) << 1);
-        const int64_t off = s.panel_off + ((int64_t)(row >> 7) * s.kb + kslice) * TC_A_TILE + (rr >> 3) * 1024 +
-                            (rr & 7) * 128 + (((byte >> 4) ^ (rr & 7)) << 4);
-        if (tf32) {
-          float h[4], l[4];
-  #pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            h[e] = tf32_rna(x[e]);
-            l[e] = tf32_rna(x[e] - h[e]);  // exact in FP32
+#pragma unroll
+      for (int j = 0; j < U; ++j)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          x[j][0] = fmaf(cf[j][u], v[j][u].x, x[j][0]);
+          x[j][1] = fmaf(cf[j][u], v[j][u].y, x[j][1]);
+          x[j][2] = fmaf(cf[j][u], v[j][u].z, x[j][2]);
+          x[j][3] = fmaf(cf[j][u], v[j][u].w, x[j][3]);
+          if (!TF) {
+            x[j][4] = fmaf(cf[j][u], w[j][u].x, x[j][4]);
+            x[j][5] = fmaf(cf[j][u], w[j][u].y, x[j][5]);
+            x[j][6] = fmaf(cf[j][u], w[j][u].z, x[j][6]);
+            x[j][7] = fmaf(cf[j][u], w[j][u].w, x[j][7]);
           }
-          *(float4 *)(p.hi + off) = make_float4(h[0], h[1], h[2], h[3]);
-          *(float4 *)(p.lo + off) = make_float4(l[0], l[1], l[2], l[3]);
-        } else {
-          uint32_t hw[4], lw[4];
-  #pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const uint32_t h0 = bf16_rne_bits(x[2 * e]), h1 = bf16_rne_bits(x[2 * e + 1]);
-            const uint32_t l0 = bf16_rne_bits(x[2 * e] - __uint_as_float(h0 << 16));
-            const uint32_t l1 = bf16_rne_bits(x[2 * e + 1] - __uint_as_float(h1 << 16));
-            hw[e] = h0 | (h1 << 16);
-            lw[e] = l0 | (l1 << 16);
-          }
-          *(uint4 *)(p.hi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-          *(uint4 *)(p.lo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < U; ++j) {
+      if (nv[j] <= 0) continue;
+      if (nv[j] < E) {  // ragged end of a block row: scalar loads
+        for (int t = 0; t < nt[j]; ++t) {
+          const MpoTermS tm = p.terms[sg[j].term_begin + t];
+          const float cf = (float)tm.coef;
+          const float *src = p.x1 + tm.x1_off + (int64_t)r[j] * tm.ld + kloc[j];
+#pragma unroll
+          for (int e = 0; e < E; ++e)
+            if (e < nv[j]) x[j][e] = fmaf(cf, __ldg(src + e), x[j][e]);
+        }
       }
-      }
+      mpo_store<KIND>(x[j], sg[j], r[j], kloc[j], p.hi, p.lo);
     }
   }
 }
@@ -467,11 +492,13 @@ ctn_status split_matvec(HeffSplit *s, const void *psi, void *out, cudaStream_t s
     prm.x1 = (const float *)(w + s->o_x1);
     prm.hi = w + s->o_a4h;
     prm.lo = w + s->o_a4l;
-    int dev = 0, nsm = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const int64_t grid = std::min<int64_t>(prm.nitems, (int64_t)nsm * 8);
-    k_mpo_split<<<(unsigned)grid, MPO_THREADS, 0, st>>>(prm);
+    // four waves of resident CTAs: items of uneven size balance through the CTA scheduler
+    auto launch = [&](auto kern) -> void {
+      const int64_t grid = std::min<int64_t>(prm.nitems, (int64_t)nsm_count() * resident_ctas(kern, MPO_THREADS) * 4);
+      kern<<<(unsigned)grid, MPO_THREADS, 0, st>>>(prm);
+    };
+    if (kind == TC_TF32) launch(k_mpo_split<TC_TF32>);
+    else launch(k_mpo_split<TC_BF16>);
     CTN_CHECK_LAUNCH();
   }
   if (ms4) CTN_CUDA(cudaEventRecord(ev[3], st));

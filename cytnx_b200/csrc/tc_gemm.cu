@@ -20,6 +20,15 @@
 
 namespace ctn {
 
+int nsm_count() {
+  int dev = 0, n = 148;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();  // no device here: clear the error, use the B200 count
+    n = 148;
+  }
+  return n > 0 ? n : 148;
+}
+
 namespace {
 
 constexpr int NTHREADS_TC = 192;
@@ -847,12 +856,7 @@ __global__ void __launch_bounds__(256) k_pack_tile(PackTileParams p) {
   }
 }
 
-int nsm_count() {
-  int dev = 0, n = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-  return n > 0 ? n : 148;
-}
+
 
 template <int KIND, int BN, int STAGES>
 ctn_status launch_tc(const TcParams &prm, int64_t ntiles, cudaStream_t st) {
@@ -1135,13 +1139,18 @@ ctn_status Packer::run(const void *src, int src_is_f32, uint8_t *hi, uint8_t *lo
     tp.src = src;
     tp.hi = hi;
     tp.lo = lo;
-    const int64_t g2 = std::min<int64_t>(tp.nitems, (int64_t)nsm_count() * 8);
+    // four waves of resident CTAs over the grid-stride item loop: items of uneven size
+    // balance through the hardware CTA scheduler
+    auto launch = [&](auto kern) -> void {
+      const int64_t g2 = std::min<int64_t>(tp.nitems, (int64_t)nsm_count() * resident_ctas(kern, 256) * 4);
+      kern<<<(unsigned)g2, 256, 0, st>>>(tp);
+    };
     if (kind == TC_TF32) {
-      if (src_is_f32) k_pack_tile<TC_TF32, true><<<(unsigned)g2, 256, 0, st>>>(tp);
-      else k_pack_tile<TC_TF32, false><<<(unsigned)g2, 256, 0, st>>>(tp);
+      if (src_is_f32) launch(k_pack_tile<TC_TF32, true>);
+      else launch(k_pack_tile<TC_TF32, false>);
     } else {
-      if (src_is_f32) k_pack_tile<TC_BF16, true><<<(unsigned)g2, 256, 0, st>>>(tp);
-      else k_pack_tile<TC_BF16, false><<<(unsigned)g2, 256, 0, st>>>(tp);
+      if (src_is_f32) launch(k_pack_tile<TC_BF16, true>);
+      else launch(k_pack_tile<TC_BF16, false>);
     }
     CTN_CHECK_LAUNCH();
     return CTN_OK;
@@ -1159,13 +1168,16 @@ ctn_status Packer::run(const void *src, int src_is_f32, uint8_t *hi, uint8_t *lo
   prm.src = src;
   prm.hi = hi;
   prm.lo = lo;
-  const int64_t grid = std::min<int64_t>(prm.nitems, (int64_t)nsm_count() * 8);
+  auto launch = [&](auto kern) -> void {
+    const int64_t grid = std::min<int64_t>(prm.nitems, (int64_t)nsm_count() * resident_ctas(kern, PACK_THREADS) * 4);
+    kern<<<(unsigned)grid, PACK_THREADS, 0, st>>>(prm);
+  };
   if (kind == TC_TF32) {
-    if (src_is_f32) k_pack_items<TC_TF32, true><<<(unsigned)grid, PACK_THREADS, 0, st>>>(prm);
-    else k_pack_items<TC_TF32, false><<<(unsigned)grid, PACK_THREADS, 0, st>>>(prm);
+    if (src_is_f32) launch(k_pack_items<TC_TF32, true>);
+    else launch(k_pack_items<TC_TF32, false>);
   } else {
-    if (src_is_f32) k_pack_items<TC_BF16, true><<<(unsigned)grid, PACK_THREADS, 0, st>>>(prm);
-    else k_pack_items<TC_BF16, false><<<(unsigned)grid, PACK_THREADS, 0, st>>>(prm);
+    if (src_is_f32) launch(k_pack_items<TC_BF16, true>);
+    else launch(k_pack_items<TC_BF16, false>);
   }
   CTN_CHECK_LAUNCH();
   return CTN_OK;

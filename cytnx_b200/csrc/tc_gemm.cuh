@@ -136,6 +136,19 @@ struct Packer {
 
 // compiled tile widths: positive = 1-CTA tile of 128 x bn, negative = 2-CTA tile of 256 x |bn|
 bool tc_tile_width_supported(int width);
+// SM count of the current device (148 when it cannot be queried)
+int nsm_count();
+// resident CTAs per SM of a kernel at a block size (queried once per kernel)
+template <class K>
+int resident_ctas(K kernel, int threads) {
+  static int occ = 0;
+  if (!occ) {
+    int o = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kernel, threads, 0) != cudaSuccess) cudaGetLastError();
+    occ = o > 0 ? o : 4;
+  }
+  return occ;
+}
 
 // Work items of `per_item` consecutive chunks over segments with chunk prefix sums
 // `begin`; each item records the first and last segment it overlaps (seg0, seg1).
