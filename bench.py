@@ -42,7 +42,7 @@ sys.path.insert(0, ROOT)
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--D", type=int, default=4096)
@@ -70,28 +70,60 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+    """SM clocks, power and clock-event (throttle) reasons sampled during the timed region:
+    through NVML every 10 ms when the bindings are importable, else nvidia-smi every 200 ms.
+    Read-only: no GPU setting is changed."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    _BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
     def __init__(self, index: int):
         self.index = index
+        self.uuid = None
         try:
             import torch
 
             u = str(torch.cuda.get_device_properties(index).uuid)
-            self.index = u if u.startswith("GPU-") else f"GPU-{u}"
+            self.uuid = u if u.startswith("GPU-") else f"GPU-{u}"
+            self.index = self.uuid
         except Exception:
             pass
         self.rows = []
         self._stop = threading.Event()
         self._t = None
+        self._nvml = None
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByUUID(self.uuid) if self.uuid else pynvml.nvmlDeviceGetHandleByIndex(index)
+            self._nvml = (pynvml, h)
+        except Exception:
+            self._nvml = None
+
+    def _sample_nvml(self):
+        nv, h = self._nvml
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+        try:
+            rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        except Exception:
+            rs = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+        act = lambda k: "Active" if rs & self._BITS[k] else "Not Active"  # noqa: E731
+        self.rows.append([str(self.index), str(sm), str(mx), f"{pw:.1f}", hex(rs), act("hw_slowdown"),
+                          act("hw_thermal_slowdown"), act("sw_thermal_slowdown"), act("sw_power_cap")])
 
     def _run(self):
         while not self._stop.is_set():
             try:
+                if self._nvml is not None:
+                    self._sample_nvml()
+                    self._stop.wait(0.01)
+                    continue
                 r = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
                                     "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
                 if r.returncode == 0 and r.stdout.strip():
