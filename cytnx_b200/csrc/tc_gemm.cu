@@ -11,6 +11,7 @@
 //                        overlap the main loop of tile i+1.
 // Every wait is bounded: on expiry the kernel records an error code in p.err, drains
 // its own bulk copies and MMAs (again bounded), frees its TMEM and returns.
+#include <cuda.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -398,11 +399,13 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
 // halves, and each CTA's TMEM receives the accumulator rows of its own 128 rows.  Per SM
 // this moves half of B per tile, so the operand ingest per flop drops by a third (BN=128)
 // to a half (BN=256) against the 1-CTA form.
-// Synchronisation: the follower's bulk copies complete on its own full barrier and its
-// relay thread (warp 1) forwards each completion to the leader's full barrier with a
-// remote arrive; the leader's MMA commits are multicast to both CTAs' empty / tfull
-// barriers; the follower's epilogue warps arrive on the leader's tempty barriers.  Every
-// wait is bounded; both CTAs meet at a cluster barrier before TMEM is released.
+// Synchronisation: both CTAs load their operand slices with 2-D TMA copies of the
+// (pre-swizzled) panels in the cta_group::2 form, which completes the bytes on the
+// leader's full barrier; the leader's producer expects the bytes of both CTAs.  The
+// leader's MMA commits are multicast to both CTAs' empty / tfull barriers; the
+// follower's epilogue warps arrive on the leader's tempty barriers.  Every wait is
+// bounded; both CTAs meet at a cluster barrier before TMEM is released.  No load is a
+// multicast: each CTA reads its own slices of this GPU's memory.
 __device__ __forceinline__ uint32_t cluster_rank() {
   uint32_t r;
   asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
@@ -413,6 +416,16 @@ __device__ __forceinline__ uint32_t peer_addr(const void *p, uint32_t rank) {
   uint32_t r;
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
   return r;
+}
+// 2-D TMA load of `rows` rows x 128 bytes at row y of a panel viewed as [rows][128 B]
+// (no swizzle: the panel bytes are copied as they are); completes on the leader's
+// barrier `bar_cluster` (cta_group::2)
+__device__ __forceinline__ void tma_rows_pair(void *dst, const CUtensorMap *map, int y, uint32_t bar_cluster) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+      "[%4];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(y), "r"(bar_cluster)
+      : "memory");
 }
 __device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
   asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
@@ -459,7 +472,10 @@ struct TcSmem2 {
 };
 
 template <int KIND, int BN, int STAGES>
-__global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p) {
+__global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p, const __grid_constant__ CUtensorMap ta_hi,
+                                                                  const __grid_constant__ CUtensorMap ta_lo,
+                                                                  const __grid_constant__ CUtensorMap tb_hi,
+                                                                  const __grid_constant__ CUtensorMap tb_lo) {
   using SM = TcSmem2<KIND, BN, STAGES>;
   static_assert(BN % 16 == 0 && BN >= 32 && BN <= 256, "2-CTA tile width");
   extern __shared__ uint8_t smem_raw[];
@@ -477,7 +493,7 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p) {
   constexpr uint32_t TMEM_COLS = 2 * BN <= 64 ? 64 : 2 * BN <= 128 ? 128 : 2 * BN <= 256 ? 256 : 512;
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
-      mbar_init(&full[s], rank == 0 ? 2 : 1);  // leader: own copies + the follower's relay
+      mbar_init(&full[s], 1);  // leader: its producer's expect_tx (bytes of both CTAs)
       mbar_init(&empty[s], 1);
     }
     for (int a = 0; a < 2; ++a) {
@@ -519,13 +535,16 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p) {
           break;
         }
         uint8_t *st = smem + stage * SM::STAGE_BYTES;
-        mbar_expect_tx(&full[stage], SM::STAGE_BYTES);
-        const int64_t ao = g.a_off + ((int64_t)mt128 * g.kb + kb) * SM::A_BYTES;
-        const int64_t bo = g.b_off + ((int64_t)tl.nt * g.kb + kb) * (2 * SM::B_BYTES) + (int64_t)rank * SM::B_BYTES;
-        bulk_g2s(st, p.a_hi + ao, SM::A_BYTES, &full[stage]);
-        bulk_g2s(st + SM::A_BYTES, p.a_lo + ao, SM::A_BYTES, &full[stage]);
-        bulk_g2s(st + 2 * SM::A_BYTES, p.b_hi + bo, SM::B_BYTES, &full[stage]);
-        bulk_g2s(st + 2 * SM::A_BYTES + SM::B_BYTES, p.b_lo + bo, SM::B_BYTES, &full[stage]);
+        if (rank == 0) mbar_expect_tx(&full[stage], 2 * SM::STAGE_BYTES);
+        const uint32_t fb = peer_addr(&full[stage], 0);
+        // panel rows of 128 bytes: A tile (mt128, kb) and this CTA's half of B tile (nt, kb)
+        const int ya = (int)((g.a_off + ((int64_t)mt128 * g.kb + kb) * SM::A_BYTES) / TC_ROW_BYTES);
+        const int yb = (int)((g.b_off + ((int64_t)tl.nt * g.kb + kb) * (2 * SM::B_BYTES) + (int64_t)rank * SM::B_BYTES) /
+                             TC_ROW_BYTES);
+        tma_rows_pair(st, &ta_hi, ya, fb);
+        tma_rows_pair(st + SM::A_BYTES, &ta_lo, ya, fb);
+        tma_rows_pair(st + 2 * SM::A_BYTES, &tb_hi, yb, fb);
+        tma_rows_pair(st + 2 * SM::A_BYTES + SM::B_BYTES, &tb_lo, yb, fb);
         filled[stage]++;
         if (++stage == STAGES) {
           stage = 0;
@@ -533,28 +552,11 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p) {
         }
       }
     }
-    // drain: every issued fill must have landed before the CTA may exit (bounded)
-    for (int s = 0; s < STAGES; ++s)
-      if (filled[s]) mbar_wait(&full[s], (filled[s] - 1) & 1, p.err, 5);
-  } else if (warp == 1 && lane == 0 && rank == 1) {
-    // ---------------------------------------------------------------- relay (follower)
-    int stage = 0;
-    uint32_t phase = 0;
-    bool ok = true;
-    for (int64_t t = pair; t < p.ntiles && ok; t += npairs) {
-      const TcGroup g = p.groups[p.tiles[t].group];
-      for (int kb = 0; kb < g.kb; ++kb) {
-        if (!mbar_wait(&full[stage], phase, p.err, 7)) {
-          ok = false;
-          break;
-        }
-        mbar_arrive_remote(peer_addr(&full[stage], 0));
-        if (++stage == STAGES) {
-          stage = 0;
-          phase ^= 1;
-        }
-      }
-    }
+    // drain: the leader's full barriers count the bytes of both CTAs, so the leader waits
+    // for every issued fill; the follower is held at the final cluster barrier meanwhile
+    if (rank == 0)
+      for (int s = 0; s < STAGES; ++s)
+        if (filled[s]) mbar_wait(&full[s], (filled[s] - 1) & 1, p.err, 5);
   } else if (warp == 1 && lane == 0 && rank == 0) {
     // ---------------------------------------------------------------- MMA issuer (leader)
     int stage = 0;
@@ -875,6 +877,22 @@ ctn_status launch_tc(const TcParams &prm, int64_t ntiles, cudaStream_t st) {
   return CTN_OK;
 }
 
+// 2-D view [bytes / 128][128] (uint8, no swizzle) of a panel buffer, boxes of `box_rows` rows
+static ctn_status encode_rows_map(CUtensorMap *m, const void *base, int64_t bytes, int box_rows) {
+  const cuuint64_t dims[2] = {128, (cuuint64_t)(bytes / 128)};
+  const cuuint64_t strides[1] = {128};
+  const cuuint32_t box[2] = {128, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = cuTensorMapEncodeTiled(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void *>(base), dims, strides,
+                                            box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("tcgen05 2-CTA GEMM: cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return CTN_ERR_CUDA;
+  }
+  return CTN_OK;
+}
+
 template <int KIND, int BN, int STAGES>
 ctn_status launch_tc_pair(const TcParams &prm, int64_t ntiles, cudaStream_t st) {
   using SM = TcSmem2<KIND, BN, STAGES>;
@@ -900,7 +918,14 @@ ctn_status launch_tc_pair(const TcParams &prm, int64_t ntiles, cudaStream_t st) 
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  CTN_CUDA(cudaLaunchKernelEx(&cfg, k_tc_gemm_pair<KIND, BN, STAGES>, prm));
+  CUtensorMap ma_hi, ma_lo, mb_hi, mb_lo;
+  CTN_REQUIRE(prm.a_bytes > 0 && prm.b_bytes > 0 && prm.a_bytes % 128 == 0 && prm.b_bytes % 128 == 0,
+              "tcgen05 2-CTA GEMM: panel sizes unknown");
+  CTN_TRY(encode_rows_map(&ma_hi, prm.a_hi, prm.a_bytes, TC_BM));
+  CTN_TRY(encode_rows_map(&ma_lo, prm.a_lo, prm.a_bytes, TC_BM));
+  CTN_TRY(encode_rows_map(&mb_hi, prm.b_hi, prm.b_bytes, BN / 2));
+  CTN_TRY(encode_rows_map(&mb_lo, prm.b_lo, prm.b_bytes, BN / 2));
+  CTN_CUDA(cudaLaunchKernelEx(&cfg, k_tc_gemm_pair<KIND, BN, STAGES>, prm, ma_hi, ma_lo, mb_hi, mb_lo));
   return CTN_OK;
 }
 
@@ -1024,6 +1049,8 @@ ctn_status TcGemm::run(const uint8_t *a_hi, const uint8_t *a_lo, const uint8_t *
   prm.rowmap = (const int64_t *)(q + groups.size() * sizeof(TcGroup) + tiles.size() * sizeof(TcTile));
   prm.ntiles = (int64_t)tiles.size();
   prm.epi_staged = epi_staged ? 1 : 0;
+  prm.a_bytes = a_bytes;
+  prm.b_bytes = b_bytes;
   prm.a_hi = a_hi;
   prm.a_lo = a_lo;
   prm.b_hi = b_hi;
@@ -1044,6 +1071,8 @@ ctn_status tc_launch_tables(int kind, int bn, const TcGroup *d_groups, const TcT
   prm.rowmap = d_rowmap;
   prm.ntiles = ntiles;
   prm.epi_staged = 0;
+  prm.a_bytes = 0;
+  prm.b_bytes = 0;
   prm.a_hi = a_hi;
   prm.a_lo = a_lo;
   prm.b_hi = b_hi;

@@ -52,6 +52,7 @@ struct TcParams {
   const int64_t *rowmap;
   int *err;  // device error word: 0 ok, else the code of the wait that gave up
   int epi_staged;  // 1: epilogue through the shared-memory slab (whole row segments), 0: direct
+  int64_t a_bytes, b_bytes;  // panel sizes (2-CTA form: extents of its TMA views)
 };
 
 // byte offset of element (r, k) inside a panel of tiles with `rows` rows per tile
