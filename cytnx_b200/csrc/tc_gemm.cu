@@ -11,13 +11,13 @@
 //                        overlap the main loop of tile i+1.
 // Every wait is bounded: on expiry the kernel records an error code in p.err, drains
 // its own bulk copies and MMAs (again bounded), frees its TMEM and returns.
-#include <cuda.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
 #include <cstring>
 
 #include "tc_gemm.cuh"
+#include "tmap.h"
 
 namespace ctn {
 
@@ -883,7 +883,12 @@ static ctn_status encode_rows_map(CUtensorMap *m, const void *base, int64_t byte
   const cuuint64_t strides[1] = {128};
   const cuuint32_t box[2] = {128, (cuuint32_t)box_rows};
   const cuuint32_t estr[2] = {1, 1};
-  const CUresult r = cuTensorMapEncodeTiled(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void *>(base), dims, strides,
+  const EncodeTiledFn enc = encode_tiled();
+  if (!enc) {
+    set_error("tcgen05 2-CTA GEMM: the driver provides no cuTensorMapEncodeTiled");
+    return CTN_ERR_UNSUPPORTED;
+  }
+  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void *>(base), dims, strides,
                                             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
