@@ -432,6 +432,7 @@ def main():
     roof.update({"unit": "TFLOP/s", "frac": roof["achieved"] / roof["peak"], "traffic": None,
                  "kernel_flops_per_matvec": g_flops, "kernel_ms_per_matvec": g_ms})
     clocks = sampler.summary()
+    permute = run_permute(args, dev, st, pk.get("hbm_gbs"))
     batched = run_batched(args, world, rank, dev, st) if args.batch_problems > 0 else None
     mps_ad = run_mps_autograd(args, dev) if args.mps_lbfgs_steps > 0 else None
     if rank == 0:
@@ -467,6 +468,7 @@ def main():
                       "dgemm_tflops_measured": dgemm_tflops, "tf32_tflops_measured": tf32_tflops},
             "clocks": clocks,
             "cpu_baseline": cpu,
+            "permute": permute,
             "batched_hubbard": batched,
             "autograd_mps": mps_ad,
         }
@@ -550,6 +552,61 @@ def run_batched(args, world, rank, dev, st):
         rec["rel_err_vs_fp64_median_rank0"] = float(e.median().item())
         del rec["_B"], rec["_y"]
     out["setup_s"] = time.perf_counter() - t_setup
+    return out
+
+
+def run_permute(args, dev, st, hbm_peak):
+    """Tensor permute + contiguous (ctn_permute): the configuration's 24 permutations of a
+    [64,2,2,64] float64 tensor (L2-resident, launch-latency bound) and HBM-bound
+    transposes of 512 MB tensors; GB/s = 2 x bytes / device time."""
+    import itertools
+
+    import torch
+
+    from cytnx_b200 import _lib
+
+    lib = _lib.lib()
+
+    def timed(x, perm, reps):
+        y = torch.empty_like(x)
+        did = {torch.float64: 3, torch.float32: 4, torch.int16: 9}[x.dtype]
+        osh = np.array(x.shape, dtype=np.uint64)
+        mp = np.array(perm, dtype=np.uint64)
+
+        def go():
+            _lib.check(lib.ctn_permute(x.data_ptr(), y.data_ptr(), did, x.dim(), osh.ctypes.data_as(_lib.P_u64),
+                                       mp.ctypes.data_as(_lib.P_u64), _lib.stream_ptr()), "permute")
+        go()
+        torch.cuda.synchronize()
+        if not torch.equal(y.reshape(-1), x.permute(*perm).contiguous().reshape(-1)):
+            raise RuntimeError(f"permute mismatch for {tuple(x.shape)} {perm}")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            go()
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        return ms, 2 * x.numel() * x.element_size() / (ms * 1e-3) / 1e9
+
+    out = {"small": {}, "large": []}
+    x = torch.randn(64, 2, 2, 64, dtype=torch.float64, device=dev)
+    tot = 0.0
+    for perm in itertools.permutations(range(4)):
+        ms, _ = timed(x, perm, 200)
+        tot += ms
+    out["small"] = {"shape": [64, 2, 2, 64], "dtype": "f64", "perms": 24, "total_ms_24": tot,
+                    "mean_us_per_perm": tot / 24 * 1e3, "bytes_per_perm": 2 * x.numel() * 8}
+    for shape, perm, dt in (((2048, 4, 4, 2048), (3, 1, 2, 0), torch.float64),
+                            ((2048, 4, 4, 2048), (0, 2, 1, 3), torch.float64),
+                            ((2048, 4, 4, 2048), (1, 0, 3, 2), torch.float64),
+                            ((4096, 4, 4, 4096), (3, 1, 2, 0), torch.float32),
+                            ((4096, 4, 4, 4096), (3, 1, 2, 0), torch.int16)):
+        xl = (torch.randn(*shape, device=dev) * 100).to(dt)
+        ms, gbs = timed(xl, perm, 20)
+        out["large"].append({"shape": list(shape), "perm": list(perm), "dtype": str(dt).replace("torch.", ""),
+                             "ms": ms, "GB_s": gbs, "frac_of_hbm": gbs / hbm_peak if hbm_peak else None})
+        del xl
     return out
 
 
