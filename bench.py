@@ -433,6 +433,7 @@ def main():
                  "kernel_flops_per_matvec": g_flops, "kernel_ms_per_matvec": g_ms})
     clocks = sampler.summary()
     permute = run_permute(args, dev, st, pk.get("hbm_gbs"))
+    fp64_d1024 = run_fp64_d1024(args, dev, st)
     batched = run_batched(args, world, rank, dev, st) if args.batch_problems > 0 else None
     mps_ad = run_mps_autograd(args, dev) if args.mps_lbfgs_steps > 0 else None
     if rank == 0:
@@ -469,6 +470,7 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cpu,
             "permute": permute,
+            "fp64_D1024": fp64_d1024,
             "batched_hubbard": batched,
             "autograd_mps": mps_ad,
         }
@@ -553,6 +555,54 @@ def run_batched(args, world, rank, dev, st):
         del rec["_B"], rec["_y"]
     out["setup_s"] = time.perf_counter() - t_setup
     return out
+
+
+def run_fp64_d1024(args, dev, st):
+    """Plain FP64 U(1) configuration: two-site XXZ H_eff at D=1024, 40 Lanczos iterations
+    (the reference's Gnd recurrence) and the block SVD truncation of the ground state back
+    to D (Svd_truncate, rowrank 2: (a, s1) | (s2, b))."""
+    import torch
+
+    import cytnx_b200 as c
+    from cytnx_b200 import workloads as W
+
+    spec = W.xxz_spec(1024)
+    mpo = W.xxz_mpo_values(1.0, 1.0, 0.0)
+    psi, L, M1, M2, R = W.build_two_site(spec, mpo, seed=0, device=dev.index)
+    H = c.TwoSiteHeff(L, M1, M2, R, psi, precision="fp64")
+    flops = H.algorithmic_flops()
+    x = psi.flat_view()
+    y = torch.empty_like(x)
+    for _ in range(5):
+        H.apply_flat(x, y, "fp64")
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 200
+    e0.record(st)
+    for _ in range(reps):
+        H.apply_flat(x, y, "fp64")
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    H.lanczos(psi, maxiter=4, cvgcrit=1e-300)  # warm
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    E, vec, it = H.lanczos(psi, maxiter=40, cvgcrit=1e-300)
+    torch.cuda.synchronize()
+    t_lan = time.perf_counter() - t0
+    vec.set_rowrank_(2)
+    c.linalg.Svd_truncate(vec, 1024)  # warm (cuSOLVER handles)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    S, U, Vt = c.linalg.Svd_truncate(vec, 1024)
+    torch.cuda.synchronize()
+    t_svd = time.perf_counter() - t0
+    s = S.flat_view()
+    kept = int(S.shape()[0])
+    return {"workload": "u1_xxz_two_site_heff_D1024_fp64", "algorithmic_flops_per_matvec": flops,
+            "matvec_ms": ms, "matvec_tflops": flops / (ms * 1e-3) / 1e12, "lanczos_iters": it,
+            "lanczos_s_per_step": t_lan / max(it, 1), "energy_40": E, "svd_truncate_s": t_svd,
+            "svd_kept": kept, "svd_norm2_kept": float((s * s).sum().item())}
 
 
 def run_permute(args, dev, st, hbm_peak):
