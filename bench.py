@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--matvec-only", action="store_true",
                     help="profiling driver: bind the headline form with --tiles, run warmup + steps matvecs, exit")
     ap.add_argument("--tiles", default="", help="step-1,step-4 tile widths for --matvec-only (e.g. 192,128)")
+    ap.add_argument("--permute-only", action="store_true",
+                    help="profiling driver: the large permutes of the permute section, once each, then exit")
     ap.add_argument("--batch-only", type=int, default=0,
                     help="profiling driver: the first N batched Hubbard problems, headline form, --tiles, eager matvecs")
     ap.add_argument("--mps-lbfgs-steps", type=int, default=200,
@@ -208,6 +210,11 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
     from cytnx_b200 import workloads as W
+
+    if args.permute_only:  # one launch per large permute (after one untimed warm launch each)
+        out = run_permute(args, torch.device(f"cuda:{local}"), torch.cuda.current_stream(), None, reps=1, small=False)
+        print(json.dumps({"permute_only": True, "large": [(o["shape"], o["perm"], o["dtype"]) for o in out["large"]]}))
+        return
 
     if args.batch_only > 0:  # small fixed launch sequence of the batched path for ncu
         from cytnx_b200.batch import BatchedTwoSiteHeff
@@ -605,7 +612,7 @@ def run_fp64_d1024(args, dev, st):
             "svd_kept": kept, "svd_norm2_kept": float((s * s).sum().item())}
 
 
-def run_permute(args, dev, st, hbm_peak):
+def run_permute(args, dev, st, hbm_peak, reps=None, small=True):
     """Tensor permute + contiguous (ctn_permute): the configuration's 24 permutations of a
     [64,2,2,64] float64 tensor (L2-resident, launch-latency bound) and HBM-bound
     transposes of 512 MB tensors; GB/s = 2 x bytes / device time."""
@@ -642,8 +649,8 @@ def run_permute(args, dev, st, hbm_peak):
     out = {"small": {}, "large": []}
     x = torch.randn(64, 2, 2, 64, dtype=torch.float64, device=dev)
     tot = 0.0
-    for perm in itertools.permutations(range(4)):
-        ms, _ = timed(x, perm, 200)
+    for perm in itertools.permutations(range(4)) if small else ():
+        ms, _ = timed(x, perm, reps or 200)
         tot += ms
     out["small"] = {"shape": [64, 2, 2, 64], "dtype": "f64", "perms": 24, "total_ms_24": tot,
                     "mean_us_per_perm": tot / 24 * 1e3, "bytes_per_perm": 2 * x.numel() * 8}
@@ -653,7 +660,7 @@ def run_permute(args, dev, st, hbm_peak):
                             ((4096, 4, 4, 4096), (3, 1, 2, 0), torch.float32),
                             ((4096, 4, 4, 4096), (3, 1, 2, 0), torch.int16)):
         xl = (torch.randn(*shape, device=dev) * 100).to(dt)
-        ms, gbs = timed(xl, perm, 20)
+        ms, gbs = timed(xl, perm, reps or 20)
         out["large"].append({"shape": list(shape), "perm": list(perm), "dtype": str(dt).replace("torch.", ""),
                              "ms": ms, "GB_s": gbs, "frac_of_hbm": gbs / hbm_peak if hbm_peak else None})
         del xl
