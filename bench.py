@@ -371,7 +371,8 @@ def main():
     # ---- Lanczos (the reference's Gnd recurrence, fixed iteration count): seconds per step
     lanczos = {}
     for form in forms:
-        H.lanczos(psi, maxiter=4, cvgcrit=1e-300, precision=form)  # warm: Krylov buffers, first-call costs
+        # warm at the same size: the Krylov buffers come from the caching allocator afterwards
+        H.lanczos(psi, maxiter=args.lanczos_iters, cvgcrit=1e-300, precision=form)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         E, vec, it = H.lanczos(psi, maxiter=args.lanczos_iters, cvgcrit=1e-300, precision=form)

@@ -120,28 +120,6 @@ __global__ void __launch_bounds__(RT) k_lanczos_update(double *__restrict__ w, c
   finish(s, partials, ticket, nrm, 1);
 }
 
-// w -= alpha*p1 + beta*p0 + gamma*q, ||w|| to *nrm (p0 / q may be null)
-__global__ void __launch_bounds__(RT) k_lanczos_update3(double *__restrict__ w, const double *__restrict__ p1,
-                                                       const double *__restrict__ p0, const double *__restrict__ q,
-                                                       int64_t n, const double *alpha, const double *beta,
-                                                       const double *gamma, double *partials, unsigned *ticket,
-                                                       double *nrm) {
-  const double a = *alpha;
-  const double b = p0 ? *beta : 0.0;
-  const double c = q ? *gamma : 0.0;
-  double s = 0.0;
-  const int64_t step = (int64_t)gridDim.x * RT;
-  for (int64_t i = (int64_t)blockIdx.x * RT + threadIdx.x; i < n; i += step) {
-    double v = w[i] - a * p1[i];
-    if (p0) v -= b * p0[i];
-    if (q) v -= c * q[i];
-    w[i] = v;
-    s = fma(v, v, s);
-  }
-  s = block_sum(s);
-  finish(s, partials, ticket, nrm, 1);
-}
-
 // y = x / *a (y = 0 when *a is zero: a Lanczos breakdown leaves the next vector empty)
 __global__ void __launch_bounds__(RT) k_div_copy(const double *__restrict__ x, double *__restrict__ y,
                                                 int64_t n, const double *a) {
@@ -151,16 +129,55 @@ __global__ void __launch_bounds__(RT) k_div_copy(const double *__restrict__ x, d
   for (int64_t i = (int64_t)blockIdx.x * RT + threadIdx.x; i < n; i += step) y[i] = zero ? 0.0 : x[i] / al;
 }
 
-// <w, a> and <w, b> in one pass over w (two reductions, partials side by side)
-__global__ void __launch_bounds__(RT) k_dot2(const double *__restrict__ w, const double *__restrict__ a,
-                                            const double *__restrict__ b, int64_t n, double *partials,
-                                            unsigned *ticket, double *out_a, double *out_b) {
+// ---- Krylov steps on unnormalised storage.  The restarted Lanczos keeps u_j = s_j q_j
+// (s_j = |u_j|, a device scalar) instead of normalising every new vector in a separate
+// pass: the matvec is linear, so w = H u_j serves for H q_j = w / s_j, and the scale
+// goes into the coefficients.  Both kernels read 16-byte vectors, two per array per
+// thread and iteration, when every pointer is 16-byte aligned.
+
+__device__ __forceinline__ double safe_inv(double s) { return s != 0.0 ? 1.0 / s : 0.0; }
+
+// <w, a> / s^2 and <w, b> / s in one pass (s = *s_ptr, 1 when s_ptr is null; a zero s
+// gives zeros: the vector behind it is empty after a breakdown)
+template <bool VEC>
+__global__ void __launch_bounds__(RT) k_dot2s(const double *__restrict__ w, const double *__restrict__ a,
+                                             const double *__restrict__ b, int64_t n, const double *s_ptr,
+                                             double *partials, unsigned *ticket, double *out_a, double *out_b) {
   double sa = 0.0, sb = 0.0;
+  const int64_t tid = (int64_t)blockIdx.x * RT + threadIdx.x;
   const int64_t step = (int64_t)gridDim.x * RT;
-  for (int64_t i = (int64_t)blockIdx.x * RT + threadIdx.x; i < n; i += step) {
-    const double x = w[i];
-    sa = fma(x, a[i], sa);
-    sb = fma(x, b[i], sb);
+  if (VEC) {
+    const int64_t n2 = n / 2;
+    const double2 *w2 = reinterpret_cast<const double2 *>(w), *a2 = reinterpret_cast<const double2 *>(a),
+                  *b2 = reinterpret_cast<const double2 *>(b);
+    for (int64_t i = tid; i < n2; i += 2 * step) {
+      const bool two = i + step < n2;
+      const double2 x0 = w2[i], y0 = a2[i], z0 = b2[i];
+      double2 x1 = make_double2(0.0, 0.0), y1 = x1, z1 = x1;
+      if (two) {
+        x1 = w2[i + step];
+        y1 = a2[i + step];
+        z1 = b2[i + step];
+      }
+      sa = fma(x0.x, y0.x, sa);
+      sa = fma(x0.y, y0.y, sa);
+      sb = fma(x0.x, z0.x, sb);
+      sb = fma(x0.y, z0.y, sb);
+      sa = fma(x1.x, y1.x, sa);
+      sa = fma(x1.y, y1.y, sa);
+      sb = fma(x1.x, z1.x, sb);
+      sb = fma(x1.y, z1.y, sb);
+    }
+    if (tid == 0 && (n & 1)) {
+      sa = fma(w[n - 1], a[n - 1], sa);
+      sb = fma(w[n - 1], b[n - 1], sb);
+    }
+  } else {
+    for (int64_t i = tid; i < n; i += step) {
+      const double x = w[i];
+      sa = fma(x, a[i], sa);
+      sb = fma(x, b[i], sb);
+    }
   }
   sa = block_sum(sa);
   sb = block_sum(sb);
@@ -182,10 +199,65 @@ __global__ void __launch_bounds__(RT) k_dot2(const double *__restrict__ w, const
   va = block_sum(va);
   vb = block_sum(vb);
   if (threadIdx.x == 0) {
-    *out_a = va;
-    *out_b = vb;
+    const double inv = s_ptr ? safe_inv(*s_ptr) : 1.0;
+    *out_a = va * inv * inv;
+    *out_b = vb * inv;
     *ticket = 0u;
   }
+}
+
+// dst = (w - alpha u) / s - (s / sp) up - gamma q,  ||dst|| -> *nrm.  alpha and gamma are
+// the coefficients of q_j = u / s (from k_dot2s with the same s); up = u_{j-1} with its
+// own scale sp, so (s / sp) up = beta_{j-1} q_{j-1}.  up and q may be null.
+template <bool VEC>
+__global__ void __launch_bounds__(RT) k_lanczos_step(const double *__restrict__ w, const double *__restrict__ u,
+                                                    const double *__restrict__ up, const double *__restrict__ q,
+                                                    double *__restrict__ dst, int64_t n, const double *alpha,
+                                                    const double *gamma, const double *s_ptr, const double *sp_ptr,
+                                                    double *partials, unsigned *ticket, double *nrm) {
+  const double s = *s_ptr;
+  const double inv = safe_inv(s);
+  const double ca = *alpha * inv;
+  const double cp = up ? s * safe_inv(*sp_ptr) : 0.0;
+  const double cg = q ? *gamma : 0.0;
+  double acc = 0.0;
+  const int64_t tid = (int64_t)blockIdx.x * RT + threadIdx.x;
+  const int64_t step = (int64_t)gridDim.x * RT;
+  auto one = [&](double wv, double uv, double pv, double qv) -> double {
+    double v = fma(-ca, uv, wv * inv);
+    v = fma(-cp, pv, v);
+    v = fma(-cg, qv, v);
+    acc = fma(v, v, acc);
+    return v;
+  };
+  if (VEC) {
+    const int64_t n2 = n / 2;
+    const double2 *w2 = reinterpret_cast<const double2 *>(w), *u2 = reinterpret_cast<const double2 *>(u),
+                  *p2 = reinterpret_cast<const double2 *>(up), *q2 = reinterpret_cast<const double2 *>(q);
+    double2 *d2 = reinterpret_cast<double2 *>(dst);
+    const double2 z = make_double2(0.0, 0.0);
+    for (int64_t i = tid; i < n2; i += 2 * step) {
+      const bool two = i + step < n2;
+      const double2 w0 = w2[i], u0 = u2[i], p0 = up ? p2[i] : z, q0 = q ? q2[i] : z;
+      double2 w1 = z, u1 = z, p1 = z, q1 = z;
+      if (two) {
+        w1 = w2[i + step];
+        u1 = u2[i + step];
+        if (up) p1 = p2[i + step];
+        if (q) q1 = q2[i + step];
+      }
+      d2[i] = make_double2(one(w0.x, u0.x, p0.x, q0.x), one(w0.y, u0.y, p0.y, q0.y));
+      if (two) d2[i + step] = make_double2(one(w1.x, u1.x, p1.x, q1.x), one(w1.y, u1.y, p1.y, q1.y));
+    }
+    if (tid == 0 && (n & 1)) {
+      const int64_t k = n - 1;
+      dst[k] = one(w[k], u[k], up ? up[k] : 0.0, q ? q[k] : 0.0);
+    }
+  } else {
+    for (int64_t i = tid; i < n; i += step) dst[i] = one(w[i], u[i], up ? up[i] : 0.0, q ? q[i] : 0.0);
+  }
+  acc = block_sum(acc);
+  finish(acc, partials, ticket, nrm, 1);
 }
 
 // out = sum_j c[j] * K[j]  (Krylov combination), c on device
@@ -215,15 +287,7 @@ int grid_for(int64_t n) {
 size_t reduce_ws_bytes() { return (MAXCTA + 8) * sizeof(double); }
 size_t reduce2_ws_bytes() { return (2 * MAXCTA + 8) * sizeof(double); }
 
-// ws2 layout: [2 * MAXCTA partials][ticket]
-ctn_status dot2_f64(const double *w, const double *a, const double *b, int64_t n, double *out_a, double *out_b,
-                    double *ws2, cudaStream_t st) {
-  const int g = grid_for(n);
-  k_dot2<<<g, RT, 0, st>>>(w, a, b, n, ws2, reinterpret_cast<unsigned *>(ws2 + 2 * MAXCTA), out_a, out_b);
-  CTN_CHECK_LAUNCH();
-  return CTN_OK;
-}
-
+// ws2 layout (dot2s_f64): [2 * MAXCTA partials][ticket]
 // ws layout: [partials MAXCTA doubles][ticket (8 bytes)]
 ctn_status dot_f64(const double *x, const double *y, int64_t n, double *out, double *ws, cudaStream_t st) {
   int g = grid_for(n);
@@ -254,15 +318,34 @@ ctn_status lanczos_update_f64(double *w, const double *p1, const double *p0, int
   CTN_CHECK_LAUNCH();
   return CTN_OK;
 }
-ctn_status lanczos_update3_f64(double *w, const double *p1, const double *p0, const double *q, int64_t n,
-                               const double *alpha, const double *beta, const double *gamma, double *nrm, double *ws,
-                               cudaStream_t st) {
-  const int g = std::min(grid_for(n), MAXCTA);
-  k_lanczos_update3<<<g, RT, 0, st>>>(w, p1, p0, q, n, alpha, beta, gamma, ws,
-                                      reinterpret_cast<unsigned *>(ws + MAXCTA), nrm);
+static bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+ctn_status dot2s_f64(const double *w, const double *a, const double *b, int64_t n, const double *s, double *out_a,
+                     double *out_b, double *ws2, cudaStream_t st) {
+  const int g = grid_for(n);
+  unsigned *ticket = reinterpret_cast<unsigned *>(ws2 + 2 * MAXCTA);
+  if (aligned16(w) && aligned16(a) && aligned16(b))
+    k_dot2s<true><<<g, RT, 0, st>>>(w, a, b, n, s, ws2, ticket, out_a, out_b);
+  else
+    k_dot2s<false><<<g, RT, 0, st>>>(w, a, b, n, s, ws2, ticket, out_a, out_b);
   CTN_CHECK_LAUNCH();
   return CTN_OK;
 }
+
+ctn_status lanczos_step_f64(const double *w, const double *u, const double *up, const double *q, double *dst,
+                            int64_t n, const double *alpha, const double *gamma, const double *s, const double *sp,
+                            double *nrm, double *ws, cudaStream_t st) {
+  const int g = grid_for(n);
+  unsigned *ticket = reinterpret_cast<unsigned *>(ws + MAXCTA);
+  const bool vec = aligned16(w) && aligned16(u) && aligned16(dst) && (!up || aligned16(up)) && (!q || aligned16(q));
+  if (vec)
+    k_lanczos_step<true><<<g, RT, 0, st>>>(w, u, up, q, dst, n, alpha, gamma, s, sp, ws, ticket, nrm);
+  else
+    k_lanczos_step<false><<<g, RT, 0, st>>>(w, u, up, q, dst, n, alpha, gamma, s, sp, ws, ticket, nrm);
+  CTN_CHECK_LAUNCH();
+  return CTN_OK;
+}
+
 ctn_status div_copy_f64(const double *x, double *y, int64_t n, const double *a, cudaStream_t st) {
   k_div_copy<<<grid_for(n), RT, 0, st>>>(x, y, n, a);
   CTN_CHECK_LAUNCH();

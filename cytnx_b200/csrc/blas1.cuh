@@ -5,19 +5,22 @@
 namespace ctn {
 // bytes of the reduction workspace (partials + ticket); must be zeroed once before first use
 size_t reduce_ws_bytes();
-// the same for dot2_f64 (two reductions in one pass)
+// the same for dot2s_f64 (two reductions in one pass)
 size_t reduce2_ws_bytes();
-ctn_status dot2_f64(const double *w, const double *a, const double *b, int64_t n, double *out_a, double *out_b,
-                    double *ws2, cudaStream_t st);
 ctn_status dot_f64(const double *x, const double *y, int64_t n, double *out, double *ws, cudaStream_t st);
 ctn_status nrm2_f64(const double *x, int64_t n, double *out, double *ws, cudaStream_t st);
 ctn_status axpy_f64(const double *x, double *y, int64_t n, const double *a, double a_scale, cudaStream_t st);
 ctn_status scal_f64(double *x, int64_t n, const double *a, int invert, cudaStream_t st);
 ctn_status lanczos_update_f64(double *w, const double *p1, const double *p0, int64_t n, const double *alpha,
                               const double *beta, double *nrm, double *ws, cudaStream_t st);
-ctn_status lanczos_update3_f64(double *w, const double *p1, const double *p0, const double *q, int64_t n,
-                               const double *alpha, const double *beta, const double *gamma, double *nrm, double *ws,
-                               cudaStream_t st);
+// Krylov steps on unnormalised storage u_j = s_j q_j (s on device):
+//   out_a = <w, a> / s^2, out_b = <w, b> / s  (s null: no scaling)
+ctn_status dot2s_f64(const double *w, const double *a, const double *b, int64_t n, const double *s, double *out_a,
+                     double *out_b, double *ws2, cudaStream_t st);
+//   dst = (w - alpha u) / s - (s / sp) up - gamma q and ||dst|| -> nrm  (up, q may be null)
+ctn_status lanczos_step_f64(const double *w, const double *u, const double *up, const double *q, double *dst,
+                            int64_t n, const double *alpha, const double *gamma, const double *s, const double *sp,
+                            double *nrm, double *ws, cudaStream_t st);
 ctn_status div_copy_f64(const double *x, double *y, int64_t n, const double *a, cudaStream_t st);
 ctn_status combine_f64(const double *K, int64_t n, int m, const double *c, double *out, cudaStream_t st);
 }  // namespace ctn

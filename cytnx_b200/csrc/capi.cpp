@@ -277,14 +277,18 @@ ctn_status lanczos_refined(int (*mv_lo)(void *, const double *, double *, void *
   CTN_TRY(div_copy_f64(psi0, krylov, n, scal + 0, st));
   double theta = 0.0, rho = 0.0;
   int c = 0;
-  std::vector<double> As(krydim), Bs(krydim), evals, evecs;
+  std::vector<double> As(krydim), Bs(krydim), coef(krydim), evals, evecs;
+  // Krylov storage: slot 0 holds the unit vector q0; slot j >= 1 holds u_j = s_j q_j with
+  // s_j = beta[j-1] = |u_j| (never normalised in a separate pass: H u_j = s_j H q_j, and
+  // the scales enter the recurrence coefficients and the final combination)
   for (c = 0; c < max_restarts; ++c) {
     double *q0 = krylov;
-    // FP64 refinement: theta = <q0, H q0>, r = H q0 - theta q0, rho = |r|  (alpha[0], beta[0])
-    if (mv_hi(u_hi, q0, w, st) != 0) return CTN_ERR_CUDA;
+    double *u1 = krylov + n;
+    // FP64 refinement: theta = <q0, H q0>, u1 = r = H q0 - theta q0, rho = |r|  (alpha[0], beta[0])
+    if (mv_hi(u_hi, q0, u1, st) != 0) return CTN_ERR_CUDA;
     ++n_hi;
-    CTN_TRY(dot_f64(w, q0, n, alpha + 0, ws, st));
-    CTN_TRY(lanczos_update_f64(w, q0, nullptr, n, alpha + 0, nullptr, beta + 0, ws, st));
+    CTN_TRY(dot_f64(u1, q0, n, alpha + 0, ws, st));
+    CTN_TRY(lanczos_update_f64(u1, q0, nullptr, n, alpha + 0, nullptr, beta + 0, ws, st));
     double tr[2];
     CTN_CUDA(cudaMemcpyAsync(&tr[0], alpha + 0, sizeof(double), cudaMemcpyDeviceToHost, st));
     CTN_CUDA(cudaMemcpyAsync(&tr[1], beta + 0, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -293,19 +297,20 @@ ctn_status lanczos_refined(int (*mv_lo)(void *, const double *, double *, void *
     rho = tr[1];
     CTN_REQUIRE(std::isfinite(theta) && std::isfinite(rho), "[Lanczos refined] non-finite Rayleigh quotient");
     if (rho <= tol * std::fabs(theta) || rho == 0.0 || c == max_restarts - 1) break;
-    CTN_TRY(div_copy_f64(w, krylov + n, n, beta + 0, st));
-    // low-precision Krylov steps, all scalars kept on the device (no host round trip)
+    // low-precision Krylov steps, all scalars kept on the device (no host round trip):
+    //   w = H u_j;  alpha_j = <w, u_j> / s_j^2, gamma = <w, q0> / s_j;
+    //   u_{j+1} = (w - alpha_j u_j) / s_j - beta_{j-1} q_{j-1} - gamma q0, beta_j = |u_{j+1}|
+    // (for j = 1, q_{j-1} is q0 and its measured overlap gamma replaces beta_0).  The last
+    // step needs alpha only: beta_{m-1} is not an entry of the m x m tridiagonal.
     for (int j = 1; j < krydim; ++j) {
-      const double *qj = krylov + (int64_t)j * n;
-      const double *qp = krylov + (int64_t)(j - 1) * n;
-      if (mv_lo(u_lo, qj, w, st) != 0) return CTN_ERR_CUDA;
+      const double *uj = krylov + (int64_t)j * n;
+      const double *up = j >= 2 ? krylov + (int64_t)(j - 1) * n : nullptr;
+      if (mv_lo(u_lo, uj, w, st) != 0) return CTN_ERR_CUDA;
       ++n_lo;
-      CTN_TRY(dot2_f64(w, qj, q0, n, alpha + j, scal + 4, ws2, st));
-      if (j == 1)  // q_{j-1} is q0: its measured overlap replaces beta
-        CTN_TRY(lanczos_update3_f64(w, qj, q0, nullptr, n, alpha + j, scal + 4, nullptr, beta + j, ws, st));
-      else
-        CTN_TRY(lanczos_update3_f64(w, qj, qp, q0, n, alpha + j, beta + j - 1, scal + 4, beta + j, ws, st));
-      if (j + 1 < krydim) CTN_TRY(div_copy_f64(w, krylov + (int64_t)(j + 1) * n, n, beta + j, st));
+      CTN_TRY(dot2s_f64(w, uj, q0, n, beta + j - 1, alpha + j, scal + 4, ws2, st));
+      if (j + 1 < krydim)
+        CTN_TRY(lanczos_step_f64(w, uj, up, q0, krylov + (int64_t)(j + 1) * n, n, alpha + j, scal + 4, beta + j - 1,
+                                 j >= 2 ? beta + j - 2 : nullptr, beta + j, ws, st));
     }
     CTN_CUDA(cudaMemcpyAsync(As.data(), alpha, sizeof(double) * krydim, cudaMemcpyDeviceToHost, st));
     CTN_CUDA(cudaMemcpyAsync(Bs.data(), beta, sizeof(double) * krydim, cudaMemcpyDeviceToHost, st));
@@ -322,7 +327,10 @@ ctn_status lanczos_refined(int (*mv_lo)(void *, const double *, double *, void *
     evals.assign(m, 0.0);
     evecs.assign((size_t)m * m, 0.0);
     CTN_TRY(tql(m, As.data(), Bs.data(), evals.data(), evecs.data()));
-    CTN_CUDA(cudaMemcpyAsync(cdev, evecs.data(), sizeof(double) * m, cudaMemcpyHostToDevice, st));
+    // v = y_0 q0 + sum_{j>=1} y_j u_j / s_j  (s_j = beta_{j-1} > 0 for j < m)
+    coef[0] = evecs[0];
+    for (int j = 1; j < m; ++j) coef[j] = evecs[j] / Bs[j - 1];
+    CTN_CUDA(cudaMemcpyAsync(cdev, coef.data(), sizeof(double) * m, cudaMemcpyHostToDevice, st));
     CTN_TRY(combine_f64(krylov, n, m, cdev, w, st));
     CTN_TRY(nrm2_f64(w, n, scal + 0, ws, st));
     CTN_TRY(div_copy_f64(w, krylov, n, scal + 0, st));

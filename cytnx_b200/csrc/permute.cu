@@ -174,6 +174,101 @@ __global__ void __launch_bounds__(256) k_transpose_short(const T *__restrict__ s
   }
 }
 
+// Short output axis (nb < 16) under a long input axis (na >= 256): a CTA stages a tile of
+// TA = 256 x APT consecutive a by all nb b of one batch point in shared memory.  Reads:
+// nb coalesced input rows, all APT x nb loads of a thread issued together.  Writes: when
+// the output stride of a equals nb the tile is ONE contiguous output run of cnt_a x nb
+// elements, written in 16-byte vectors when the run starts on a 16-byte boundary;
+// otherwise the tile's runs of nb elements go out in warp-wide sweeps.  NB bounds nb at
+// compile time so the staging registers stay few (occupancy carries the bytes in flight).
+constexpr int STAGED_THREADS = 256;
+
+template <typename T, int NB, int APT>
+__global__ void __launch_bounds__(STAGED_THREADS) k_transpose_staged(const T *__restrict__ src, T *__restrict__ dst,
+                                                                     TransGeom g) {
+  extern __shared__ __align__(16) unsigned char staged_smem[];
+  T *tile = reinterpret_cast<T *>(staged_smem);
+  constexpr int TA = STAGED_THREADS * APT;
+  const int nb = (int)g.nb;
+  const int tid = threadIdx.x;
+  const int64_t tiles_a = (g.na + TA - 1) / TA;
+  const int64_t total = tiles_a * g.batch;
+  for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
+    int64_t bidx = t / tiles_a;
+    const int64_t a0 = (t - bidx * tiles_a) * TA;
+    int64_t in_off = 0, out_off = 0;
+    for (int i = g.nbatch_dims - 1; i >= 0; --i) {
+      const int64_t d = g.bshape[i];
+      const int64_t q = bidx / d;
+      const int64_t c = bidx - q * d;
+      in_off += c * g.bin[i];
+      out_off += c * g.bout[i];
+      bidx = q;
+    }
+    const int cnt_a = (int)(g.na - a0 < TA ? g.na - a0 : TA);
+    const T *s = src + in_off + a0;
+    T v[APT][NB];
+#pragma unroll
+    for (int p = 0; p < APT; ++p)
+#pragma unroll
+      for (int b = 0; b < NB; ++b)
+        if (b < nb && p * STAGED_THREADS + tid < cnt_a) v[p][b] = s[(int64_t)b * g.in_stride_b + p * STAGED_THREADS + tid];
+    __syncthreads();  // the previous tile's writers are done reading the stage
+#pragma unroll
+    for (int p = 0; p < APT; ++p)
+#pragma unroll
+      for (int b = 0; b < NB; ++b)
+        if (b < nb && p * STAGED_THREADS + tid < cnt_a) tile[(p * STAGED_THREADS + tid) * nb + b] = v[p][b];
+    __syncthreads();
+    const int cnt = cnt_a * nb;  // elements staged
+    if (g.out_stride_a == nb) {
+      T *o = dst + out_off + a0 * nb;
+      if (sizeof(T) < 16 && (reinterpret_cast<uintptr_t>(o) & 15) == 0) {
+        constexpr int V = 16 / sizeof(T);
+        const int nv = cnt / V;
+        const uint4 *s4 = reinterpret_cast<const uint4 *>(tile);
+        uint4 *o4 = reinterpret_cast<uint4 *>(o);
+        for (int i = tid; i < nv; i += STAGED_THREADS) o4[i] = s4[i];
+        for (int i = nv * V + tid; i < cnt; i += STAGED_THREADS) o[i] = tile[i];
+      } else {
+        for (int i = tid; i < cnt; i += STAGED_THREADS) o[i] = tile[i];
+      }
+    } else {
+      for (int i = tid; i < cnt; i += STAGED_THREADS) {
+        const int a = i / nb, b = i - a * nb;
+        dst[out_off + (a0 + a) * g.out_stride_a + b] = tile[i];
+      }
+    }
+  }
+}
+
+// Launches k_transpose_staged when the geometry suits it (na >= 256, nb < 16, the stage
+// within 48 KB); returns false otherwise.
+template <typename T, int NB>
+static bool launch_staged_nb(const void *src, void *dst, const TransGeom &g, int nsm, cudaStream_t st) {
+  int apt = NB <= 8 ? 2 : 1;
+  if ((size_t)STAGED_THREADS * apt * g.nb * sizeof(T) > 48 * 1024) apt = 1;
+  const size_t smem = (size_t)STAGED_THREADS * apt * g.nb * sizeof(T);
+  if (smem > 48 * 1024) return false;
+  const int64_t ta = (int64_t)STAGED_THREADS * apt;
+  const int64_t total = (g.na + ta - 1) / ta * g.batch;
+  const int64_t blocks = std::min<int64_t>(total, (int64_t)nsm * 64);
+  if (apt == 2)
+    k_transpose_staged<T, NB, 2><<<(unsigned)blocks, STAGED_THREADS, smem, st>>>((const T *)src, (T *)dst, g);
+  else
+    k_transpose_staged<T, NB, 1><<<(unsigned)blocks, STAGED_THREADS, smem, st>>>((const T *)src, (T *)dst, g);
+  return true;
+}
+
+template <typename T>
+static bool launch_staged(const void *src, void *dst, const TransGeom &g, int nsm, cudaStream_t st) {
+  if (g.na < STAGED_THREADS || g.nb >= 16 || g.nb < 2) return false;
+  if (g.nb <= 2) return launch_staged_nb<T, 2>(src, dst, g, nsm, st);
+  if (g.nb <= 4) return launch_staged_nb<T, 4>(src, dst, g, nsm, st);
+  if (g.nb <= 8) return launch_staged_nb<T, 8>(src, dst, g, nsm, st);
+  return launch_staged_nb<T, 16>(src, dst, g, nsm, st);
+}
+
 static int sm_count() {
   static int n = 0;
   if (n == 0) {
@@ -575,6 +670,10 @@ static ctn_status launch_perm(const void *src, void *dst, int rank, const uint64
     g.batch *= rshape[j];
   }
   if (g.nb < 16) {
+    if (launch_staged<T>(src, dst, g, nsm, st)) {
+      CTN_CHECK_LAUNCH();
+      return CTN_OK;
+    }
     const int64_t rows = g.na * g.batch;
     const int64_t blocks = std::min<int64_t>((rows + 255) / 256, (int64_t)nsm * 16);
     k_transpose_short<T><<<(unsigned)blocks, 256, 0, st>>>((const T *)src, (T *)dst, g);

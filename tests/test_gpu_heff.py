@@ -190,3 +190,57 @@ def test_refined_lanczos_reaches_fp64_energy(form):
     H.apply_flat(v, hv, "fp64")
     assert abs(float(torch.dot(v, hv)) - E) < 1e-12 * abs(E)
     assert abs(float(torch.linalg.vector_norm(hv - E * v)) - got["residual"]) < 1e-9 * abs(E)
+
+
+@pytest.mark.parametrize("n,krydim", [(60, 10), (5, 8)])
+def test_refined_lanczos_c_abi_dense_operator(n, krydim):
+    """ctn_lanczos_refined through the C ABI with caller matvecs: an FP64 operator for the
+    refinement and the same operator with a relative 1e-6 perturbation for the Krylov
+    steps.  (5, 8): the Krylov space runs out after five vectors (near-zero beta)."""
+    import ctypes
+
+    from cytnx_b200 import _lib
+
+    g = torch.Generator().manual_seed(n)
+    A = torch.randn(n, n, generator=g, dtype=torch.float64)
+    Hm = ((A + A.T) / 2).cuda()
+    noise = torch.randn(n, generator=g, dtype=torch.float64).cuda()
+    x0 = torch.randn(n, generator=g, dtype=torch.float64).cuda()
+    K = torch.empty(krydim * n, dtype=torch.float64, device="cuda")
+    work = torch.empty(n + 3200 + 3 * krydim, dtype=torch.float64, device="cuda")
+    eig = torch.empty(n, dtype=torch.float64, device="cuda")
+    bufs = (K, work, eig, x0)
+
+    def view(ptr):
+        for b in bufs:
+            base = b.data_ptr()
+            if base <= ptr < base + 8 * b.numel():
+                off = (ptr - base) // 8
+                return b[off:off + n]
+        raise AssertionError("pointer outside the test's buffers")
+
+    def mv_hi(user, x, y, stream):
+        view(y).copy_(Hm @ view(x))
+        return 0
+
+    def mv_lo(user, x, y, stream):
+        xv = view(x)
+        view(y).copy_(Hm @ xv + 1e-6 * torch.linalg.vector_norm(xv) * noise)
+        return 0
+
+    f_lo, f_hi = _lib.MATVEC_FN(mv_lo), _lib.MATVEC_FN(mv_hi)
+    E, res = ctypes.c_double(), ctypes.c_double()
+    rs = ctypes.c_int()
+    cnt = np.zeros(2, dtype=np.int64)
+    _lib.check(_lib.lib().ctn_lanczos_refined(f_lo, None, f_hi, None, x0.data_ptr(), n, krydim, 300, 1e-12,
+                                              K.data_ptr(), work.data_ptr(), eig.data_ptr(), ctypes.byref(E),
+                                              ctypes.byref(res), ctypes.byref(rs), cnt.ctypes.data_as(_lib.P_i64),
+                                              _lib.stream_ptr()), "ctn_lanczos_refined")
+    e0 = float(np.linalg.eigvalsh(Hm.cpu().numpy())[0])
+    assert abs(E.value - e0) <= 1e-11 * abs(e0)
+    assert res.value <= 1e-12 * abs(E.value)
+    v = eig.cpu().numpy()
+    assert abs(np.linalg.norm(v) - 1.0) < 1e-12
+    hv = Hm.cpu().numpy() @ v
+    assert np.linalg.norm(hv - E.value * v) <= 2e-12 * abs(E.value)
+    assert cnt[1] == rs.value + 1

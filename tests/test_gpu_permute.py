@@ -78,6 +78,54 @@ def test_large_transpose_and_unaligned_views():
     assert np.array_equal(t.permute(1, 0).contiguous().numpy(), ref.T)
 
 
+@pytest.mark.parametrize("dtype", [np.float64, np.float32, np.int16, np.bool_, np.complex128])
+def test_short_output_axis_staged(dtype):
+    """Output's fastest axis shorter than 16 under a long input axis: contiguous output runs
+    (output stride of the input's fastest axis == the short extent), strided runs, ragged
+    tiles, every short extent 2..15 (complex128 at 13..15 takes the unstaged kernel)."""
+    rng = np.random.default_rng(5)
+
+    def make(shape):
+        if dtype == np.bool_:
+            return rng.integers(0, 2, shape).astype(np.bool_)
+        if dtype == np.complex128:
+            return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(dtype)
+        if dtype == np.int16:
+            return rng.integers(-30000, 30000, shape).astype(dtype)
+        return rng.standard_normal(shape).astype(dtype)
+
+    cases = [((3, 5, 600), (0, 2, 1)), ((5, 3, 1030), (1, 2, 0)), ((4, 6, 530), (2, 1, 0)),
+             ((2, 1030), (1, 0)), ((7, 2, 2, 513), (1, 0, 3, 2)), ((256, 4), (1, 0))]
+    cases += [((nb, 300), (1, 0)) for nb in range(2, 16)]
+    for shape, p in cases:
+        a = make(shape)
+        out = _permute_dev(a, p)
+        assert np.array_equal(out, O.permute(a, p)), (shape, p)
+
+
+def test_short_output_axis_unaligned_destination():
+    """ctn_permute into a destination 4 bytes past a 16-byte boundary (the element-wise
+    store path of the staged kernel) and at a 16-byte boundary, same input."""
+    from cytnx_b200 import _lib
+
+    rng = np.random.default_rng(6)
+    shape, p = (3, 4, 777), (0, 2, 1)
+    a = rng.standard_normal(shape).astype(np.float32)
+    x = torch.from_numpy(a).cuda()
+    ref = O.permute(a, p).reshape(-1)
+    for off in (0, 1):
+        buf = torch.zeros(a.size + 8, dtype=torch.float32, device="cuda")
+        dst = buf[4 + off:4 + off + a.size]
+        osh = np.array(shape, dtype=np.uint64)
+        mp = np.array(p, dtype=np.uint64)
+        _lib.check(_lib.lib().ctn_permute(x.data_ptr(), dst.data_ptr(), 4, 3, osh.ctypes.data_as(_lib.P_u64),
+                                          mp.ctypes.data_as(_lib.P_u64), _lib.stream_ptr()), "permute")
+        torch.cuda.synchronize()
+        got = buf.cpu().numpy()
+        assert np.array_equal(got[4 + off:4 + off + a.size], ref)
+        assert not got[:4 + off].any() and not got[4 + off + a.size:].any()
+
+
 def test_lazy_permute_composition():
     import cytnx_b200 as c
 
