@@ -271,6 +271,64 @@ __global__ void __launch_bounds__(RT) k_combine(const double *__restrict__ K, in
   }
 }
 
+// ---- block Krylov kernels for the thick-restart Lanczos (k extreme eigenpairs).
+// The basis V holds m vectors of n doubles back to back (V[j] = V + j * n).
+
+// h[j] = <V[j], w> for j < m (accumulate: h[j] += ...).  Each CTA reduces its slice of
+// every dot and writes m partials; the last CTA sums them in a fixed order.
+__global__ void __launch_bounds__(RT) k_multidot(const double *__restrict__ V, const double *__restrict__ w,
+                                                int64_t n, int m, double *partials, unsigned *ticket, double *h,
+                                                int accumulate) {
+  const int64_t step = (int64_t)gridDim.x * RT;
+  for (int j = 0; j < m; ++j) {
+    const double *v = V + (int64_t)j * n;
+    double s = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * RT + threadIdx.x; i < n; i += step) s = fma(v[i], w[i], s);
+    s = block_sum(s);
+    if (threadIdx.x == 0) partials[(int64_t)blockIdx.x * m + j] = s;
+  }
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned t = atomicAdd(ticket, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  for (int j = threadIdx.x; j < m; j += RT) {
+    double v = 0.0;
+    for (int b = 0; b < (int)gridDim.x; ++b) v += ((volatile double *)partials)[(int64_t)b * m + j];
+    h[j] = accumulate ? h[j] + v : v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *ticket = 0u;
+}
+
+// w -= sum_j V[j] h[j]  (j < m)
+__global__ void __launch_bounds__(RT) k_multiaxpy(const double *__restrict__ V, const double *__restrict__ h,
+                                                 int64_t n, int m, double *__restrict__ w) {
+  const int64_t step = (int64_t)gridDim.x * RT;
+  for (int64_t i = (int64_t)blockIdx.x * RT + threadIdx.x; i < n; i += step) {
+    double s = w[i];
+    for (int j = 0; j < m; ++j) s = fma(-h[j], V[(int64_t)j * n + i], s);
+    w[i] = s;
+  }
+}
+
+// out[c] = sum_j V[j] Y[j * ldy + c]  (c < nc, j < m): Ritz vectors from the basis
+__global__ void __launch_bounds__(RT) k_basis_combine(const double *__restrict__ V, int64_t n, int m,
+                                                     const double *__restrict__ Y, int ldy, int nc,
+                                                     double *__restrict__ out) {
+  const int64_t step = (int64_t)gridDim.x * RT;
+  for (int64_t i = (int64_t)blockIdx.x * RT + threadIdx.x; i < n; i += step) {
+    for (int c = 0; c < nc; ++c) {
+      double s = 0.0;
+      for (int j = 0; j < m; ++j) s = fma(Y[j * ldy + c], V[(int64_t)j * n + i], s);
+      out[(int64_t)c * n + i] = s;
+    }
+  }
+}
+
 int grid_for(int64_t n) {
   static int nsm = 0;
   if (!nsm) {
@@ -353,6 +411,28 @@ ctn_status div_copy_f64(const double *x, double *y, int64_t n, const double *a, 
 }
 ctn_status combine_f64(const double *K, int64_t n, int m, const double *c, double *out, cudaStream_t st) {
   k_combine<<<grid_for(n), RT, 0, st>>>(K, n, m, c, out);
+  CTN_CHECK_LAUNCH();
+  return CTN_OK;
+}
+
+// ws layout: [ticket (8 bytes, fixed place for every m)][grid * m partials]; ws must hold
+// multidot_ws_doubles(m_max) doubles
+size_t multidot_ws_doubles(int m) { return (size_t)MAXCTA * (size_t)m + 8; }
+ctn_status multidot_f64(const double *V, const double *w, int64_t n, int m, double *h, int accumulate, double *ws,
+                        cudaStream_t st) {
+  const int g = grid_for(n);
+  k_multidot<<<g, RT, 0, st>>>(V, w, n, m, ws + 8, reinterpret_cast<unsigned *>(ws), h, accumulate);
+  CTN_CHECK_LAUNCH();
+  return CTN_OK;
+}
+ctn_status multiaxpy_f64(const double *V, const double *h, int64_t n, int m, double *w, cudaStream_t st) {
+  k_multiaxpy<<<grid_for(n), RT, 0, st>>>(V, h, n, m, w);
+  CTN_CHECK_LAUNCH();
+  return CTN_OK;
+}
+ctn_status basis_combine_f64(const double *V, int64_t n, int m, const double *Y, int ldy, int nc, double *out,
+                             cudaStream_t st) {
+  k_basis_combine<<<grid_for(n), RT, 0, st>>>(V, n, m, Y, ldy, nc, out);
   CTN_CHECK_LAUNCH();
   return CTN_OK;
 }

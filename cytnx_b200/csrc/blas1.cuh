@@ -23,4 +23,14 @@ ctn_status lanczos_step_f64(const double *w, const double *u, const double *up, 
                             double *nrm, double *ws, cudaStream_t st);
 ctn_status div_copy_f64(const double *x, double *y, int64_t n, const double *a, cudaStream_t st);
 ctn_status combine_f64(const double *K, int64_t n, int m, const double *c, double *out, cudaStream_t st);
+// block Krylov helpers (basis V: m vectors of n doubles back to back)
+size_t multidot_ws_doubles(int m);  // zeroed before first use (its first word is the ticket)
+//   h[j] (+)= <V[j], w>, j < m
+ctn_status multidot_f64(const double *V, const double *w, int64_t n, int m, double *h, int accumulate, double *ws,
+                        cudaStream_t st);
+//   w -= sum_j h[j] V[j]
+ctn_status multiaxpy_f64(const double *V, const double *h, int64_t n, int m, double *w, cudaStream_t st);
+//   out[c] = sum_j Y[j * ldy + c] V[j], c < nc
+ctn_status basis_combine_f64(const double *V, int64_t n, int m, const double *Y, int ldy, int nc, double *out,
+                             cudaStream_t st);
 }  // namespace ctn

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <mutex>
 #include <numeric>
 #include <vector>
@@ -363,4 +364,219 @@ extern "C" ctn_status ctn_lanczos_gnd(ctn_matvec_fn matvec, void *user, const do
                                       int *iters, void *stream) {
   return ctn::lanczos_gnd(matvec, user, psi0, n, maxiter, cvgcrit, krylov, work, eigvec, energy, iters,
                           ctn::as_stream(stream));
+}
+
+namespace ctn {
+// Dense symmetric eigenproblem by the cyclic Jacobi method (Golub & Van Loan, Matrix
+// Computations, sec. 8.5: two-sided rotations that zero one off-diagonal pair at a time,
+// swept until the off-diagonal mass is negligible).  a: n x n row-major (copied);
+// w: eigenvalues (diagonal order); z: n x n row-major, eigenvectors as COLUMNS.
+static ctn_status jacobi_eigh(int n, const double *ain, double *w, double *z) {
+  std::vector<double> a(ain, ain + (size_t)n * n);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) z[(size_t)i * n + j] = i == j ? 1.0 : 0.0;
+  double fro = 0.0;
+  for (double x : a) fro += x * x;
+  fro = std::sqrt(fro);
+  bool done = n <= 1 || fro == 0.0;
+  for (int sweep = 0; sweep < 100 && !done; ++sweep) {
+    double off = 0.0;
+    for (int i = 0; i < n; ++i)
+      for (int j = i + 1; j < n; ++j) off += a[(size_t)i * n + j] * a[(size_t)i * n + j];
+    if (std::sqrt(off) <= 1e-18 * fro) {
+      done = true;
+      break;
+    }
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = a[(size_t)p * n + q];
+        if (apq == 0.0) continue;
+        const double tau = (a[(size_t)q * n + q] - a[(size_t)p * n + p]) / (2.0 * apq);
+        const double t = (tau >= 0 ? 1.0 : -1.0) / (std::fabs(tau) + std::sqrt(1.0 + tau * tau));
+        const double c = 1.0 / std::sqrt(1.0 + t * t), s = t * c;
+        for (int k = 0; k < n; ++k) {  // A <- A J (columns p, q)
+          const double akp = a[(size_t)k * n + p], akq = a[(size_t)k * n + q];
+          a[(size_t)k * n + p] = c * akp - s * akq;
+          a[(size_t)k * n + q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < n; ++k) {  // A <- J^T A (rows p, q)
+          const double apk = a[(size_t)p * n + k], aqk = a[(size_t)q * n + k];
+          a[(size_t)p * n + k] = c * apk - s * aqk;
+          a[(size_t)q * n + k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < n; ++k) {  // Z <- Z J
+          const double zkp = z[(size_t)k * n + p], zkq = z[(size_t)k * n + q];
+          z[(size_t)k * n + p] = c * zkp - s * zkq;
+          z[(size_t)k * n + q] = s * zkp + c * zkq;
+        }
+      }
+    if (sweep == 99) {
+      set_error("ctn_sym_eigh: Jacobi sweeps did not converge");
+      return CTN_ERR_NUMERIC;
+    }
+  }
+  for (int i = 0; i < n; ++i) w[i] = a[(size_t)i * n + i];
+  return CTN_OK;
+}
+
+// work layout: [w n][H (ncv + 1) x ncv][Y ncv x ncv][scalars 8][h ncv + 9][multidot ws]
+// [reduction ws][restart combination n x ncv]
+size_t lanczos_which_work_doubles(int64_t n, int ncv) {
+  const size_t ld = (size_t)ncv + 1;
+  return (size_t)n + ld * ncv + (size_t)ncv * ncv + 8 + ld + 8 + multidot_ws_doubles((int)ld) +
+         reduce_ws_bytes() / sizeof(double) + (size_t)n * (size_t)ncv;
+}
+
+// Thick-restart Lanczos for the k extreme eigenpairs of a symmetric operator (Wu & Simon,
+// SIAM J. Matrix Anal. Appl. 22 (2000) 602; the symmetric Krylov-Schur restart of Stewart,
+// SIAM J. Matrix Anal. Appl. 23 (2001) 601).  It computes what the reference obtains from
+// ARPACK's implicitly restarted Lanczos (src/linalg/Lanczos.cpp:250-402: dsaupd/dseupd,
+// which = SA / LA / LM, ncv = min(n, 2k + 10) by default, convergence of a Ritz pair when
+// its estimate |beta_m y_m| <= tol * max(eps^(2/3), |theta|), tol <= 0 meaning machine
+// precision).  Each cycle extends the basis to ncv vectors with full (twice-applied
+// classical Gram-Schmidt) re-orthogonalisation on the device, solves the projected
+// matrix on the host, and keeps k + (m - k) / 2 wanted Ritz vectors plus the residual
+// direction for the next cycle.
+ctn_status lanczos_which(int (*mv)(void *, const double *, double *, void *), void *user, const double *v0,
+                         int64_t n, int which, int k, int ncv, int maxiter, double tol, double *V, double *work,
+                         double *evals, double *evecs, int *iters, int *nconv_out, cudaStream_t st) {
+  CTN_REQUIRE(which >= 0 && which <= 2, "[ERROR][Lanczos] 'which' should be 'LM', 'LA', 'SA'");
+  CTN_REQUIRE(n > 0 && k >= 1 && k <= n, "[ERROR][Lanczos] k should be in 1..n");
+  CTN_REQUIRE(maxiter >= 1, "[ERROR][Lanczos] Maxiter must be >= 1");
+  CTN_REQUIRE(tol >= 0, "[ERROR][Lanczos] cvg_crit should be >= 0");
+  if (ncv == 0) ncv = (int)std::min<int64_t>(n, 2 * (int64_t)k + 10);
+  CTN_REQUIRE(ncv <= n && (ncv > k || ncv == n), "[ERROR][Lanczos] ncv should be 2+k<=ncv<=nx");
+  const int ld = ncv + 1;  // device H: column j at H + j * ld (rows 0..j+1)
+  double *w = work;
+  double *Hd = w + n;
+  double *Yd = Hd + (size_t)ld * ncv;
+  double *scal = Yd + (size_t)ncv * ncv;  // [0] norm [1] one [2..] spare
+  double *tmp_h = scal + 8;                // ld doubles
+  double *mws = tmp_h + ld + 8;            // multidot workspace
+  double *rws = mws + multidot_ws_doubles(ld);
+  double *Vtmp = rws + reduce_ws_bytes() / sizeof(double);  // n x ncv: restart combination
+  CTN_CUDA(cudaMemsetAsync(mws, 0, multidot_ws_doubles(ld) * sizeof(double), st));
+  CTN_CUDA(cudaMemsetAsync(rws, 0, reduce_ws_bytes(), st));
+  CTN_CUDA(cudaMemsetAsync(Hd, 0, sizeof(double) * (size_t)ld * ncv, st));
+  const double one = 1.0;
+  CTN_CUDA(cudaMemcpyAsync(scal + 1, &one, sizeof(double), cudaMemcpyHostToDevice, st));
+  CTN_TRY(nrm2_f64(v0, n, scal + 0, rws, st));
+  double nrm0 = 0.0;
+  CTN_CUDA(cudaMemcpyAsync(&nrm0, scal + 0, sizeof(double), cudaMemcpyDeviceToHost, st));
+  CTN_CUDA(cudaStreamSynchronize(st));
+  CTN_REQUIRE(nrm0 > 0 && std::isfinite(nrm0), "[ERROR][Lanczos] initial vector has zero or non-finite norm");
+  CTN_TRY(div_copy_f64(v0, V, n, scal + 0, st));
+
+  const double eps = std::numeric_limits<double>::epsilon() * 0.5;  // unit roundoff (dlamch 'E')
+  const double eps23 = std::pow(eps, 2.0 / 3.0);
+  const double tol_eff = tol > 0 ? tol : eps;
+  std::vector<double> Hh((size_t)ld * ncv), T, th, Y, theta_kept;
+  std::vector<int> order;
+  int p = 0, it = 0, nconv = 0, m = 0;
+  bool finished = false;
+  std::vector<double> Ysel;
+  for (it = 0; it < maxiter && !finished; ++it) {
+    for (int j = p; j < ncv; ++j) {
+      if (mv(user, V + (int64_t)j * n, w, st) != 0) return CTN_ERR_CUDA;
+      double *hj = Hd + (size_t)j * ld;
+      CTN_TRY(multidot_f64(V, w, n, j + 1, hj, 0, mws, st));
+      CTN_TRY(multiaxpy_f64(V, hj, n, j + 1, w, st));
+      CTN_TRY(multidot_f64(V, w, n, j + 1, tmp_h, 0, mws, st));  // second Gram-Schmidt pass
+      CTN_TRY(multiaxpy_f64(V, tmp_h, n, j + 1, w, st));
+      CTN_TRY(axpy_f64(tmp_h, hj, j + 1, scal + 1, 1.0, st));
+      CTN_TRY(nrm2_f64(w, n, hj + j + 1, rws, st));
+      CTN_TRY(div_copy_f64(w, V + (int64_t)(j + 1) * n, n, hj + j + 1, st));
+    }
+    CTN_CUDA(cudaMemcpyAsync(Hh.data(), Hd, sizeof(double) * Hh.size(), cudaMemcpyDeviceToHost, st));
+    CTN_CUDA(cudaStreamSynchronize(st));
+    double anorm = 0.0;
+    for (int i = 0; i < p; ++i) anorm = std::max(anorm, std::fabs(theta_kept[i]));
+    for (int j = p; j < ncv; ++j)
+      for (int i = 0; i <= j + 1; ++i) {
+        CTN_REQUIRE(std::isfinite(Hh[(size_t)j * ld + i]), "[ERROR][Lanczos] non-finite projection");
+        anorm = std::max(anorm, std::fabs(Hh[(size_t)j * ld + i]));
+      }
+    m = ncv;
+    bool breakdown = false;
+    for (int j = p; j < ncv; ++j)
+      if (Hh[(size_t)j * ld + j + 1] <= 64.0 * eps * anorm) {  // invariant subspace reached
+        m = j + 1;
+        breakdown = true;
+        break;
+      }
+    // projected matrix: the kept Ritz values on the diagonal of the first p rows, the
+    // Gram-Schmidt coefficients of the extension columns (couplings included) above it
+    T.assign((size_t)m * m, 0.0);
+    for (int i = 0; i < p; ++i) T[(size_t)i * m + i] = theta_kept[i];
+    for (int j = p; j < m; ++j)
+      for (int i = 0; i <= j; ++i) T[(size_t)i * m + j] = T[(size_t)j * m + i] = Hh[(size_t)j * ld + i];
+    th.assign(m, 0.0);
+    Y.assign((size_t)m * m, 0.0);
+    CTN_TRY(jacobi_eigh(m, T.data(), th.data(), Y.data()));
+    order.resize(m);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+      if (which == 0) return th[a] < th[b];               // SA
+      if (which == 1) return th[a] > th[b];               // LA
+      return std::fabs(th[a]) > std::fabs(th[b]);         // LM
+    });
+    const double beta_last = breakdown ? 0.0 : Hh[(size_t)(m - 1) * ld + m];
+    const int kk_want = std::min(k, m);
+    nconv = 0;
+    for (int c = 0; c < kk_want; ++c) {
+      const double est = std::fabs(beta_last * Y[(size_t)(m - 1) * m + order[c]]);
+      if (est <= tol_eff * std::max(eps23, std::fabs(th[order[c]]))) ++nconv;
+    }
+    if (nconv >= k || breakdown || it == maxiter - 1) {
+      finished = true;
+      break;
+    }
+    // thick restart: keep kk wanted Ritz vectors, then the residual direction v_m
+    const int kk = std::max(k, std::min(m - 1, k + (m - k) / 2));
+    Ysel.assign((size_t)m * kk, 0.0);
+    for (int j = 0; j < m; ++j)
+      for (int c = 0; c < kk; ++c) Ysel[(size_t)j * kk + c] = Y[(size_t)j * m + order[c]];
+    CTN_CUDA(cudaMemcpyAsync(Yd, Ysel.data(), sizeof(double) * Ysel.size(), cudaMemcpyHostToDevice, st));
+    double *comb = Vtmp;
+    CTN_TRY(basis_combine_f64(V, n, m, Yd, kk, kk, comb, st));
+    CTN_CUDA(cudaMemcpyAsync(V, comb, sizeof(double) * (size_t)n * kk, cudaMemcpyDeviceToDevice, st));
+    CTN_CUDA(cudaMemcpyAsync(V + (int64_t)kk * n, V + (int64_t)m * n, sizeof(double) * (size_t)n,
+                             cudaMemcpyDeviceToDevice, st));
+    theta_kept.assign(kk, 0.0);
+    for (int c = 0; c < kk; ++c) theta_kept[c] = th[order[c]];
+    CTN_CUDA(cudaStreamSynchronize(st));  // Ysel is reused by the next cycle
+    p = kk;
+  }
+  // eigenpairs in the reference's order (sort_indices of Lanczos.cpp: by value or |value|)
+  for (int c = 0; c < k; ++c) evals[c] = c < m ? th[order[c]] : 0.0;
+  if (evecs) {
+    const int kc = std::min(k, m);
+    Ysel.assign((size_t)m * kc, 0.0);
+    for (int j = 0; j < m; ++j)
+      for (int c = 0; c < kc; ++c) Ysel[(size_t)j * kc + c] = Y[(size_t)j * m + order[c]];
+    CTN_CUDA(cudaMemcpyAsync(Yd, Ysel.data(), sizeof(double) * Ysel.size(), cudaMemcpyHostToDevice, st));
+    CTN_TRY(basis_combine_f64(V, n, m, Yd, kc, kc, evecs, st));
+  }
+  CTN_CUDA(cudaStreamSynchronize(st));
+  if (iters) *iters = it + (finished ? 1 : 0);
+  if (nconv_out) *nconv_out = nconv;
+  return CTN_OK;
+}
+}  // namespace ctn
+
+extern "C" size_t ctn_lanczos_which_work_doubles(int64_t n, int ncv) {
+  return ctn::lanczos_which_work_doubles(n, ncv);
+}
+
+extern "C" ctn_status ctn_lanczos_which(ctn_matvec_fn matvec, void *user, const double *v0, int64_t n, int which,
+                                        int k, int ncv, int maxiter, double tol, double *basis, double *work,
+                                        double *evals, double *evecs, int *iters, int *nconv, void *stream) {
+  CTN_REQUIRE(matvec && v0 && basis && work && evals, "ctn_lanczos_which: null argument");
+  return ctn::lanczos_which(matvec, user, v0, n, which, k, ncv, maxiter, tol, basis, work, evals, evecs, iters, nconv,
+                            ctn::as_stream(stream));
+}
+
+extern "C" ctn_status ctn_sym_eigh(int n, const double *a, double *w, double *z) {
+  CTN_REQUIRE(n >= 0 && a && w && z, "ctn_sym_eigh: bad argument");
+  return ctn::jacobi_eigh(n, a, w, z);
 }

@@ -11,7 +11,7 @@
 from __future__ import annotations
 
 import ctypes
-from typing import List, Sequence
+from typing import Optional, List, Sequence
 
 import numpy as np
 import torch
@@ -112,12 +112,29 @@ class _Callback:
             return 1
 
 
-def Lanczos(Hop, Tin, method: str = "Gnd", CvgCrit: float = 1.0e-14, Maxiter: int = 10000, k: int = 1,
-            is_V: bool = True, is_row: bool = False, max_krydim: int = 0, verbose: bool = False, which=None):
-    """Ground state of a Hermitian LinOp (the 'Gnd' method of linalg::Lanczos)."""
-    if which is not None or method not in ("Gnd",):
-        raise CytnxError(f"[ERROR][Lanczos] method '{method if which is None else which}' is not on this build's "
-                         "path; use method='Gnd'")
+_WHICH = {"SA": 0, "LA": 1, "LM": 2}
+
+
+def Lanczos(Hop, Tin, method: Optional[str] = None, CvgCrit: Optional[float] = None, Maxiter: int = 10000,
+            k: int = 1, is_V: bool = True, is_row: bool = False, max_krydim: int = 0, verbose: bool = False,
+            which: Optional[str] = None, ncv: int = 0):
+    """linalg::Lanczos in its two forms (src/linalg/Lanczos.cpp):
+    * method form, ``Lanczos(Hop, Tin, method="Gnd", CvgCrit=1e-14, Maxiter=10000, ...)``: the
+      ground state by the Lanczos_Gnd_Ut recurrence (:135-196);
+    * which form, ``Lanczos(Hop, Tin, which="SA" | "LA" | "LM", Maxiter=10000, CvgCrit=0, k=1,
+      is_V=True, ncv=0)``: the k extreme eigenpairs (:250-580; ARPACK there, a thick-restart
+      Lanczos with full re-orthogonalisation on the device here)."""
+    if which is not None:
+        if method is not None:
+            raise CytnxError("[ERROR][Lanczos] give either method or which, not both")
+        return _lanczos_which(Hop, Tin, which, Maxiter, 0.0 if CvgCrit is None else CvgCrit, k, is_V, ncv, verbose)
+    method = "Gnd" if method is None else method
+    CvgCrit = 1.0e-14 if CvgCrit is None else CvgCrit
+    if method == "ER":
+        raise CytnxError("[ERROR][Lanczos] method 'ER' is not on this build's path; use method='Gnd' or the "
+                         "which form (which='SA' gives the k lowest eigenpairs)")
+    if method != "Gnd":
+        raise CytnxError("[ERROR][Lanczos] Invalid Lanczos method, should be either 'ER' or 'Gnd'.")
     if k != 1:
         raise CytnxError("[ERROR][Lanczos] method 'Gnd' returns only the ground state (k = 1)")
     if CvgCrit <= 0:
@@ -158,4 +175,70 @@ def Lanczos(Hop, Tin, method: str = "Gnd", CvgCrit: float = 1.0e-14, Maxiter: in
         out.append(v0.with_flat(eig) if is_uni else Tensor.from_torch(eig.view(*v0.shape())))
     if verbose:
         print(f"[Lanczos] Gnd finished after {iters.value} iterations, E = {energy.value:.14f}")
+    return out
+
+
+def _lanczos_which(Hop, Tin, which, Maxiter, CvgCrit, k, is_V, ncv, verbose):
+    """The which form (ctn_lanczos_which); argument checks and error texts of
+    src/linalg/Lanczos.cpp:459-580."""
+    if which not in _WHICH:
+        raise CytnxError("[ERROR][Lanczos] 'which' should be 'LM', 'LA', 'SA'")
+    if Hop.dtype() != Type.Double:
+        raise CytnxError("[ERROR][Lanczos] the which form runs FP64 (Type.Double) operators on this build")
+    nx = int(Hop.nx())
+    if k < 1:
+        raise CytnxError("[ERROR][Lanczos] k should be >0")
+    if k > nx:
+        raise CytnxError("[ERROR][Lanczos] k can only be up to total dimension of input vector D")
+    if CvgCrit < 0:
+        raise CytnxError("[ERROR][Lanczos] cvg_crit should be >= 0")
+    if ncv != 0 and (ncv < 2 + k or ncv > nx):
+        raise CytnxError("[ERROR][Lanczos] ncv should be 2+k<=ncv<=nx")
+    if Maxiter < 1:
+        raise CytnxError("[ERROR][Lanczos] Maxiter must be >= 1")
+    is_uni = isinstance(Tin, UniTensor)
+    if is_uni:
+        if Tin.dtype() != Type.Double:
+            raise CytnxError("[ERROR][Lanczos] Tin should have datatype consistent with Hop")
+        v0 = Tin.contiguous()
+        x0 = v0.flat_view()
+    else:
+        if Tin.dtype() != Type.Double:
+            raise CytnxError("[ERROR][Lanczos] Tin should have datatype consistent with Hop")
+        if len(Tin.shape()) != 1:
+            raise CytnxError("[ERROR][Lanczos] Tin should be rank-1")
+        v0 = Tin.contiguous()
+        x0 = v0.to_torch().reshape(-1)
+    n = x0.numel()
+    if n != nx:
+        raise CytnxError(f"[ERROR][Lanczos] Tin should have dimension consistent with Hop: [{nx}]")
+    require_cuda(x0, "Lanczos")
+    ncv_r = ncv if ncv else min(n, 2 * k + 10)
+    if ncv_r <= k and ncv_r != n:
+        raise CytnxError("[ERROR][Lanczos] ncv should be 2+k<=ncv<=nx")
+    lib = _lib.lib()
+    basis = torch.empty((ncv_r + 1) * n, dtype=torch.float64, device=x0.device)
+    work = torch.empty(int(lib.ctn_lanczos_which_work_doubles(n, ncv_r)), dtype=torch.float64, device=x0.device)
+    evecs = torch.empty(k * n, dtype=torch.float64, device=x0.device) if is_V else None
+    evals = np.zeros(k, dtype=np.float64)
+    cb = _Callback(Hop, v0, basis, work, n, is_uni)
+    iters, nconv = ctypes.c_int(0), ctypes.c_int(0)
+    st = lib.ctn_lanczos_which(cb.fn, None, x0.data_ptr(), n, _WHICH[which], int(k), int(ncv_r), int(Maxiter),
+                               float(CvgCrit), basis.data_ptr(), work.data_ptr(), evals.ctypes.data_as(_lib.P_dbl),
+                               evecs.data_ptr() if is_V else None, ctypes.byref(iters), ctypes.byref(nconv),
+                               _lib.stream_ptr())
+    if cb.err is not None:
+        raise cb.err
+    _lib.check(st, "Lanczos")
+    if verbose and nconv.value < k:
+        print(f"[WARNING][Lanczos]: Maximum number of iterations reached ({nconv.value} of {k} converged).")
+    E = Tensor.from_numpy(evals.copy(), Device.cpu)
+    if is_uni:
+        out = [UniTensor(E, False, 0)]
+        if is_V:
+            out += [v0.with_flat(evecs[c * n:(c + 1) * n].clone()) for c in range(k)]
+        return out
+    out = [E]
+    if is_V:
+        out.append(Tensor.from_torch(evecs.view(n) if k == 1 else evecs.view(k, n)))
     return out

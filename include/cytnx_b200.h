@@ -38,6 +38,9 @@
  *   ctn_lanczos_gnd
  *       linalg::Lanczos(..., method="Gnd") -> Lanczos_Gnd_Ut
  *       (src/linalg/Lanczos_Gnd_Ut.cpp:29-199).
+ *   ctn_lanczos_which / ctn_sym_eigh
+ *       linalg::Lanczos(Hop, Tin, which = "SA" / "LA" / "LM", maxiter, cvg_crit, k, is_V, ncv)
+ *       (src/linalg/Lanczos.cpp:250-402: ARPACK dsaupd/dseupd).
  */
 #ifndef CYTNX_B200_H
 #define CYTNX_B200_H
@@ -202,6 +205,10 @@ ctn_status ctn_scal_f64(double *x, int64_t n, const double *a_dev, int invert, v
 /* symmetric tridiagonal eigensolver (host, FP64): d[n] diagonal, e[n-1] off-diagonal.
  * Eigenvalues ascending into w[n]; if z != NULL the eigenvectors as rows of z[n][n]. */
 ctn_status ctn_tridiag_eigh(int n, const double *d, const double *e, double *w, double *z);
+/* dense symmetric eigenproblem (host, cyclic Jacobi): a n x n row-major, w eigenvalues in
+ * no particular order, z n x n row-major with the eigenvectors as columns.  The projected
+ * matrix solve of ctn_lanczos_which (the reference calls LAPACK inside ARPACK dseupd). */
+ctn_status ctn_sym_eigh(int n, const double *a, double *w, double *z);
 
 /* ---------------------------------------------------------------- two-site H_eff
  * Plan for out = H_eff psi with the network of example/DMRG/dmrg_two_sites_U1.py:
@@ -304,6 +311,21 @@ ctn_status ctn_lanczos_refined(ctn_matvec_fn matvec_lo, void *user_lo, ctn_matve
                                void *user_hi, const double *psi0, int64_t n, int krydim, int max_restarts,
                                double tol, double *krylov, double *work, double *eigvec, double *energy,
                                double *residual, int *restarts, int64_t *matvecs, void *stream);
+/* k extreme eigenpairs of a symmetric operator (the "which" form of linalg::Lanczos,
+ * src/linalg/Lanczos.cpp:250-402, which drives ARPACK dsaupd/dseupd there): thick-restart
+ * Lanczos with full re-orthogonalisation on the device.  which: 0 = "SA" (smallest
+ * algebraic), 1 = "LA" (largest algebraic), 2 = "LM" (largest magnitude).  ncv: basis size
+ * (0: min(n, 2k + 10), the reference's default; otherwise k < ncv <= n).  A Ritz pair
+ * counts as converged when |beta_m y_m| <= tol * max(eps^(2/3), |theta|) (tol = 0: machine
+ * precision), as in ARPACK.  maxiter bounds the restart cycles.  basis: (ncv + 1) * n
+ * doubles (device); work: ctn_lanczos_which_work_doubles(n, ncv) doubles (device, with the
+ * resolved ncv).  evals (host, k) and evecs (device, k * n, or null) in the reference's
+ * order (ascending for SA, descending value / magnitude for LA / LM).  *iters: restart
+ * cycles run; *nconv: wanted pairs converged (k unless maxiter ran out). */
+size_t ctn_lanczos_which_work_doubles(int64_t n, int ncv);
+ctn_status ctn_lanczos_which(ctn_matvec_fn matvec, void *user, const double *v0, int64_t n, int which, int k,
+                             int ncv, int maxiter, double tol, double *basis, double *work, double *evals,
+                             double *evecs, int *iters, int *nconv, void *stream);
 /* the same on a planned H_eff: `precision` for the Krylov steps, FP64 for the refinement
  * (both must be bound with ctn_heff2_set_env) */
 ctn_status ctn_heff2_lanczos_refined(ctn_heff2_plan *plan, int precision, const double *psi0, int krydim,

@@ -156,3 +156,38 @@ def test_fileio_reads_reference_files():
     e = fileio.read_unitensor(os.path.join(base, "contract_ans3.cytnx"))
     z = load_golden("block_contract_ans3")
     assert np.array_equal(e["itoi"], z["itoi"])
+
+
+def test_lanczos_which_argument_errors():
+    """The which form's checks and messages (src/linalg/Lanczos.cpp:459-580) run before
+    any device work."""
+    import cytnx_b200 as c
+    from cytnx_b200._lib import CytnxError
+
+    H = c.LinOp("mv", 10, c.Type.Double, c.Device.cuda)
+    for kw, msg in ((dict(which="ML"), "'which' should be"), (dict(which="SM"), "'which' should be"),
+                    (dict(which="SA", k=0), "k should be >0"), (dict(which="SA", k=11), "k can only be up"),
+                    (dict(which="SA", CvgCrit=-1.0), "cvg_crit"), (dict(which="SA", k=3, ncv=4), "ncv should"),
+                    (dict(which="SA", ncv=11), "ncv should"), (dict(which="SA", method="Gnd"), "either method")):
+        with pytest.raises(CytnxError, match=msg):
+            c.linalg.Lanczos(H, None, **kw)
+    with pytest.raises(CytnxError, match="Invalid Lanczos method"):
+        c.linalg.Lanczos(H, None, "XY")
+
+
+def test_sym_eigh_matches_numpy():
+    import ctypes
+
+    from cytnx_b200 import _lib
+
+    rng = np.random.default_rng(1)
+    for n in (1, 2, 7, 40):
+        A = rng.standard_normal((n, n))
+        A = A + A.T
+        w = np.zeros(n)
+        z = np.zeros((n, n))
+        _lib.check(_lib.lib().ctn_sym_eigh(n, A.ctypes.data_as(_lib.P_dbl), w.ctypes.data_as(_lib.P_dbl),
+                                           z.ctypes.data_as(_lib.P_dbl)))
+        assert np.abs(np.sort(w) - np.linalg.eigvalsh(A)).max() < 1e-12 * max(1.0, np.abs(w).max())
+        assert np.abs(A @ z - z * w).max() < 1e-12 * max(1.0, np.abs(w).max())
+        assert np.abs(z.T @ z - np.eye(n)).max() < 1e-13
