@@ -105,6 +105,9 @@ _SIGS = {
                                 ctypes.POINTER(c_int), c_vp]),
     "ctn_lanczos_refined": (c_int, [MATVEC_FN, c_vp, MATVEC_FN, c_vp, c_vp, c_i64, c_int, c_int, c_dbl, c_vp, c_vp,
                                     c_vp, P_dbl, P_dbl, ctypes.POINTER(c_int), P_i64, c_vp]),
+    "ctn_lanczos_exp_work_doubles": (c_size, [c_i64, c_int]),
+    "ctn_lanczos_exp": (c_int, [MATVEC_FN, c_vp, c_vp, c_i64, c_dbl, c_dbl, c_dbl, c_int, c_vp, c_vp, c_vp, c_vp,
+                                ctypes.POINTER(c_int), c_vp]),
     "ctn_lanczos_which_work_doubles": (c_size, [c_i64, c_int]),
     "ctn_lanczos_which": (c_int, [MATVEC_FN, c_vp, c_vp, c_i64, c_int, c_int, c_int, c_int, c_dbl, c_vp, c_vp, P_dbl,
                                   c_vp, ctypes.POINTER(c_int), ctypes.POINTER(c_int), c_vp]),

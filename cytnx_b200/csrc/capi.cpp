@@ -580,3 +580,125 @@ extern "C" ctn_status ctn_sym_eigh(int n, const double *a, double *w, double *z)
   CTN_REQUIRE(n >= 0 && a && w && z, "ctn_sym_eigh: bad argument");
   return ctn::jacobi_eigh(n, a, w, z);
 }
+
+namespace ctn {
+// exp(tau H) v by the Lanczos projection of Lanczos_Exp (src/linalg/Lanczos_Exp.cpp:264-369):
+// plain three-term recurrence from v / |v|, breakdown when beta <= 100 eps scale sqrt(i)
+// (scale = running max of |alpha| + |beta| + |beta_prev| and 1), stop when the bottom-left
+// element of exp(tau T_i) falls below cvgcrit, result V exp(tau T) V^T v with the
+// un-normalised input.  T is symmetric tridiagonal, so exp(tau T) is formed from its
+// eigenpairs (the reference calls a general ExpM; the matrices agree to rounding).  Real
+// and imaginary parts of tau; out_im may be null when tau is real.
+ctn_status lanczos_exp(int (*mv)(void *, const double *, double *, void *), void *user, const double *vin,
+                       int64_t n, double tau_re, double tau_im, double cvgcrit, int maxiter, double *V, double *work,
+                       double *out_re, double *out_im, int *iters, cudaStream_t st) {
+  CTN_REQUIRE(cvgcrit > 0, "[ERROR][Lanczos_Exp] converge criteria must >0");
+  CTN_REQUIRE(maxiter >= 2, "[ERROR][Lanczos_Exp] Maxiter must >1");
+  CTN_REQUIRE(n > 0, "[ERROR][Lanczos_Exp] empty vector");
+  CTN_REQUIRE(tau_im == 0.0 || out_im, "[ERROR][Lanczos_Exp] complex tau needs the imaginary output");
+  const int mmax = (int)std::min<int64_t>(maxiter, n);
+  double *w = work;                  // matvec output / recurrence vector
+  double *scal = work + n;           // [0] |v| [1] alpha [2] beta (coefficient of v_old) [3] |w|
+  double *cdev = scal + 8;           // V^T v (mmax) then the output coefficients
+  double *mws = cdev + 2 * mmax + 8;
+  double *rws = mws + multidot_ws_doubles(mmax);
+  CTN_CUDA(cudaMemsetAsync(mws, 0, multidot_ws_doubles(mmax) * sizeof(double), st));
+  CTN_CUDA(cudaMemsetAsync(rws, 0, reduce_ws_bytes(), st));
+  double h[4];
+  auto fetch2 = [&](int a, int b) -> ctn_status {
+    CTN_CUDA(cudaMemcpyAsync(&h[a], scal + a, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CTN_CUDA(cudaMemcpyAsync(&h[b], scal + b, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CTN_CUDA(cudaStreamSynchronize(st));
+    return CTN_OK;
+  };
+  CTN_TRY(nrm2_f64(vin, n, scal + 0, rws, st));
+  CTN_TRY(div_copy_f64(vin, V, n, scal + 0, st));
+  if (mv(user, V, w, st) != 0) return CTN_ERR_CUDA;
+  CTN_TRY(dot_f64(w, V, n, scal + 1, rws, st));
+  CTN_TRY(lanczos_update_f64(w, V, nullptr, n, scal + 1, nullptr, scal + 3, rws, st));
+  CTN_TRY(fetch2(1, 3));
+  CTN_REQUIRE(std::isfinite(h[1]) && std::isfinite(h[3]), "[ERROR][Lanczos_Exp] non-finite recurrence");
+  const double eps = std::numeric_limits<double>::epsilon();
+  std::vector<double> al{h[1]}, be;  // diagonal, off-diagonal
+  double beta_prev = 0.0, scale = std::max(std::fabs(h[1]), 1.0), wnorm = h[3];
+  double alpha = h[1];
+  std::vector<double> ev, z, Bre, Bim;
+  // B = exp(tau T) for the current T (m x m, row-major), real and imaginary parts
+  auto expm = [&](int m) -> ctn_status {
+    ev.assign(m, 0.0);
+    z.assign((size_t)m * m, 0.0);
+    CTN_TRY(tql(m, al.data(), be.data(), ev.data(), z.data()));
+    Bre.assign((size_t)m * m, 0.0);
+    Bim.assign((size_t)m * m, 0.0);
+    for (int j = 0; j < m; ++j) {
+      const double mag = std::exp(tau_re * ev[j]);
+      const double er = mag * std::cos(tau_im * ev[j]), ei = mag * std::sin(tau_im * ev[j]);
+      const double *zj = &z[(size_t)j * m];
+      for (int a = 0; a < m; ++a)
+        for (int b = 0; b < m; ++b) {
+          Bre[(size_t)a * m + b] += er * zj[a] * zj[b];
+          Bim[(size_t)a * m + b] += ei * zj[a] * zj[b];
+        }
+    }
+    return CTN_OK;
+  };
+  int m = 1;
+  bool have_B = false;
+  for (int i = 1; i < mmax; ++i) {
+    const double beta = wnorm;
+    scale = std::max(scale, std::max(std::fabs(alpha) + std::fabs(beta) + std::fabs(beta_prev), 1.0));
+    if (!(beta > 100.0 * eps * scale * std::sqrt((double)i))) break;  // no new direction
+    CTN_TRY(div_copy_f64(w, V + (int64_t)i * n, n, scal + 3, st));
+    m = i + 1;
+    be.push_back(beta);
+    CTN_CUDA(cudaMemcpyAsync(scal + 2, &be.back(), sizeof(double), cudaMemcpyHostToDevice, st));
+    if (mv(user, V + (int64_t)i * n, w, st) != 0) return CTN_ERR_CUDA;
+    CTN_TRY(dot_f64(w, V + (int64_t)i * n, n, scal + 1, rws, st));
+    CTN_TRY(lanczos_update_f64(w, V + (int64_t)i * n, V + (int64_t)(i - 1) * n, n, scal + 1, scal + 2, scal + 3,
+                               rws, st));
+    CTN_TRY(fetch2(1, 3));
+    CTN_REQUIRE(std::isfinite(h[1]) && std::isfinite(h[3]), "[ERROR][Lanczos_Exp] non-finite recurrence");
+    alpha = h[1];
+    wnorm = h[3];
+    al.push_back(alpha);
+    beta_prev = beta;
+    CTN_TRY(expm(m));
+    have_B = true;
+    const double err = std::hypot(Bre[(size_t)i * m], Bim[(size_t)i * m]);
+    if (err < cvgcrit) break;
+  }
+  if (!have_B) CTN_TRY(expm(m));
+  // out = V B (V^T v): c = V^T v on the device, the coefficients on the host
+  CTN_TRY(multidot_f64(V, vin, n, m, cdev, 0, mws, st));
+  std::vector<double> c(m), dre(m, 0.0), dim(m, 0.0);
+  CTN_CUDA(cudaMemcpyAsync(c.data(), cdev, sizeof(double) * m, cudaMemcpyDeviceToHost, st));
+  CTN_CUDA(cudaStreamSynchronize(st));
+  for (int a = 0; a < m; ++a)
+    for (int b = 0; b < m; ++b) {
+      dre[a] += Bre[(size_t)a * m + b] * c[b];
+      dim[a] += Bim[(size_t)a * m + b] * c[b];
+    }
+  CTN_CUDA(cudaMemcpyAsync(cdev, dre.data(), sizeof(double) * m, cudaMemcpyHostToDevice, st));
+  CTN_TRY(basis_combine_f64(V, n, m, cdev, 1, 1, out_re, st));
+  if (out_im) {
+    CTN_CUDA(cudaMemcpyAsync(cdev + mmax, dim.data(), sizeof(double) * m, cudaMemcpyHostToDevice, st));
+    CTN_TRY(basis_combine_f64(V, n, m, cdev + mmax, 1, 1, out_im, st));
+  }
+  CTN_CUDA(cudaStreamSynchronize(st));
+  if (iters) *iters = m;
+  return CTN_OK;
+}
+}  // namespace ctn
+
+extern "C" size_t ctn_lanczos_exp_work_doubles(int64_t n, int maxiter) {
+  const int mmax = (int)std::min<int64_t>(maxiter, n);
+  return (size_t)n + 8 + 2 * (size_t)mmax + 8 + ctn::multidot_ws_doubles(mmax) + ctn::reduce_ws_bytes() / sizeof(double);
+}
+
+extern "C" ctn_status ctn_lanczos_exp(ctn_matvec_fn matvec, void *user, const double *v, int64_t n, double tau_re,
+                                      double tau_im, double cvgcrit, int maxiter, double *basis, double *work,
+                                      double *out_re, double *out_im, int *iters, void *stream) {
+  CTN_REQUIRE(matvec && v && basis && work && out_re, "ctn_lanczos_exp: null argument");
+  return ctn::lanczos_exp(matvec, user, v, n, tau_re, tau_im, cvgcrit, maxiter, basis, work, out_re, out_im, iters,
+                          ctn::as_stream(stream));
+}

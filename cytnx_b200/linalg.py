@@ -242,3 +242,47 @@ def _lanczos_which(Hop, Tin, which, Maxiter, CvgCrit, k, is_V, ncv, verbose):
     if is_V:
         out.append(Tensor.from_torch(evecs.view(n) if k == 1 else evecs.view(k, n)))
     return out
+
+
+def Lanczos_Exp(Hop, v, tau, CvgCrit: float = 1.0e-14, Maxiter: int = 10000, verbose: bool = False):
+    """exp(tau * Hop) v by Lanczos projection (linalg::Lanczos_Exp, src/linalg/Lanczos_Exp.cpp:
+    264-453): the reference's recurrence, breakdown and stopping rules (ctn_lanczos_exp), on
+    the device and for dense or block UniTensors / Tensors.  A real tau gives a Double
+    result, a complex tau (real-time evolution) a ComplexDouble one."""
+    if CvgCrit <= 0:
+        raise CytnxError("[ERROR][Lanczos_Exp] converge criteria must >0")
+    if Maxiter < 2:
+        raise CytnxError("[ERROR][Lanczos_Exp] Maxiter must >1")
+    if Hop.dtype() != Type.Double:
+        raise CytnxError("[ERROR][Lanczos_Exp] FP64 (Type.Double) operators only on this build")
+    tau = complex(tau)
+    is_uni = isinstance(v, UniTensor)
+    if is_uni:
+        v0 = v.contiguous() if v.dtype() == Type.Double else v.astype(Type.Double).contiguous()
+        x0 = v0.flat_view()
+    else:
+        v0 = v.contiguous().astype(Type.Double)
+        x0 = v0.to_torch().reshape(-1)
+    n = x0.numel()  # the vector's own size, as in the reference (no check against Hop.nx())
+    require_cuda(x0, "Lanczos_Exp")
+    lib = _lib.lib()
+    mmax = min(int(Maxiter), n)
+    basis = torch.empty(mmax * n, dtype=torch.float64, device=x0.device)
+    work = torch.empty(int(lib.ctn_lanczos_exp_work_doubles(n, int(Maxiter))), dtype=torch.float64, device=x0.device)
+    out_re = torch.empty(n, dtype=torch.float64, device=x0.device)
+    out_im = torch.empty(n, dtype=torch.float64, device=x0.device) if tau.imag != 0 else None
+    cb = _Callback(Hop, v0, basis, work, n, is_uni)
+    iters = ctypes.c_int(0)
+    st = lib.ctn_lanczos_exp(cb.fn, None, x0.data_ptr(), n, tau.real, tau.imag, float(CvgCrit), int(Maxiter),
+                             basis.data_ptr(), work.data_ptr(), out_re.data_ptr(),
+                             out_im.data_ptr() if out_im is not None else None, ctypes.byref(iters),
+                             _lib.stream_ptr())
+    if cb.err is not None:
+        raise cb.err
+    _lib.check(st, "Lanczos_Exp")
+    if verbose:
+        print(f"[Lanczos_Exp] Krylov dimension {iters.value}")
+    flat = out_re if out_im is None else torch.complex(out_re, out_im)
+    if is_uni:
+        return v0.with_flat(flat)
+    return Tensor.from_torch(flat.view(*v0.shape()))

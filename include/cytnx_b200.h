@@ -38,6 +38,8 @@
  *   ctn_lanczos_gnd
  *       linalg::Lanczos(..., method="Gnd") -> Lanczos_Gnd_Ut
  *       (src/linalg/Lanczos_Gnd_Ut.cpp:29-199).
+ *   ctn_lanczos_exp
+ *       linalg::Lanczos_Exp (src/linalg/Lanczos_Exp.cpp:264-453).
  *   ctn_lanczos_which / ctn_sym_eigh
  *       linalg::Lanczos(Hop, Tin, which = "SA" / "LA" / "LM", maxiter, cvg_crit, k, is_V, ncv)
  *       (src/linalg/Lanczos.cpp:250-402: ARPACK dsaupd/dseupd).
@@ -322,6 +324,16 @@ ctn_status ctn_lanczos_refined(ctn_matvec_fn matvec_lo, void *user_lo, ctn_matve
  * resolved ncv).  evals (host, k) and evecs (device, k * n, or null) in the reference's
  * order (ascending for SA, descending value / magnitude for LA / LM).  *iters: restart
  * cycles run; *nconv: wanted pairs converged (k unless maxiter ran out). */
+/* exp(tau H) v for a symmetric operator by Lanczos projection: linalg::Lanczos_Exp
+ * (src/linalg/Lanczos_Exp.cpp:264-453, CPU and dense-only there).  Plain three-term
+ * recurrence from v / |v| with the reference's breakdown rule and its stopping rule
+ * |exp(tau T)[i][0]| < cvgcrit; result V exp(tau T) V^T v.  tau = tau_re + i tau_im (real
+ * time needs tau_im != 0 and out_im).  basis: min(maxiter, n) * n doubles; work:
+ * ctn_lanczos_exp_work_doubles(n, maxiter) doubles (device).  *iters: Krylov dimension used. */
+size_t ctn_lanczos_exp_work_doubles(int64_t n, int maxiter);
+ctn_status ctn_lanczos_exp(ctn_matvec_fn matvec, void *user, const double *v, int64_t n, double tau_re,
+                           double tau_im, double cvgcrit, int maxiter, double *basis, double *work, double *out_re,
+                           double *out_im, int *iters, void *stream);
 size_t ctn_lanczos_which_work_doubles(int64_t n, int ncv);
 ctn_status ctn_lanczos_which(ctn_matvec_fn matvec, void *user, const double *v0, int64_t n, int which, int k,
                              int ncv, int maxiter, double tol, double *basis, double *work, double *evals,

@@ -191,3 +191,14 @@ def test_sym_eigh_matches_numpy():
         assert np.abs(np.sort(w) - np.linalg.eigvalsh(A)).max() < 1e-12 * max(1.0, np.abs(w).max())
         assert np.abs(A @ z - z * w).max() < 1e-12 * max(1.0, np.abs(w).max())
         assert np.abs(z.T @ z - np.eye(n)).max() < 1e-13
+
+
+def test_lanczos_exp_argument_errors():
+    import cytnx_b200 as c
+    from cytnx_b200._lib import CytnxError
+
+    H = c.LinOp("mv", 10, c.Type.Double, c.Device.cuda)
+    with pytest.raises(CytnxError, match="converge criteria must >0"):
+        c.linalg.Lanczos_Exp(H, None, -0.1, CvgCrit=0.0)
+    with pytest.raises(CytnxError, match="Maxiter must >1"):
+        c.linalg.Lanczos_Exp(H, None, -0.1, Maxiter=1)
