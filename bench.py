@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--matvec-only", action="store_true",
                     help="profiling driver: bind the headline form with --tiles, run warmup + steps matvecs, exit")
     ap.add_argument("--tiles", default="", help="step-1,step-4 tile widths for --matvec-only (e.g. 192,128)")
+    ap.add_argument("--lanczos-only", type=int, default=0,
+                    help="profiling driver: N restart cycles of the refined Lanczos (headline form, --tiles, "
+                         "Krylov dimension 32), the cycles inside a profiler start/stop range, then exit")
     ap.add_argument("--permute-only", action="store_true",
                     help="profiling driver: the large permutes of the permute section, once each, then exit")
     ap.add_argument("--batch-only", type=int, default=0,
@@ -287,6 +290,23 @@ def main():
         if world > 1:
             dist.destroy_process_group()
         return
+    if args.lanczos_only > 0:  # restart cycles of the refined driver inside a profiler range (ncu)
+        if args.tiles and args.precision != "fp64":
+            b1, b4 = (int(t) for t in args.tiles.split(","))
+            H.set_tiles(b1, b4, args.precision)
+        H.lanczos_refined(psi, precision=args.precision, krylov_dim=32, max_restarts=2, tol=0.0)  # warm
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        r = H.lanczos_refined(psi, precision=args.precision, krylov_dim=32, max_restarts=args.lanczos_only, tol=0.0)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        if rank == 0:
+            print(json.dumps({"lanczos_only": True, "precision": args.precision, "D": args.D,
+                              "matvecs_lo": r["matvecs_lo"], "matvecs_fp64": r["matvecs_fp64"],
+                              "energy": r["energy"]}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
     flops = H.algorithmic_flops()
     tiles = {f: H.autotune(f) for f in ("bf16x3", "3xtf32")}
     x = psi.flat_view()
@@ -383,7 +403,8 @@ def main():
     # refinement matvec per restart; energies are FP64 Rayleigh quotients of the returned vectors
     refined = {}
     for form in forms:
-        H.lanczos_refined(psi, precision=form, krylov_dim=8, max_restarts=2, tol=0.0)  # warm
+        # warm at the same Krylov dimension (its buffers come from the caching allocator afterwards)
+        H.lanczos_refined(psi, precision=form, krylov_dim=32, max_restarts=2, tol=0.0)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         r = H.lanczos_refined(psi, precision=form, krylov_dim=32, max_restarts=300, tol=1e-12)
