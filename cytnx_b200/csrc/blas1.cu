@@ -261,13 +261,44 @@ __global__ void __launch_bounds__(RT) k_lanczos_step(const double *__restrict__ 
 }
 
 // out = sum_j c[j] * K[j]  (Krylov combination), c on device
+// (16-byte loads of four Krylov vectors at a time when every row is 16-byte aligned)
+template <bool VEC>
 __global__ void __launch_bounds__(RT) k_combine(const double *__restrict__ K, int64_t n, int m,
                                                const double *__restrict__ c, double *__restrict__ out) {
+  const int64_t tid = (int64_t)blockIdx.x * RT + threadIdx.x;
   const int64_t step = (int64_t)gridDim.x * RT;
-  for (int64_t i = (int64_t)blockIdx.x * RT + threadIdx.x; i < n; i += step) {
-    double s = 0.0;
-    for (int j = 0; j < m; ++j) s = fma(c[j], K[(int64_t)j * n + i], s);
-    out[i] = s;
+  if (VEC) {
+    const int64_t n2 = n / 2;
+    const double2 *K2 = reinterpret_cast<const double2 *>(K);
+    double2 *o2 = reinterpret_cast<double2 *>(out);
+    for (int64_t i = tid; i < n2; i += step) {
+      double sx = 0.0, sy = 0.0;
+      int j = 0;
+      for (; j + 4 <= m; j += 4) {
+        const double2 a0 = K2[(int64_t)j * n2 + i], a1 = K2[(int64_t)(j + 1) * n2 + i];
+        const double2 a2 = K2[(int64_t)(j + 2) * n2 + i], a3 = K2[(int64_t)(j + 3) * n2 + i];
+        sx = fma(c[j], a0.x, sx);
+        sy = fma(c[j], a0.y, sy);
+        sx = fma(c[j + 1], a1.x, sx);
+        sy = fma(c[j + 1], a1.y, sy);
+        sx = fma(c[j + 2], a2.x, sx);
+        sy = fma(c[j + 2], a2.y, sy);
+        sx = fma(c[j + 3], a3.x, sx);
+        sy = fma(c[j + 3], a3.y, sy);
+      }
+      for (; j < m; ++j) {
+        const double2 a = K2[(int64_t)j * n2 + i];
+        sx = fma(c[j], a.x, sx);
+        sy = fma(c[j], a.y, sy);
+      }
+      o2[i] = make_double2(sx, sy);
+    }
+  } else {
+    for (int64_t i = tid; i < n; i += step) {
+      double s = 0.0;
+      for (int j = 0; j < m; ++j) s = fma(c[j], K[(int64_t)j * n + i], s);
+      out[i] = s;
+    }
   }
 }
 
@@ -329,6 +360,13 @@ __global__ void __launch_bounds__(RT) k_basis_combine(const double *__restrict__
   }
 }
 
+// streaming kernels of the refined Lanczos step: up to MAXCTA CTAs (about seven per SM) for
+// more loads in flight
+int grid_stream(int64_t n) {
+  const int64_t g = (n + RT * 4 - 1) / (RT * 4);
+  return (int)std::max<int64_t>(1, std::min<int64_t>(g, MAXCTA));
+}
+
 int grid_for(int64_t n) {
   static int nsm = 0;
   if (!nsm) {
@@ -380,7 +418,7 @@ static bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 
 
 ctn_status dot2s_f64(const double *w, const double *a, const double *b, int64_t n, const double *s, double *out_a,
                      double *out_b, double *ws2, cudaStream_t st) {
-  const int g = grid_for(n);
+  const int g = grid_stream(n);
   unsigned *ticket = reinterpret_cast<unsigned *>(ws2 + 2 * MAXCTA);
   if (aligned16(w) && aligned16(a) && aligned16(b))
     k_dot2s<true><<<g, RT, 0, st>>>(w, a, b, n, s, ws2, ticket, out_a, out_b);
@@ -393,7 +431,7 @@ ctn_status dot2s_f64(const double *w, const double *a, const double *b, int64_t 
 ctn_status lanczos_step_f64(const double *w, const double *u, const double *up, const double *q, double *dst,
                             int64_t n, const double *alpha, const double *gamma, const double *s, const double *sp,
                             double *nrm, double *ws, cudaStream_t st) {
-  const int g = grid_for(n);
+  const int g = grid_stream(n);
   unsigned *ticket = reinterpret_cast<unsigned *>(ws + MAXCTA);
   const bool vec = aligned16(w) && aligned16(u) && aligned16(dst) && (!up || aligned16(up)) && (!q || aligned16(q));
   if (vec)
@@ -410,7 +448,10 @@ ctn_status div_copy_f64(const double *x, double *y, int64_t n, const double *a, 
   return CTN_OK;
 }
 ctn_status combine_f64(const double *K, int64_t n, int m, const double *c, double *out, cudaStream_t st) {
-  k_combine<<<grid_for(n), RT, 0, st>>>(K, n, m, c, out);
+  if ((n & 1) == 0 && aligned16(K) && aligned16(out))
+    k_combine<true><<<grid_stream(n), RT, 0, st>>>(K, n, m, c, out);
+  else
+    k_combine<false><<<grid_for(n), RT, 0, st>>>(K, n, m, c, out);
   CTN_CHECK_LAUNCH();
   return CTN_OK;
 }
