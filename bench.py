@@ -257,11 +257,14 @@ def main():
         val = flops / sec / 1e12
         line = {"metric": "U(1) H_eff matvec TFLOP/s & Lanczos s/step, split-prec vs FP64, dE<=1e-9",
                 "impl": "reference", "value": val, "unit": "TFLOP/s", "n_gpus": args.gpus, "steps": n,
-                "warmup": 1, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+                "steps_requested": args.steps, "warmup": 1, "ms_per_step": sec * 1e3, "higher_is_better": True,
+                "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded numpy PCG64)",
                 "config": dict(config_base, parallelism="cpu"),
                 "cpu_baseline": {"value": val, "unit": "TFLOP/s", "cores": threads, "kind": "port",
-                                 "sample": f"{n} matvecs at D={args.D} (oracle restatement, OpenBLAS dgemm)"},
+                                 "sample": f"{n} whole matvecs at D={args.D} after one untimed one (oracle "
+                                           f"restatement, OpenBLAS dgemm; one matvec takes seconds on the host, so "
+                                           f"the run is bounded by time, not by --steps)"},
                 "e2e": {"value": val, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
