@@ -163,7 +163,10 @@ ctn_status lanczos_gnd(int (*mv)(void *, const double *, double *, void *), void
   CTN_REQUIRE(cvgcrit > 0, "[Lanczos] converge criteria must >0");
   CTN_REQUIRE(n > 0, "[Lanczos] empty vector");
   double *w = work;                      // new_psi
-  double *scal = work + n;               // device scalars [0]=norm [1]=alpha [2]=beta [3]=nrm
+  // device scalars: [0] |psi0|, [1] alpha, [2] / [3] the norms of w, alternately written by one
+  // update and read as beta (the coefficient of psi_{i-1}) by the next, so no value travels
+  // back to the device; one host read of [1..3] per iteration (the reference's .item() calls)
+  double *scal = work + n;
   double *ws = work + n + 8;             // reduction workspace (zeroed below)
   CTN_CUDA(cudaMemsetAsync(ws, 0, reduce_ws_bytes(), st));
   double host[4];
@@ -182,10 +185,10 @@ ctn_status lanczos_gnd(int (*mv)(void *, const double *, double *, void *), void
   // i = 0
   if (mv(user, krylov, w, st) != 0) return CTN_ERR_CUDA;
   CTN_TRY(dot_f64(w, krylov, n, scal + 1, ws, st));
-  CTN_TRY(lanczos_update_f64(w, krylov, nullptr, n, scal + 1, scal + 2, scal + 3, ws, st));
-  CTN_TRY(fetch(1, &host[1]));
-  CTN_TRY(fetch(3, &host[3]));
-  double alpha = host[1], beta = host[3];
+  CTN_TRY(lanczos_update_f64(w, krylov, nullptr, n, scal + 1, nullptr, scal + 2, ws, st));
+  CTN_CUDA(cudaMemcpyAsync(&host[1], scal + 1, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CTN_CUDA(cudaStreamSynchronize(st));
+  double alpha = host[1], beta = host[2];
   As.push_back(alpha);
   Bs.push_back(beta);
   if (beta == 0.0) {
@@ -194,8 +197,7 @@ ctn_status lanczos_gnd(int (*mv)(void *, const double *, double *, void *), void
     CTN_CUDA(cudaMemcpyAsync(eigvec, krylov, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     return CTN_OK;
   }
-  CTN_CUDA(cudaMemcpyAsync(scal + 2, &beta, sizeof(double), cudaMemcpyHostToDevice, st));
-  CTN_TRY(div_copy_f64(w, krylov + n, n, scal + 3, st));
+  CTN_TRY(div_copy_f64(w, krylov + n, n, scal + 2, st));
   nk = 2;
   double E = alpha;
   evals.assign(1, alpha);
@@ -205,23 +207,22 @@ ctn_status lanczos_gnd(int (*mv)(void *, const double *, double *, void *), void
     it = i + 1;
     const double *p1 = krylov + (int64_t)i * n;
     const double *p0 = krylov + (int64_t)(i - 1) * n;
+    double *b_old = scal + 2 + ((i - 1) & 1), *b_new = scal + 2 + (i & 1);
     if (mv(user, p1, w, st) != 0) return CTN_ERR_CUDA;
     CTN_TRY(dot_f64(w, p1, n, scal + 1, ws, st));
-    // beta (old) is at scal[2]
-    CTN_TRY(lanczos_update_f64(w, p1, p0, n, scal + 1, scal + 2, scal + 3, ws, st));
-    CTN_TRY(fetch(1, &host[1]));
-    CTN_TRY(fetch(3, &host[3]));
+    CTN_TRY(lanczos_update_f64(w, p1, p0, n, scal + 1, b_old, b_new, ws, st));
+    CTN_CUDA(cudaMemcpyAsync(&host[1], scal + 1, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CTN_CUDA(cudaStreamSynchronize(st));
     alpha = host[1];
     As.push_back(alpha);
     const int m = (int)As.size();
     evals.assign(m, 0.0);
     evecs.assign((size_t)m * m, 0.0);
     CTN_TRY(tql(m, As.data(), Bs.data(), evals.data(), evecs.data()));
-    beta = host[3];
+    beta = host[2 + (i & 1)];
     Bs.push_back(beta);
     if (beta == 0.0) break;
-    CTN_CUDA(cudaMemcpyAsync(scal + 2, &beta, sizeof(double), cudaMemcpyHostToDevice, st));
-    CTN_TRY(div_copy_f64(w, krylov + (int64_t)(i + 1) * n, n, scal + 3, st));
+    CTN_TRY(div_copy_f64(w, krylov + (int64_t)(i + 1) * n, n, b_new, st));
     nk = i + 2;
     const double ediff = std::fabs(E - evals[0]);
     if (ediff < cvgcrit) break;
