@@ -249,7 +249,14 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
   const uint32_t tmem_base = *tmem_holder;
 
   constexpr uint32_t FMT = KIND == TC_TF32 ? 2u : 1u;
-  constexpr uint32_t IDESC = (1u << 4) | (FMT << 7) | (FMT << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+  // instruction descriptor without its N field: each tile sets N to the columns it has
+  // (the last tile of a group is narrower than BN; N is rounded up to a multiple of 16,
+  // the padded panel rows are zero), so no MMA work and no B bytes go to padding
+  constexpr uint32_t IDESC0 = (1u << 4) | (FMT << 7) | (FMT << 10) | ((uint32_t)(TC_BM >> 4) << 24);
+  auto tile_n = [](const TcGroup &g, const TcTile &tl) -> int {
+    const int rem = g.N - tl.nt * BN;
+    return rem >= BN ? BN : ((rem + 15) & ~15);
+  };
   constexpr int KSTEPS = 4;  // MMA K per instruction = 32 bytes of the 128-byte slice
 
   if (warp == 0 && lane == 0) {
@@ -262,19 +269,20 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
     for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
       const TcTile tl = p.tiles[t];
       const TcGroup g = p.groups[tl.group];
+      const uint32_t b_bytes = (uint32_t)tile_n(g, tl) * TC_ROW_BYTES;  // the tile's B rows only
       for (int kb = 0; kb < g.kb; ++kb) {
         if (!mbar_wait(&empty[stage], phase ^ 1, p.err, 1)) {
           ok = false;
           break;
         }
         uint8_t *st = smem + stage * SM::STAGE_BYTES;
-        mbar_expect_tx(&full[stage], SM::STAGE_BYTES);
+        mbar_expect_tx(&full[stage], 2 * SM::A_BYTES + 2 * b_bytes);
         const int64_t ao = g.a_off + ((int64_t)tl.mt * g.kb + kb) * SM::A_BYTES;
         const int64_t bo = g.b_off + ((int64_t)tl.nt * g.kb + kb) * SM::B_BYTES;
         bulk_g2s(st, p.a_hi + ao, SM::A_BYTES, &full[stage]);
         bulk_g2s(st + SM::A_BYTES, p.a_lo + ao, SM::A_BYTES, &full[stage]);
-        bulk_g2s(st + 2 * SM::A_BYTES, p.b_hi + bo, SM::B_BYTES, &full[stage]);
-        bulk_g2s(st + 2 * SM::A_BYTES + SM::B_BYTES, p.b_lo + bo, SM::B_BYTES, &full[stage]);
+        bulk_g2s(st + 2 * SM::A_BYTES, p.b_hi + bo, b_bytes, &full[stage]);
+        bulk_g2s(st + 2 * SM::A_BYTES + SM::B_BYTES, p.b_lo + bo, b_bytes, &full[stage]);
         filled[stage]++;
         if (++stage == STAGES) {
           stage = 0;
@@ -296,6 +304,7 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
     for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
       const TcTile tl = p.tiles[t];
       const TcGroup g = p.groups[tl.group];
+      const uint32_t idesc = IDESC0 | ((uint32_t)(tile_n(g, tl) >> 3) << 17);
       if (!mbar_wait(&tempty[acc], acc_phase ^ 1, p.err, 2)) break;
       tc_fence_after();
       const uint32_t d = tmem_base + (uint32_t)(acc * BN);
@@ -311,9 +320,9 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
 #pragma unroll
         for (int j = 0; j < KSTEPS; ++j) {
           const uint64_t adv = (uint64_t)(j * 32) >> 4;  // +32 bytes along K inside the swizzle row
-          tc_mma(d, alo + adv, bhi + adv, IDESC, (kb | j) != 0, KIND);
-          tc_mma(d, ahi + adv, blo + adv, IDESC, 1u, KIND);
-          tc_mma(d, ahi + adv, bhi + adv, IDESC, 1u, KIND);
+          tc_mma(d, alo + adv, bhi + adv, idesc, (kb | j) != 0, KIND);
+          tc_mma(d, ahi + adv, blo + adv, idesc, 1u, KIND);
+          tc_mma(d, ahi + adv, bhi + adv, idesc, 1u, KIND);
         }
         issued = true;
         tc_commit(&empty[stage]);
