@@ -120,15 +120,15 @@ class TwoSiteHeff(LinOp):
         self._ws.pop(prec, None)
         self._bound.discard(prec)
 
-    def autotune(self, precision: Optional[str] = None, step1=(128, 160, 192, 256), step4=(96, 128, 144, 160, 256),
-                 reps: int = 5, epilogues=(0, 1)) -> dict:
+    def autotune(self, precision: Optional[str] = None, step1=(128, 160, 192, 256, -192),
+                 step4=(96, 128, 144, 160, 256, -128), reps: int = 5, epilogues=(0, 1)) -> dict:
         """Pick the tensor-core tile width and epilogue form of steps 1 and 4 by timing them.
 
         The two GEMMs are independent kernels, so each is tuned with the other fixed:
         every width re-packs the operand panels (they depend on the width); for each
         width both epilogue forms (0 direct, 1 staged through shared memory) are timed
-        with the per-phase CUDA-event profile (ctn_heff2_profile).  Negative widths
-        (2-CTA tiles) may be passed as candidates too."""
+        with the per-phase CUDA-event profile (ctn_heff2_profile).  Negative widths are the
+        2-CTA tiles (256 rows, cluster of two SMs); one of each step is a default candidate."""
         import ctypes as ct
 
         precision = (precision or self.precision).lower()
