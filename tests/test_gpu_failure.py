@@ -1,0 +1,50 @@
+"""Fault injection on the device path without a GPU fault: NaN injected into an input vector
+or an environment block comes back as an error status from the drivers, and the context stays
+usable for the next call."""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _build(D=64, seed=1):
+    from cytnx_b200 import workloads as W
+
+    return W.build_two_site(W.xxz_spec(D), W.xxz_mpo_values(1.0, 1.0), seed=seed, device=0)
+
+
+def test_nan_in_start_vector_is_reported():
+    import cytnx_b200 as c
+    from cytnx_b200._lib import CytnxError
+
+    psi, L, M1, M2, R = _build()
+    H = c.TwoSiteHeff(L, M1, M2, R, psi)
+    bad = psi.clone()
+    bad.flat_view()[3] = math.nan
+    with pytest.raises(CytnxError, match="non-finite"):
+        H.lanczos_refined(bad, precision="bf16x3", krylov_dim=8, max_restarts=4)
+    with pytest.raises(CytnxError, match="non-finite"):
+        c.linalg.Lanczos(Hop=H, Tin=bad, method="Gnd", Maxiter=4, CvgCrit=1e-12)
+    # the context is intact: the same operator still runs on a good vector
+    r = H.lanczos_refined(psi, precision="bf16x3", krylov_dim=8, max_restarts=40, tol=1e-10)
+    assert math.isfinite(r["energy"]) and r["residual"] <= 1e-10 * abs(r["energy"])
+
+
+def test_nan_in_environment_is_reported():
+    import cytnx_b200 as c
+    from cytnx_b200._lib import CytnxError
+
+    psi, L, M1, M2, R = _build(seed=2)
+    Lb = L.clone()
+    Lb.flat_view()[0] = math.nan
+    H = c.TwoSiteHeff(Lb, M1, M2, R, psi)
+    with pytest.raises(CytnxError, match="non-finite"):
+        H.lanczos_refined(psi, precision="bf16x3", krylov_dim=8, max_restarts=4)
+    H2 = c.TwoSiteHeff(L, M1, M2, R, psi)
+    x = psi.flat_view()
+    y = torch.empty_like(x)
+    H2.apply_flat(x, y, "fp64")
+    assert torch.isfinite(y).all()
