@@ -103,6 +103,24 @@ def test_short_output_axis_staged(dtype):
         assert np.array_equal(out, O.permute(a, p)), (shape, p)
 
 
+@pytest.mark.parametrize("dtype", [np.float64, np.int64, np.complex64, np.float32, np.int32, np.int16, np.bool_])
+def test_tma_staged_transpose_ragged(dtype):
+    """Transposes above 1 MB with 16-byte input strides: the TMA-staged kernel (1-, 2- and 4-byte
+    elements) and the register tile (8-byte elements), ragged tiles along both transposed axes,
+    with and without a batch axis."""
+    rng = np.random.default_rng(7)
+    for shape, p in [((300, 5, 704), (2, 1, 0)), ((64, 3, 7, 1040), (3, 1, 2, 0)), ((2000, 520), (1, 0))]:
+        if dtype == np.bool_:
+            a = rng.integers(0, 2, shape).astype(np.bool_)
+        elif np.issubdtype(dtype, np.complexfloating):
+            a = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(dtype)
+        elif np.issubdtype(dtype, np.floating):
+            a = rng.standard_normal(shape).astype(dtype)
+        else:
+            a = rng.integers(0, 120, shape).astype(dtype)
+        assert np.array_equal(_permute_dev(a, p), O.permute(a, p)), (shape, p)
+
+
 def test_short_output_axis_unaligned_destination():
     """ctn_permute into a destination 4 bytes past a 16-byte boundary (the element-wise
     store path of the staged kernel) and at a 16-byte boundary, same input."""
