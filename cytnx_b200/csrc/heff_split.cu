@@ -456,6 +456,7 @@ ctn_status split_set_env(HeffSplit *s, const void *L, const void *R, void *ws, c
   }
   CTN_TRY(s->g1.upload(st));
   CTN_TRY(s->g4.upload(st));
+  CTN_TRY(s->g1.bind_c32((float *)(s->ws + s->o_x1), st));
   CTN_TRY(s->pk_P.upload(st));
   return CTN_OK;
 }

@@ -207,7 +207,7 @@ struct TcSmem {
   static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
   static constexpr int RING = STAGES * STAGE_BYTES;
   static constexpr int BAR_OFF = RING;                 // full[S], empty[S], tfull[2], tempty[2], drain
-  static constexpr int EPI_OFF = RING + 256;  // four warps' epilogue slabs
+  static constexpr int EPI_OFF = RING + 1024;  // four warps' epilogue slabs (1024-aligned: TMA store boxes)
   static constexpr int TOTAL = EPI_OFF + EPI_BYTES;
 };
 
@@ -369,6 +369,12 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
       // made every store instruction touch 32 rows and kept the epilogue of a 128 x 192
       // FP32 tile at ~4 us, longer than the next tile's MMAs.
       const bool any_row = __any_sync(0xffffffffu, dst >= 0);  // warp-uniform: rows of this quarter inside M
+      // Row-strided FP32 output with a tensor map: each 32 x 32 piece goes into this warp's
+      // 4 KB box (SWIZZLE_128B layout, conflict-free) and one lane stores it with a 2-D TMA
+      // store; rows past M and columns past N are clipped by the tensor map.  The box is
+      // reused once the previous store has read it (bulk-group wait on the read).
+      const bool tma_out = p.cmaps != nullptr && g.mode == 0 && p.epi_staged;
+      uint8_t *box = reinterpret_cast<uint8_t *>(smem + SM::EPI_OFF) + (warp - 2) * 4096;
 #pragma unroll 1
       for (int c0 = 0; c0 < BN && any_row; c0 += 32) {
         uint32_t v[32];
@@ -378,7 +384,27 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
         const int cg0 = tl.nt * BN + c0;
         if (cg0 >= g.N) continue;  // warp-uniform: the whole piece is past the tile edge
         const int ncol = min(min(32, BN - c0), g.N - cg0);  // a 32-column piece may pass the tile edge
-        if (p.epi_staged) {
+        if (tma_out) {
+          if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+          __syncwarp();
+#pragma unroll
+          for (int j = 0; j < 8; ++j)
+            *reinterpret_cast<float4 *>(box + lane * 128 + ((j ^ (lane & 7)) << 4)) =
+                make_float4(__uint_as_float(v[4 * j]), __uint_as_float(v[4 * j + 1]), __uint_as_float(v[4 * j + 2]),
+                            __uint_as_float(v[4 * j + 3]));
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) {
+            const CUtensorMap *map = reinterpret_cast<const CUtensorMap *>(p.cmaps) + tl.group;
+            const int row0 = tl.mt * TC_BM + q * 32;
+            asm volatile(
+                "cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                    reinterpret_cast<uint64_t>(map)),
+                "r"(cg0), "r"(row0), "r"(smem_u32(box))
+                : "memory");
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+          }
+        } else if (p.epi_staged) {
           epi_store_piece(v, slab, lane, dst, cg0, ncol, g.mode, p.c32, p.c64);
         } else if (dst >= 0) {
           epi_store_direct(v, dst, cg0, ncol, g.mode, p.c32, p.c64);
@@ -392,6 +418,7 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
         acc_phase ^= 1;
       }
     }
+    if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");  // this warp's TMA stores done
   }
   tc_fence_before();
   __syncthreads();
@@ -1052,11 +1079,52 @@ ctn_status TcGemm::upload(cudaStream_t st) {
   return CTN_OK;
 }
 
+ctn_status TcGemm::bind_c32(float *c32, cudaStream_t st) {
+  if (pair || !c32) return CTN_OK;
+  bool any = false;
+  for (const auto &g : groups) any |= g.mode == 0;
+  if (!any) return CTN_OK;
+  int dev = 0;
+  CTN_CUDA(cudaGetDevice(&dev));
+  if (d_cmaps && cmaps_for == c32 && cmaps_dev == dev) return CTN_OK;
+  const EncodeTiledFn enc = encode_tiled();
+  if (!enc) return CTN_OK;  // no driver entry point: the plain staged stores stay in use
+  std::vector<CUtensorMap> maps(groups.size());
+  std::memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
+  for (size_t i = 0; i < groups.size(); ++i) {
+    const TcGroup &g = groups[i];
+    if (g.mode != 0) continue;
+    void *base = c32 + g.c_off;
+    if ((reinterpret_cast<uintptr_t>(base) & 15) != 0 || ((int64_t)g.ldc * 4) % 16 != 0) return CTN_OK;
+    const cuuint64_t dims[2] = {(cuuint64_t)g.N, (cuuint64_t)g.M};
+    const cuuint64_t strides[1] = {(cuuint64_t)g.ldc * 4};
+    const cuuint32_t box[2] = {32, 32};
+    const cuuint32_t estr[2] = {1, 1};
+    if (enc(&maps[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return CTN_OK;  // keep the plain stores
+  }
+  if (d_cmaps && cmaps_dev != dev) {
+    cudaFree(d_cmaps);
+    d_cmaps = nullptr;
+  }
+  if (!d_cmaps) CTN_CUDA(cudaMalloc(&d_cmaps, maps.size() * sizeof(CUtensorMap)));
+  CTN_CUDA(cudaMemcpyAsync(d_cmaps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, st));
+  CTN_CUDA(cudaStreamSynchronize(st));
+  cmaps_for = c32;
+  cmaps_dev = dev;
+  return CTN_OK;
+}
+
 ctn_status TcGemm::run(const uint8_t *a_hi, const uint8_t *a_lo, const uint8_t *b_hi, const uint8_t *b_lo,
                        float *c32, double *c64, int *err, cudaStream_t st) {
   if (tiles.empty()) return CTN_OK;
   CTN_TRY(upload(st));
   TcParams prm;
+  int dev = 0;
+  CTN_CUDA(cudaGetDevice(&dev));
+  prm.cmaps = (d_cmaps && c32 && cmaps_for == c32 && cmaps_dev == dev) ? d_cmaps : nullptr;
   const char *q = (const char *)d_mem;
   prm.groups = (const TcGroup *)q;
   prm.tiles = (const TcTile *)(q + groups.size() * sizeof(TcGroup));
@@ -1080,6 +1148,7 @@ ctn_status tc_launch_tables(int kind, int bn, const TcGroup *d_groups, const TcT
                             const uint8_t *b_lo, float *c32, double *c64, int *err, cudaStream_t st) {
   if (ntiles == 0) return CTN_OK;
   TcParams prm;
+  prm.cmaps = nullptr;
   prm.groups = d_groups;
   prm.tiles = d_tiles;
   prm.rowmap = d_rowmap;
@@ -1118,6 +1187,7 @@ ctn_status pack_launch_tables(int kind, const PackSeg *d_segs, const int64_t *d_
 
 TcGemm::~TcGemm() {
   if (d_mem) cudaFree(d_mem);
+  if (d_cmaps) cudaFree(d_cmaps);
 }
 
 void Packer::finalize() {

@@ -53,6 +53,9 @@ struct TcParams {
   int *err;  // device error word: 0 ok, else the code of the wait that gave up
   int epi_staged;  // 1: epilogue through the shared-memory slab (whole row segments), 0: direct
   int64_t a_bytes, b_bytes;  // panel sizes (2-CTA form: extents of its TMA views)
+  // one 2-D FP32 tensor map per group (CUtensorMap, 128 bytes each) over the row-strided
+  // output of mode-0 groups, or null: the staged epilogue then stores 32 x 32 pieces by TMA
+  const void *cmaps;
 };
 
 // byte offset of element (r, k) inside a panel of tiles with `rows` rows per tile
@@ -92,8 +95,14 @@ struct TcGemm {
   int add_group(int M, int N, int K, int mode, int64_t c_off, int ldc, int64_t rm_off);
   void finalize();  // builds the tile list (largest K first)
   ctn_status upload(cudaStream_t st);
+  // encode (once per output buffer) the TMA store maps of the mode-0 groups over c32; run()
+  // with the same c32 then stores those groups' tiles by TMA
+  ctn_status bind_c32(float *c32, cudaStream_t st);
   ctn_status run(const uint8_t *a_hi, const uint8_t *a_lo, const uint8_t *b_hi, const uint8_t *b_lo, float *c32,
                  double *c64, int *err, cudaStream_t st);
+  void *d_cmaps = nullptr;
+  const float *cmaps_for = nullptr;
+  int cmaps_dev = -1;
   ~TcGemm();
 };
 
