@@ -503,7 +503,7 @@ struct TcSmem2 {
   static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
   static constexpr int RING = STAGES * STAGE_BYTES;
   static constexpr int BAR_OFF = RING;  // full[S], empty[S], tfull[2], tempty[2], drain
-  static constexpr int EPI_OFF = RING + 256;
+  static constexpr int EPI_OFF = RING + 1024;  // 1024-aligned: TMA store boxes
   static constexpr int TOTAL = EPI_OFF + EPI_BYTES;
 };
 
@@ -661,6 +661,9 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p, con
       int64_t dst = -1;
       if (r < g.M) dst = g.mode == 0 ? g.c_off + (int64_t)r * g.ldc : p.rowmap[g.rm_off + r];
       const bool any_row = __any_sync(0xffffffffu, dst >= 0);  // warp-uniform: rows of this quarter inside M
+      // row-strided FP32 output with a tensor map: TMA stores of 32 x 32 pieces (as in k_tc_gemm)
+      const bool tma_out = p.cmaps != nullptr && g.mode == 0 && p.epi_staged;
+      uint8_t *box = reinterpret_cast<uint8_t *>(smem + SM::EPI_OFF) + (warp - 2) * 4096;
 #pragma unroll 1
       for (int c0 = 0; c0 < BN && any_row; c0 += 32) {
         uint32_t v[32];
@@ -670,7 +673,27 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p, con
         const int cg0 = tl.nt * BN + c0;
         if (cg0 >= g.N) continue;  // warp-uniform: the whole piece is past the tile edge
         const int ncol = min(min(32, BN - c0), g.N - cg0);  // a 32-column piece may pass the tile edge
-        if (p.epi_staged) {
+        if (tma_out) {
+          if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+          __syncwarp();
+#pragma unroll
+          for (int j = 0; j < 8; ++j)
+            *reinterpret_cast<float4 *>(box + lane * 128 + ((j ^ (lane & 7)) << 4)) =
+                make_float4(__uint_as_float(v[4 * j]), __uint_as_float(v[4 * j + 1]), __uint_as_float(v[4 * j + 2]),
+                            __uint_as_float(v[4 * j + 3]));
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) {
+            const CUtensorMap *map = reinterpret_cast<const CUtensorMap *>(p.cmaps) + tl.group;
+            const int row0 = (2 * tl.mt + (int)rank) * TC_BM + q * 32;
+            asm volatile(
+                "cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                    reinterpret_cast<uint64_t>(map)),
+                "r"(cg0), "r"(row0), "r"(smem_u32(box))
+                : "memory");
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+          }
+        } else if (p.epi_staged) {
           epi_store_piece(v, slab, lane, dst, cg0, ncol, g.mode, p.c32, p.c64);
         } else if (dst >= 0) {
           epi_store_direct(v, dst, cg0, ncol, g.mode, p.c32, p.c64);
@@ -687,6 +710,7 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p, con
         acc_phase ^= 1;
       }
     }
+    if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");  // this warp's TMA stores done
   }
   tc_fence_before();
   cluster_sync_all();  // no CTA leaves while its peer may still touch its shared memory or TMEM
@@ -1080,7 +1104,7 @@ ctn_status TcGemm::upload(cudaStream_t st) {
 }
 
 ctn_status TcGemm::bind_c32(float *c32, cudaStream_t st) {
-  if (pair || !c32) return CTN_OK;
+  if (!c32) return CTN_OK;
   bool any = false;
   for (const auto &g : groups) any |= g.mode == 0;
   if (!any) return CTN_OK;
