@@ -41,11 +41,15 @@ static ctn_status device_ws(double **ws) {
 // Numer. Math. 11 (1968) 293-306).  d: diagonal (n), e: sub-diagonal (n-1).
 // Eigenvalues ascending; z (n x n, row-major) receives eigenvectors as ROWS, which is
 // the is_row=true layout linalg::Tridiag returns (src/linalg/Tridiag.cpp:83-95).
+// With zrows == nullptr the rotations are not accumulated (O(n^2) instead of O(n^3)); the
+// eigenvalues do not depend on the accumulation and come out bit-identical.
 static ctn_status tql(int n, const double *din, const double *ein, double *w, double *zrows) {
   std::vector<double> d(din, din + n), e(n, 0.0);
   for (int i = 0; i + 1 < n; ++i) e[i] = ein[i];
-  std::vector<double> z((size_t)n * n, 0.0);  // column-major accumulation: z[k + n*i] = comp k of vec i
-  for (int i = 0; i < n; ++i) z[(size_t)i * n + i] = 1.0;
+  // column-major accumulation: z[k + n*i] = comp k of vec i
+  std::vector<double> z(zrows ? (size_t)n * n : 0, 0.0);
+  if (zrows)
+    for (int i = 0; i < n; ++i) z[(size_t)i * n + i] = 1.0;
   for (int l = 0; l < n; ++l) {
     int iter = 0;
     int m;
@@ -83,11 +87,13 @@ static ctn_status tql(int n, const double *din, const double *ein, double *w, do
           p = s * r;
           d[i + 1] = g + p;
           g = c * r - b;
-          double *zi = &z[(size_t)i * n], *zi1 = &z[(size_t)(i + 1) * n];
-          for (int k = 0; k < n; ++k) {
-            f = zi1[k];
-            zi1[k] = s * zi[k] + c * f;
-            zi[k] = c * zi[k] - s * f;
+          if (zrows) {
+            double *zi = &z[(size_t)i * n], *zi1 = &z[(size_t)(i + 1) * n];
+            for (int k = 0; k < n; ++k) {
+              f = zi1[k];
+              zi1[k] = s * zi[k] + c * f;
+              zi[k] = c * zi[k] - s * f;
+            }
           }
         }
         if (early) continue;
@@ -152,13 +158,27 @@ extern "C" ctn_status ctn_tridiag_eigh(int n, const double *d, const double *e, 
 }
 
 namespace ctn {
+// per-thread pinned landing slots for the per-iteration scalars: a device-to-host copy into
+// pageable memory returns only when it has completed, which would hold the host at every
+// queued read; into pinned memory it is queued like a kernel
+static ctn_status pinned_scalars(double **out) {
+  static thread_local double *buf = nullptr;
+  if (!buf) CTN_CUDA(cudaHostAlloc((void **)&buf, 16 * sizeof(double), cudaHostAllocPortable));
+  *out = buf;
+  return CTN_OK;
+}
+
 // Lanczos_Gnd_Ut (src/linalg/Lanczos_Gnd_Ut.cpp:29-162): 3-term recurrence, Tridiag
 // re-solved each iteration, stop on |dE| < cvgcrit or beta == 0; the Ritz vector is
 // the combination of the stored Krylov vectors.  The vectors stay on the device; the
 // two scalars per iteration come to the host as the reference's .item() calls do.
+// speculate: queue iteration i+1 on the device before the host solves iteration i's
+// tridiagonal, so the host solve runs under the next matvec; the iteration queued after the
+// last one runs and is discarded (one extra matvec, results unchanged).  Only for matvecs
+// without side effects.
 ctn_status lanczos_gnd(int (*mv)(void *, const double *, double *, void *), void *user, const double *psi0,
                        int64_t n, int maxiter, double cvgcrit, double *krylov, double *work, double *eigvec,
-                       double *energy, int *iters, cudaStream_t st) {
+                       double *energy, int *iters, cudaStream_t st, bool speculate) {
   CTN_REQUIRE(maxiter >= 2, "[Lanczos] Maxiter must >1");
   CTN_REQUIRE(cvgcrit > 0, "[Lanczos] converge criteria must >0");
   CTN_REQUIRE(n > 0, "[Lanczos] empty vector");
@@ -168,72 +188,72 @@ ctn_status lanczos_gnd(int (*mv)(void *, const double *, double *, void *), void
   // back to the device; one host read of [1..3] per iteration (the reference's .item() calls)
   double *scal = work + n;
   double *ws = work + n + 8;             // reduction workspace (zeroed below)
+  double *cdev = ws + reduce_ws_bytes() / sizeof(double);
+  double *pin;
+  CTN_TRY(pinned_scalars(&pin));
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  struct EvGuard {
+    cudaEvent_t *e;
+    ~EvGuard() {
+      for (int k = 0; k < 2; ++k)
+        if (e[k]) cudaEventDestroy(e[k]);
+    }
+  } guard{ev};
+  for (int k = 0; k < 2; ++k) CTN_CUDA(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming));
   CTN_CUDA(cudaMemsetAsync(ws, 0, reduce_ws_bytes(), st));
-  double host[4];
-  auto fetch = [&](int idx, double *dst) -> ctn_status {
-    CTN_CUDA(cudaMemcpyAsync(dst, scal + idx, sizeof(double), cudaMemcpyDeviceToHost, st));
-    CTN_CUDA(cudaStreamSynchronize(st));
-    return CTN_OK;
-  };
   // psi_1 = Tin / |Tin|
   CTN_TRY(nrm2_f64(psi0, n, scal + 0, ws, st));
-  CTN_TRY(fetch(0, &host[0]));
-  CTN_REQUIRE(host[0] > 0 && std::isfinite(host[0]), "[Lanczos] initial vector has zero or non-finite norm");
-  CTN_TRY(div_copy_f64(psi0, krylov, n, scal + 0, st));
-  std::vector<double> As, Bs, evals, evecs;
-  int nk = 1;  // Krylov vectors stored
-  // i = 0
-  if (mv(user, krylov, w, st) != 0) return CTN_ERR_CUDA;
-  CTN_TRY(dot_f64(w, krylov, n, scal + 1, ws, st));
-  CTN_TRY(lanczos_update_f64(w, krylov, nullptr, n, scal + 1, nullptr, scal + 2, ws, st));
-  CTN_CUDA(cudaMemcpyAsync(&host[1], scal + 1, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CTN_CUDA(cudaMemcpyAsync(pin + 8, scal + 0, sizeof(double), cudaMemcpyDeviceToHost, st));
   CTN_CUDA(cudaStreamSynchronize(st));
-  double alpha = host[1], beta = host[2];
-  As.push_back(alpha);
-  Bs.push_back(beta);
-  if (beta == 0.0) {
-    *energy = alpha;
-    *iters = 1;
-    CTN_CUDA(cudaMemcpyAsync(eigvec, krylov, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  CTN_REQUIRE(pin[8] > 0 && std::isfinite(pin[8]), "[Lanczos] initial vector has zero or non-finite norm");
+  CTN_TRY(div_copy_f64(psi0, krylov, n, scal + 0, st));
+  // iteration i on the device: (i >= 1) psi_i = w / beta_{i-1}; w = H psi_i; alpha_i = <w, psi_i>;
+  // w -= alpha_i psi_i + beta_{i-1} psi_{i-1}; beta_i = |w|; alpha_i, beta_i -> pinned slot i & 1
+  auto queue = [&](int i) -> ctn_status {
+    double *pi = krylov + (int64_t)i * n;
+    double *b_new = scal + 2 + (i & 1);
+    const double *b_old = i ? scal + 2 + ((i - 1) & 1) : nullptr;
+    if (i) CTN_TRY(div_copy_f64(w, pi, n, b_old, st));
+    if (mv(user, pi, w, st) != 0) return CTN_ERR_CUDA;
+    CTN_TRY(dot_f64(w, pi, n, scal + 1, ws, st));
+    CTN_TRY(lanczos_update_f64(w, pi, i ? pi - n : nullptr, n, scal + 1, b_old, b_new, ws, st));
+    CTN_CUDA(cudaMemcpyAsync(pin + 4 * (i & 1), scal + 1, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CTN_CUDA(cudaEventRecord(ev[i & 1], st));
     return CTN_OK;
-  }
-  CTN_TRY(div_copy_f64(w, krylov + n, n, scal + 2, st));
-  nk = 2;
-  double E = alpha;
-  evals.assign(1, alpha);
-  evecs.assign(1, 1.0);
-  int it = 1;
-  for (int i = 1; i < maxiter; ++i) {
+  };
+  std::vector<double> As, Bs, evals, evecs;
+  double E = 0.0;
+  int it = 0;
+  CTN_TRY(queue(0));
+  for (int i = 0; i < maxiter; ++i) {
     it = i + 1;
-    const double *p1 = krylov + (int64_t)i * n;
-    const double *p0 = krylov + (int64_t)(i - 1) * n;
-    double *b_old = scal + 2 + ((i - 1) & 1), *b_new = scal + 2 + (i & 1);
-    if (mv(user, p1, w, st) != 0) return CTN_ERR_CUDA;
-    CTN_TRY(dot_f64(w, p1, n, scal + 1, ws, st));
-    CTN_TRY(lanczos_update_f64(w, p1, p0, n, scal + 1, b_old, b_new, ws, st));
-    CTN_CUDA(cudaMemcpyAsync(&host[1], scal + 1, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CTN_CUDA(cudaStreamSynchronize(st));
-    alpha = host[1];
+    CTN_CUDA(cudaEventSynchronize(ev[i & 1]));
+    const double alpha = pin[4 * (i & 1)], beta = pin[4 * (i & 1) + 1 + (i & 1)];
     As.push_back(alpha);
+    const bool more = beta != 0.0 && i + 1 < maxiter;
+    if (speculate && more) CTN_TRY(queue(i + 1));
     const int m = (int)As.size();
     evals.assign(m, 0.0);
-    evecs.assign((size_t)m * m, 0.0);
-    CTN_TRY(tql(m, As.data(), Bs.data(), evals.data(), evecs.data()));
-    beta = host[2 + (i & 1)];
+    // eigenvalues only inside the loop: the Ritz vector is needed once, after it
+    if (m == 1)
+      evals[0] = alpha;
+    else
+      CTN_TRY(tql(m, As.data(), Bs.data(), evals.data(), nullptr));
     Bs.push_back(beta);
     if (beta == 0.0) break;
-    CTN_TRY(div_copy_f64(w, krylov + (int64_t)(i + 1) * n, n, b_new, st));
-    nk = i + 2;
-    const double ediff = std::fabs(E - evals[0]);
-    if (ediff < cvgcrit) break;
+    if (i >= 1) {
+      if (std::fabs(E - evals[0]) < cvgcrit) break;
+    }
     E = evals[0];
+    if (!speculate && more) CTN_TRY(queue(i + 1));
   }
-  (void)nk;
   // eigenvector = sum_n kry[n] psi_s[n] over the tridiagonal size
   const int m = (int)evals.size();
-  double *coef = scal + 4;  // need m doubles: place after ws instead if m > 4
-  double *cdev = ws + reduce_ws_bytes() / sizeof(double);
-  (void)coef;
+  evecs.assign((size_t)m * m, 0.0);
+  if (m == 1)
+    evecs[0] = 1.0;
+  else
+    CTN_TRY(tql(m, As.data(), Bs.data(), evals.data(), evecs.data()));
   CTN_CUDA(cudaMemcpyAsync(cdev, evecs.data(), sizeof(double) * m, cudaMemcpyHostToDevice, st));
   CTN_TRY(combine_f64(krylov, n, m, cdev, eigvec, st));
   CTN_CUDA(cudaStreamSynchronize(st));
@@ -364,7 +384,7 @@ extern "C" ctn_status ctn_lanczos_gnd(ctn_matvec_fn matvec, void *user, const do
                                       double cvgcrit, double *krylov, double *work, double *eigvec, double *energy,
                                       int *iters, void *stream) {
   return ctn::lanczos_gnd(matvec, user, psi0, n, maxiter, cvgcrit, krylov, work, eigvec, energy, iters,
-                          ctn::as_stream(stream));
+                          ctn::as_stream(stream), /*speculate=*/false);
 }
 
 namespace ctn {

@@ -457,9 +457,10 @@ int heff_mv(void *u, const double *x, double *y, void *stream) {
 extern "C" ctn_status ctn_heff2_lanczos_gnd(ctn_heff2_plan *plan, int precision, const double *psi0, int maxiter,
                                             double cvgcrit, double *krylov, double *work, double *eigvec,
                                             double *energy, int *iters, void *stream) {
+  CTN_REQUIRE(plan && psi0 && krylov && work && eigvec && energy && iters, "ctn_heff2_lanczos_gnd: null argument");
   HeffUser u{plan, precision};
-  return ctn_lanczos_gnd(heff_mv, &u, psi0, plan->psi_elems, maxiter, cvgcrit, krylov, work, eigvec, energy,
-                         iters, stream);
+  return ctn::lanczos_gnd(heff_mv, &u, psi0, plan->psi_elems, maxiter, cvgcrit, krylov, work, eigvec, energy, iters,
+                          ctn::as_stream(stream), /*speculate=*/true);
 }
 
 extern "C" ctn_status ctn_heff2_lanczos_refined(ctn_heff2_plan *plan, int precision, const double *psi0, int krydim,

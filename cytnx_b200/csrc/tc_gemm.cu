@@ -786,6 +786,9 @@ __global__ void __launch_bounds__(256) k_pack(PackParams p) {
 }
 
 constexpr int PACK_THREADS = 256;
+#ifndef PACK_TILE_WAVES_X2
+#define PACK_TILE_WAVES_X2 2
+#endif
 constexpr int PACK_UNROLL = 4;
 constexpr int PACK_ITEM = PACK_THREADS * PACK_UNROLL;
 
@@ -882,39 +885,70 @@ struct PackTileParams {
 };
 
 template <int KIND, bool F32>
-__global__ void __launch_bounds__(256) k_pack_tile(PackTileParams p) {
+__device__ __forceinline__ void pack_tile_load(const PackTileParams &p, const PackTileItem &wi,
+                                               double (&v)[32 * 8 * (KIND == TC_TF32 ? 4 : 8) / 256]) {
+  constexpr int PER = 32 * 8 * (KIND == TC_TF32 ? 4 : 8) / 256;
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int idx = threadIdx.x + u * 256;
+    const int r = idx & 31, k = idx >> 5;
+    v[u] = 0.0;
+    if (r < wi.nrows && k < wi.ncols) v[u] = load_src<F32>(p.src, wi.src + r + (int64_t)k * wi.sk);
+  }
+}
+
+// Persistent: each CTA walks items it, it + grid, ...; two items' descriptors and source
+// loads are in registers at any time (the one being split and stored and the next), and the
+// item after next is loaded as soon as the staging tile has taken the current one, so the
+// reads of the whole pack are in flight from the start when it spans about one wave.
+template <int KIND, bool F32>
+__device__ __forceinline__ void pack_tile_step(const PackTileParams &p, double (*T)[33], PackTileItem &w,
+                                               double (&v)[32 * 8 * (KIND == TC_TF32 ? 4 : 8) / 256], int64_t next) {
   constexpr int E = KIND == TC_TF32 ? 4 : 8;
-  constexpr int KT = 8 * E;             // k values per item: 8 chunks
-  constexpr int PER = 32 * KT / 256;    // source elements per thread
-  __shared__ double T[KT][33];
-  for (int64_t it = blockIdx.x; it < p.nitems; it += gridDim.x) {
-    const PackTileItem wi = p.items[it];
-    const PackSeg s = p.segs[wi.seg];
-    const int k0 = wi.kc0 * E;
-    double v[PER];
+  constexpr int PER = 32 * 8 * E / 256;
+  const PackTileItem cur = w;
+  __syncthreads();  // the previous item's readers are done with T
 #pragma unroll
-    for (int u = 0; u < PER; ++u) {
-      const int idx = threadIdx.x + u * 256;
-      const int r = idx & 31, k = idx >> 5;
-      v[u] = 0.0;
-      if (wi.r0 + r < s.rows && k0 + k < s.cols)
-        v[u] = load_src<F32>(p.src, s.src_off + (int64_t)(wi.r0 + r) * s.sr + (int64_t)(k0 + k) * s.sk);
-    }
-    __syncthreads();  // the previous item's readers are done with T
+  for (int u = 0; u < PER; ++u) {
+    const int idx = threadIdx.x + u * 256;
+    T[idx >> 5][idx & 31] = v[u];
+  }
+  __syncthreads();
+  if (next < p.nitems) {
+    w = p.items[next];
+    pack_tile_load<KIND, F32>(p, w, v);
+  }
+  const int r = threadIdx.x >> 3, c = threadIdx.x & 7;
+  if (r >= cur.nrows || c * E >= cur.ncols) return;
+  const int64_t off = cur.panel_off + tc_panel_offset(cur.row0 + r, cur.k0 + c * E, cur.tile_rows, cur.kb, KIND);
+  double x[8];
 #pragma unroll
-    for (int u = 0; u < PER; ++u) {
-      const int idx = threadIdx.x + u * 256;
-      T[idx >> 5][idx & 31] = v[u];
-    }
-    __syncthreads();
-    const int r = threadIdx.x >> 3, c = threadIdx.x & 7;
-    const int kl = k0 + c * E;  // local k of this chunk
-    if (wi.r0 + r >= s.rows || kl >= s.cols) continue;
-    const int64_t off = s.panel_off + tc_panel_offset(s.row0 + wi.r0 + r, s.k0 + kl, s.tile_rows, s.kb, KIND);
-    double x[8];
-#pragma unroll
-    for (int e = 0; e < 8; ++e) x[e] = e < E ? T[c * E + e][r] : 0.0;
-    store_split<KIND>(x, p.hi, p.lo, off);
+  for (int e = 0; e < 8; ++e) x[e] = e < E ? T[c * E + e][r] : 0.0;
+  store_split<KIND>(x, p.hi, p.lo, off);
+}
+
+template <int KIND, bool F32>
+__global__ void __launch_bounds__(256, 4) k_pack_tile(PackTileParams p) {
+  constexpr int E = KIND == TC_TF32 ? 4 : 8;
+  constexpr int PER = 32 * 8 * E / 256;  // source elements per thread per item
+  __shared__ double T[8 * E][33];
+  const int64_t g = gridDim.x;
+  int64_t it = blockIdx.x;
+  if (it >= p.nitems) return;
+  PackTileItem wa = p.items[it], wb = wa;
+  double va[PER], vb[PER];
+  pack_tile_load<KIND, F32>(p, wa, va);
+  if (it + g < p.nitems) {
+    wb = p.items[it + g];
+    pack_tile_load<KIND, F32>(p, wb, vb);
+  }
+  for (;;) {
+    pack_tile_step<KIND, F32>(p, T, wa, va, it + 2 * g);
+    it += g;
+    if (it >= p.nitems) break;
+    pack_tile_step<KIND, F32>(p, T, wb, vb, it + 2 * g);
+    it += g;
+    if (it >= p.nitems) break;
   }
 }
 
@@ -1227,10 +1261,25 @@ void Packer::finalize() {
   bool all_rows = !segs.empty();
   for (const auto &sg : segs) all_rows &= (sg.sr == 1);
   if (all_rows) {
+    // row strips innermost: CTAs scheduled together read whole source k-rows (contiguous
+    // runs of rows * 8 bytes) instead of the same 256-byte strip of many k-rows
     for (size_t i = 0; i < segs.size(); ++i) {
       const int nkc = (segs[i].cols + E - 1) / E;
-      for (int r0 = 0; r0 < segs[i].rows; r0 += 32)
-        for (int kc = 0; kc < nkc; kc += 8) tile_items.push_back(PackTileItemH{(int32_t)i, r0, kc, 0});
+      const PackSeg &sg = segs[i];
+      for (int kc = 0; kc < nkc; kc += 8)
+        for (int r0 = 0; r0 < sg.rows; r0 += 32) {
+          PackTileItemH t;
+          t.src = sg.src_off + (int64_t)r0 * sg.sr + (int64_t)kc * E * sg.sk;
+          t.sk = sg.sk;
+          t.panel_off = sg.panel_off;
+          t.row0 = sg.row0 + r0;
+          t.k0 = sg.k0 + kc * E;
+          t.nrows = std::min(32, sg.rows - r0);
+          t.ncols = std::min(8 * E, sg.cols - kc * E);
+          t.tile_rows = sg.tile_rows;
+          t.kb = sg.kb;
+          tile_items.push_back(t);
+        }
     }
   }
   // the transposing tile pack (32 rows x 8 chunks per item) pays off only when the
@@ -1276,11 +1325,12 @@ ctn_status Packer::run(const void *src, int src_is_f32, uint8_t *hi, uint8_t *lo
     tp.src = src;
     tp.hi = hi;
     tp.lo = lo;
-    // four waves of resident CTAs over the grid-stride item loop: items of uneven size
-    // balance through the hardware CTA scheduler
+    // one wave of resident CTAs, each walking several items with the next item's loads in
+    // flight (PACK_TILE_WAVES_X2 / 2 waves)
     auto launch = [&](auto kern) -> void {
-      const int64_t g2 = std::min<int64_t>(tp.nitems, (int64_t)nsm_count() * resident_ctas(kern, 256) * 4);
-      kern<<<(unsigned)g2, 256, 0, st>>>(tp);
+      const int64_t g2 =
+          std::min<int64_t>(tp.nitems, (int64_t)nsm_count() * resident_ctas(kern, 256) * PACK_TILE_WAVES_X2 / 2);
+      kern<<<(unsigned)std::max<int64_t>(g2, 1), 256, 0, st>>>(tp);
     };
     if (kind == TC_TF32) {
       if (src_is_f32) launch(k_pack_tile<TC_TF32, true>);

@@ -122,8 +122,15 @@ struct PackItem {
   int64_t chunk0;      // first chunk of this CTA work item (global chunk index)
 };
 
+// one 32-row x 8-chunk tile of a row-contiguous segment, self-contained so that a CTA needs
+// a single descriptor load before it issues the tile's source loads
 struct PackTileItemH {
-  int32_t seg, r0, kc0, pad_;
+  int64_t src;         // element offset of the tile's (row 0, k 0); rows are stride 1
+  int64_t sk;          // source stride of k
+  int64_t panel_off;   // byte offset of the group's tile (0,0)
+  int32_t row0, k0;    // destination row / k of the tile's (0,0) inside the group panel
+  int32_t nrows, ncols;  // valid rows (<= 32) and k values (<= 8 chunks) of the tile
+  int32_t tile_rows, kb;
 };
 
 struct Packer {

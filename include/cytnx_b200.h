@@ -293,7 +293,8 @@ void ctn_heff2_batch_destroy(ctn_heff2_batch *batch);
  * (maxiter + 1) * n doubles (device); work >= 4 * n + 64 doubles (device).
  * On return *energy holds the lowest Ritz value, eigvec (device, n) the Ritz
  * vector, *iters the iterations done.  Semantics follow the reference: stop
- * when |E_i - E_{i-1}| < cvgcrit or beta == 0 or maxiter reached. */
+ * when |E_i - E_{i-1}| < cvgcrit or beta == 0 or maxiter reached; matvec is called exactly
+ * *iters times. */
 typedef int (*ctn_matvec_fn)(void *user, const double *x, double *y, void *stream);
 ctn_status ctn_lanczos_gnd(ctn_matvec_fn matvec, void *user, const double *psi0, int64_t n,
                            int maxiter, double cvgcrit, double *krylov, double *work,
@@ -344,7 +345,10 @@ ctn_status ctn_heff2_lanczos_refined(ctn_heff2_plan *plan, int precision, const 
                                      int max_restarts, double tol, double *krylov, double *work,
                                      double *eigvec, double *energy, double *residual, int *restarts,
                                      int64_t *matvecs, void *stream);
-/* the same driver on a planned H_eff (no callback) */
+/* the same driver on a planned H_eff (no callback).  Each next iteration is queued on the
+ * device before the host solves the current tridiagonal, so the host solve overlaps the next
+ * matvec; after the last iteration one queued matvec is discarded (results are those of
+ * ctn_lanczos_gnd with the same matvec, bit for bit). */
 ctn_status ctn_heff2_lanczos_gnd(ctn_heff2_plan *plan, int precision, const double *psi0,
                                  int maxiter, double cvgcrit, double *krylov, double *work,
                                  double *eigvec, double *energy, int *iters, void *stream);

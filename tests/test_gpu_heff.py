@@ -122,6 +122,49 @@ def test_lanczos_heff_matches_oracle():
     assert abs(E2.item() - E) < 1e-12 * abs(E)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "bf16x3"])
+def test_lanczos_speculative_matches_callback(precision):
+    """ctn_heff2_lanczos_gnd queues each next iteration before the host's tridiagonal solve;
+    ctn_lanczos_gnd with a callback around ctn_heff2_matvec runs the same recurrence one
+    iteration at a time.  Same energy, iteration count and Ritz vector bit for bit, on a run
+    stopped by |dE| < cvgcrit and on one stopped by maxiter; the callback route calls the
+    matvec exactly iters times."""
+    import ctypes
+
+    import cytnx_b200 as c
+    from cytnx_b200 import _lib
+
+    psi, L, M1, M2, R = build(32, seed=4)
+    H = c.TwoSiteHeff(L, M1, M2, R, psi)
+    H.bind(precision)
+    prec = _lib.PRECISIONS[precision]
+    x0 = psi.contiguous().flat_view()
+    n = H.n
+    calls = [0]
+
+    def cb(user, x, y, stream):
+        calls[0] += 1
+        return _lib.lib().ctn_heff2_matvec(H._h, x, y, prec, stream)
+
+    f = _lib.MATVEC_FN(cb)
+    for cvg, maxiter in [(1e-9, 80), (1e-300, 12)]:
+        E, vec, it = H.lanczos(psi, maxiter=maxiter, cvgcrit=cvg, precision=precision)
+        v = vec.flat_view().clone()
+        K = torch.empty((maxiter + 1) * n, dtype=torch.float64, device="cuda")
+        work = torch.empty(n + 8 + 1032 + maxiter + 64, dtype=torch.float64, device="cuda")
+        eig = torch.empty(n, dtype=torch.float64, device="cuda")
+        e2, it2 = ctypes.c_double(), ctypes.c_int()
+        calls[0] = 0
+        _lib.check(_lib.lib().ctn_lanczos_gnd(f, None, x0.data_ptr(), n, maxiter, cvg, K.data_ptr(),
+                                              work.data_ptr(), eig.data_ptr(), ctypes.byref(e2), ctypes.byref(it2),
+                                              _lib.stream_ptr()), "ctn_lanczos_gnd")
+        torch.cuda.synchronize()
+        assert it2.value == it and calls[0] == it
+        assert (it < maxiter) if cvg > 1e-100 else (it == maxiter)
+        assert e2.value == E
+        assert torch.equal(eig, v)
+
+
 def test_lanczos_block_golden():
     """tests/linalg_test/Lanczos_Gnd_test.cpp:392-422: E vs Eigh to 1e-12, residual < 1e-6."""
     import cytnx_b200 as c
