@@ -22,7 +22,7 @@
 namespace ctn {
 
 namespace {
-constexpr int BM = 64, BN = 64, BK = 16;
+constexpr int BM = 64, BK = 16;  // tile rows and k depth; the tile width BN is 64 or 32
 constexpr int PAD = 4;
 constexpr int NTHREADS = 128;
 
@@ -52,14 +52,14 @@ __device__ __forceinline__ void dmma_16x8x16(double (&c)[4], const double (&a)[8
 // Shared-memory tiles keep the operand's contiguous global axis contiguous, so the
 // cp.async writes are conflict-free; the +4 double padding makes every fragment read
 // pattern below conflict-free as well (bank = 8*x + 2*y for the 4x4 lanes of a phase).
-template <bool TA, bool TB>
+template <bool TA, bool TB, int BN>
 struct SmemT {
   double A[2][TA ? BK : BM][(TA ? BM : BK) + PAD];
   double B[2][TB ? BN : BK][(TB ? BK : BN) + PAD];
 };
 
-template <bool TA, bool TB>
-__device__ __forceinline__ void load_stage(SmemT<TA, TB> &sm, int buf, const double *__restrict__ A,
+template <bool TA, bool TB, int BN>
+__device__ __forceinline__ void load_stage(SmemT<TA, TB, BN> &sm, int buf, const double *__restrict__ A,
                                            const double *__restrict__ B, const GemmPairD &p, int m, int n,
                                            int m0, int n0, int k0) {
   const int tid = threadIdx.x;
@@ -97,24 +97,27 @@ __device__ __forceinline__ void load_stage(SmemT<TA, TB> &sm, int buf, const dou
   }
 }
 
-template <bool TA, bool TB>
+// BN = 64: each of the 4 warps computes a 32 x 32 piece (2 x 4 m16n8 products per k step);
+// BN = 32: a 32 x 16 piece (2 x 2), for plans with too few 64 x 64 tiles to fill the SMs.
+template <bool TA, bool TB, int BN>
 __global__ void __launch_bounds__(NTHREADS) k_gemm_grouped_f64(
     const double *__restrict__ A, const double *__restrict__ B, double *__restrict__ C,
     const GemmTaskD *__restrict__ tasks, const GemmPairD *__restrict__ pairs,
     const GemmTileD *__restrict__ tiles, int64_t ntiles) {
-  __shared__ __align__(16) SmemT<TA, TB> sm;
+  constexpr int NJ = BN / 16;  // n8 products per warp
+  __shared__ __align__(16) SmemT<TA, TB, BN> sm;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * (BN / 2);
   const int g = lane >> 2, t4 = lane & 3;
   for (int64_t ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
     const GemmTileD tile = tiles[ti];
     const GemmTaskD task = tasks[tile.task];
     const int m0 = tile.m0, n0 = tile.n0;
-    double acc[2][4][4];
+    double acc[2][NJ][4];
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
+      for (int j = 0; j < NJ; ++j)
 #pragma unroll
         for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
 
@@ -127,7 +130,7 @@ __global__ void __launch_bounds__(NTHREADS) k_gemm_grouped_f64(
     GemmPairD cur;
     if (have) {
       cur = pairs[task.pair_begin + pi];
-      load_stage<TA, TB>(sm, 0, A, B, cur, task.m, task.n, m0, n0, 0);
+      load_stage<TA, TB, BN>(sm, 0, A, B, cur, task.m, task.n, m0, n0, 0);
     }
     cp_async_commit();
     while (have) {
@@ -140,11 +143,11 @@ __global__ void __launch_bounds__(NTHREADS) k_gemm_grouped_f64(
         if (npi < npairs) nxt = pairs[task.pair_begin + npi];
       }
       const bool have_next = npi < npairs;
-      if (have_next) load_stage<TA, TB>(sm, buf ^ 1, A, B, nxt, task.m, task.n, m0, n0, nkt * BK);
+      if (have_next) load_stage<TA, TB, BN>(sm, buf ^ 1, A, B, nxt, task.m, task.n, m0, n0, nkt * BK);
       cp_async_commit();
       cp_async_wait<1>();
       __syncthreads();
-      double a[2][8], b[4][4];
+      double a[2][8], b[NJ][4];
 #pragma unroll
       for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -153,7 +156,7 @@ __global__ void __launch_bounds__(NTHREADS) k_gemm_grouped_f64(
           a[i][e] = TA ? sm.A[buf][k][r] : sm.A[buf][r][k];
         }
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
+      for (int j = 0; j < NJ; ++j)
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
           const int k = t4 + 4 * e, cidx = wn + j * 8 + g;
@@ -162,7 +165,7 @@ __global__ void __launch_bounds__(NTHREADS) k_gemm_grouped_f64(
 #pragma unroll
       for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) dmma_16x8x16(acc[i][j], a[i], b[j]);
+        for (int j = 0; j < NJ; ++j) dmma_16x8x16(acc[i][j], a[i], b[j]);
       __syncthreads();
       buf ^= 1;
       pi = npi;
@@ -175,7 +178,7 @@ __global__ void __launch_bounds__(NTHREADS) k_gemm_grouped_f64(
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < NJ; ++j) {
         const int r0 = m0 + wm + i * 16 + g;
         const int c0 = n0 + wn + j * 8 + 2 * t4;
 #pragma unroll
@@ -193,7 +196,7 @@ __global__ void __launch_bounds__(NTHREADS) k_gemm_grouped_f64(
 }  // namespace
 
 void build_tiles_f64(const std::vector<GemmTaskD> &tasks, const std::vector<GemmPairD> &pairs,
-                     std::vector<GemmTileD> &tiles) {
+                     std::vector<GemmTileD> &tiles, int bn) {
   tiles.clear();
   std::vector<std::pair<double, GemmTileD>> tmp;
   for (size_t t = 0; t < tasks.size(); ++t) {
@@ -201,7 +204,7 @@ void build_tiles_f64(const std::vector<GemmTaskD> &tasks, const std::vector<Gemm
     double kt = 0;
     for (int p = 0; p < tk.pair_count; ++p) kt += std::max(0, pairs[tk.pair_begin + p].k);
     for (int m0 = 0; m0 < tk.m; m0 += BM)
-      for (int n0 = 0; n0 < tk.n; n0 += BN) {
+      for (int n0 = 0; n0 < tk.n; n0 += bn) {
         GemmTileD g;
         g.task = (int32_t)t;
         g.m0 = m0;
@@ -217,18 +220,28 @@ void build_tiles_f64(const std::vector<GemmTaskD> &tasks, const std::vector<Gemm
 
 ctn_status launch_gemm_f64(const double *A, const double *B, double *C, const GemmTaskD *d_tasks,
                            const GemmPairD *d_pairs, const GemmTileD *d_tiles, int64_t ntiles, int flags,
-                           cudaStream_t st) {
+                           int bn, cudaStream_t st) {
   if (ntiles == 0) return CTN_OK;
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   // 128 threads, ~17 KB smem: up to 8+ CTAs per SM resident
   const int64_t grid = std::min<int64_t>(ntiles, (int64_t)nsm * 12);
-  switch (flags & 3) {
-    case 0: k_gemm_grouped_f64<false, false><<<(unsigned)grid, NTHREADS, 0, st>>>(A, B, C, d_tasks, d_pairs, d_tiles, ntiles); break;
-    case 1: k_gemm_grouped_f64<true, false><<<(unsigned)grid, NTHREADS, 0, st>>>(A, B, C, d_tasks, d_pairs, d_tiles, ntiles); break;
-    case 2: k_gemm_grouped_f64<false, true><<<(unsigned)grid, NTHREADS, 0, st>>>(A, B, C, d_tasks, d_pairs, d_tiles, ntiles); break;
-    default: k_gemm_grouped_f64<true, true><<<(unsigned)grid, NTHREADS, 0, st>>>(A, B, C, d_tasks, d_pairs, d_tiles, ntiles); break;
+  auto go = [&](auto kern) { kern<<<(unsigned)grid, NTHREADS, 0, st>>>(A, B, C, d_tasks, d_pairs, d_tiles, ntiles); };
+  if (bn == 32) {
+    switch (flags & 3) {
+      case 0: go(k_gemm_grouped_f64<false, false, 32>); break;
+      case 1: go(k_gemm_grouped_f64<true, false, 32>); break;
+      case 2: go(k_gemm_grouped_f64<false, true, 32>); break;
+      default: go(k_gemm_grouped_f64<true, true, 32>); break;
+    }
+  } else {
+    switch (flags & 3) {
+      case 0: go(k_gemm_grouped_f64<false, false, 64>); break;
+      case 1: go(k_gemm_grouped_f64<true, false, 64>); break;
+      case 2: go(k_gemm_grouped_f64<false, true, 64>); break;
+      default: go(k_gemm_grouped_f64<true, true, 64>); break;
+    }
   }
   CTN_CHECK_LAUNCH();
   return CTN_OK;

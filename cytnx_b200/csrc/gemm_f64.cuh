@@ -23,10 +23,10 @@ struct GemmTileD {
 };
 
 void build_tiles_f64(const std::vector<GemmTaskD> &tasks, const std::vector<GemmPairD> &pairs,
-                     std::vector<GemmTileD> &tiles);
+                     std::vector<GemmTileD> &tiles, int bn);
 ctn_status launch_gemm_f64(const double *A, const double *B, double *C, const GemmTaskD *d_tasks,
                            const GemmPairD *d_pairs, const GemmTileD *d_tiles, int64_t ntiles, int flags,
-                           cudaStream_t st);
+                           int bn, cudaStream_t st);
 
 // Host tables + their device copy (uploaded once, on the first launch on a device).
 struct GroupedGemmF64 {
@@ -37,10 +37,18 @@ struct GroupedGemmF64 {
   int d_dev = -1;
   double flops = 0.0;
   int flags = 0;          // operand orientation shared by every pair of the plan
+  int bn = 64;            // tile width: 64, or 32 when 64-wide tiles would not fill the SMs
   bool mixed = false;     // pairs disagree on the orientation (rejected at run time)
 
   void finalize() {
-    build_tiles_f64(tasks, pairs, tiles);
+    // fewer than two 64 x 64 tiles per SM (148 SMs): 64 x 32 tiles, twice as many CTAs and
+    // less padding on narrow groups
+    bn = 64;
+    build_tiles_f64(tasks, pairs, tiles, bn);
+    if (tiles.size() < 2 * 148) {
+      bn = 32;
+      build_tiles_f64(tasks, pairs, tiles, bn);
+    }
     flags = pairs.empty() ? 0 : (pairs[0].flags & 3);
     mixed = false;
     for (const auto &p : pairs) mixed |= ((p.flags & 3) != flags);
@@ -83,7 +91,7 @@ struct GroupedGemmF64 {
     const GemmTaskD *dt = (const GemmTaskD *)p;
     const GemmPairD *dp = (const GemmPairD *)(p + tasks.size() * sizeof(GemmTaskD));
     const GemmTileD *dl = (const GemmTileD *)(p + tasks.size() * sizeof(GemmTaskD) + pairs.size() * sizeof(GemmPairD));
-    return launch_gemm_f64(A, B, C, dt, dp, dl, (int64_t)tiles.size(), flags, st);
+    return launch_gemm_f64(A, B, C, dt, dp, dl, (int64_t)tiles.size(), flags, bn, st);
   }
   ~GroupedGemmF64() {
     if (d_mem) cudaFree(d_mem);

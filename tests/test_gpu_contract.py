@@ -128,3 +128,66 @@ def test_contract_errors():
     _, B = _random_block(c, [(1, *q), (1, *q)], ["b", "c"], rng)  # b is BRA on both sides
     with pytest.raises(c.CytnxError):
         c.Contract(A, B)
+
+
+TASK_DT = np.dtype([("c_off", "<i8"), ("m", "<i4"), ("n", "<i4"), ("ldc", "<i4"), ("pair_begin", "<i4"),
+                    ("pair_count", "<i4"), ("pad_", "<i4")])
+PAIR_DT = np.dtype([("a_off", "<i8"), ("b_off", "<i8"), ("k", "<i4"), ("lda", "<i4"), ("ldb", "<i4"),
+                    ("flags", "<i4")])
+
+
+@pytest.mark.parametrize("flags", [0, 1, 2, 3])
+@pytest.mark.parametrize("shapes", ["wide", "narrow"])
+def test_grouped_gemm_tile_widths(flags, shapes):
+    """ctn_gemm_grouped_f64 (the Gemm_Batch replacement) against FP64 torch matmuls.  'wide':
+    five 512 x 512 tasks (320 tiles of 64 x 64, the 64-wide kernel); 'narrow': ragged small
+    tasks (fewer than two tiles per SM, the 64 x 32 kernel).  Two pairs per task with k not a
+    multiple of 16, every operand orientation, one task without pairs (zeros)."""
+    import ctypes
+
+    from cytnx_b200 import _lib
+
+    g = torch.Generator().manual_seed(11 + flags)
+    if shapes == "wide":
+        mn = [(512, 512)] * 5
+    else:
+        mn = [(70, 70), (130, 6), (5, 200), (64, 33), (1, 1)]
+    ks = [40, 23]
+    a_parts, b_parts, tasks, pairs, refs = [], [], [], [], []
+    a_off = b_off = c_off = 0
+    for t, (m, n) in enumerate(mn):
+        ref = torch.zeros(m, n, dtype=torch.float64)
+        pb = len(pairs)
+        npair = 0 if t == 2 else len(ks)
+        for k in ks[:npair]:
+            A = torch.randn(m, k, generator=g, dtype=torch.float64)
+            B = torch.randn(k, n, generator=g, dtype=torch.float64)
+            ref += A @ B
+            As = A.t().contiguous() if flags & 1 else A
+            Bs = B.t().contiguous() if flags & 2 else B
+            pairs.append((a_off, b_off, k, m if flags & 1 else k, k if flags & 2 else n, flags))
+            a_parts.append(As.reshape(-1))
+            b_parts.append(Bs.reshape(-1))
+            a_off += As.numel()
+            b_off += Bs.numel()
+        tasks.append((c_off, m, n, n, pb, npair, 0))
+        refs.append((c_off, ref))
+        c_off += m * n
+    ta = np.array(tasks, dtype=TASK_DT)
+    pa = np.array(pairs, dtype=PAIR_DT)
+    A = torch.cat(a_parts).cuda()
+    B = torch.cat(b_parts).cuda()
+    C = torch.full((c_off,), float("nan"), dtype=torch.float64, device="cuda")
+    plan = ctypes.c_void_p()
+    _lib.check(_lib.lib().ctn_gemm_grouped_plan_create(len(ta), ta.ctypes.data, len(pa), pa.ctypes.data,
+                                                       ctypes.byref(plan)), "plan")
+    try:
+        _lib.check(_lib.lib().ctn_gemm_grouped_f64(plan, A.data_ptr(), B.data_ptr(), C.data_ptr(), _lib.stream_ptr()),
+                   "gemm")
+        torch.cuda.synchronize()
+    finally:
+        _lib.lib().ctn_gemm_grouped_plan_destroy(plan)
+    Ch = C.cpu()
+    for off, ref in refs:
+        got = Ch[off:off + ref.numel()].view(ref.shape)
+        assert torch.allclose(got, ref, rtol=1e-12, atol=1e-12), (shapes, flags, float((got - ref).abs().max()))
