@@ -137,10 +137,20 @@ __global__ void __launch_bounds__(RT) k_div_copy(const double *__restrict__ x, d
 
 __device__ __forceinline__ double safe_inv(double s) { return s != 0.0 ? 1.0 / s : 0.0; }
 
+// two consecutive elements (pair index i) of w as doubles: one 16-byte load for FP64, one
+// 8-byte load for FP32
+__device__ __forceinline__ double2 ld_pair(const double *w, int64_t i) {
+  return reinterpret_cast<const double2 *>(w)[i];
+}
+__device__ __forceinline__ double2 ld_pair(const float *w, int64_t i) {
+  const float2 v = reinterpret_cast<const float2 *>(w)[i];
+  return make_double2((double)v.x, (double)v.y);
+}
+
 // <w, a> / s^2 and <w, b> / s in one pass (s = *s_ptr, 1 when s_ptr is null; a zero s
 // gives zeros: the vector behind it is empty after a breakdown)
-template <bool VEC>
-__global__ void __launch_bounds__(RT) k_dot2s(const double *__restrict__ w, const double *__restrict__ a,
+template <bool VEC, typename WT>
+__global__ void __launch_bounds__(RT) k_dot2s(const WT *__restrict__ w, const double *__restrict__ a,
                                              const double *__restrict__ b, int64_t n, const double *s_ptr,
                                              double *partials, unsigned *ticket, double *out_a, double *out_b) {
   double sa = 0.0, sb = 0.0;
@@ -148,14 +158,13 @@ __global__ void __launch_bounds__(RT) k_dot2s(const double *__restrict__ w, cons
   const int64_t step = (int64_t)gridDim.x * RT;
   if (VEC) {
     const int64_t n2 = n / 2;
-    const double2 *w2 = reinterpret_cast<const double2 *>(w), *a2 = reinterpret_cast<const double2 *>(a),
-                  *b2 = reinterpret_cast<const double2 *>(b);
+    const double2 *a2 = reinterpret_cast<const double2 *>(a), *b2 = reinterpret_cast<const double2 *>(b);
     for (int64_t i = tid; i < n2; i += 2 * step) {
       const bool two = i + step < n2;
-      const double2 x0 = w2[i], y0 = a2[i], z0 = b2[i];
+      const double2 x0 = ld_pair(w, i), y0 = a2[i], z0 = b2[i];
       double2 x1 = make_double2(0.0, 0.0), y1 = x1, z1 = x1;
       if (two) {
-        x1 = w2[i + step];
+        x1 = ld_pair(w, i + step);
         y1 = a2[i + step];
         z1 = b2[i + step];
       }
@@ -169,12 +178,12 @@ __global__ void __launch_bounds__(RT) k_dot2s(const double *__restrict__ w, cons
       sb = fma(x1.y, z1.y, sb);
     }
     if (tid == 0 && (n & 1)) {
-      sa = fma(w[n - 1], a[n - 1], sa);
-      sb = fma(w[n - 1], b[n - 1], sb);
+      sa = fma((double)w[n - 1], a[n - 1], sa);
+      sb = fma((double)w[n - 1], b[n - 1], sb);
     }
   } else {
     for (int64_t i = tid; i < n; i += step) {
-      const double x = w[i];
+      const double x = (double)w[i];
       sa = fma(x, a[i], sa);
       sb = fma(x, b[i], sb);
     }
@@ -209,8 +218,8 @@ __global__ void __launch_bounds__(RT) k_dot2s(const double *__restrict__ w, cons
 // dst = (w - alpha u) / s - (s / sp) up - gamma q,  ||dst|| -> *nrm.  alpha and gamma are
 // the coefficients of q_j = u / s (from k_dot2s with the same s); up = u_{j-1} with its
 // own scale sp, so (s / sp) up = beta_{j-1} q_{j-1}.  up and q may be null.
-template <bool VEC>
-__global__ void __launch_bounds__(RT) k_lanczos_step(const double *__restrict__ w, const double *__restrict__ u,
+template <bool VEC, typename WT>
+__global__ void __launch_bounds__(RT) k_lanczos_step(const WT *__restrict__ w, const double *__restrict__ u,
                                                     const double *__restrict__ up, const double *__restrict__ q,
                                                     double *__restrict__ dst, int64_t n, const double *alpha,
                                                     const double *gamma, const double *s_ptr, const double *sp_ptr,
@@ -232,16 +241,16 @@ __global__ void __launch_bounds__(RT) k_lanczos_step(const double *__restrict__ 
   };
   if (VEC) {
     const int64_t n2 = n / 2;
-    const double2 *w2 = reinterpret_cast<const double2 *>(w), *u2 = reinterpret_cast<const double2 *>(u),
-                  *p2 = reinterpret_cast<const double2 *>(up), *q2 = reinterpret_cast<const double2 *>(q);
+    const double2 *u2 = reinterpret_cast<const double2 *>(u), *p2 = reinterpret_cast<const double2 *>(up),
+                  *q2 = reinterpret_cast<const double2 *>(q);
     double2 *d2 = reinterpret_cast<double2 *>(dst);
     const double2 z = make_double2(0.0, 0.0);
     for (int64_t i = tid; i < n2; i += 2 * step) {
       const bool two = i + step < n2;
-      const double2 w0 = w2[i], u0 = u2[i], p0 = up ? p2[i] : z, q0 = q ? q2[i] : z;
+      const double2 w0 = ld_pair(w, i), u0 = u2[i], p0 = up ? p2[i] : z, q0 = q ? q2[i] : z;
       double2 w1 = z, u1 = z, p1 = z, q1 = z;
       if (two) {
-        w1 = w2[i + step];
+        w1 = ld_pair(w, i + step);
         u1 = u2[i + step];
         if (up) p1 = p2[i + step];
         if (q) q1 = q2[i + step];
@@ -251,10 +260,10 @@ __global__ void __launch_bounds__(RT) k_lanczos_step(const double *__restrict__ 
     }
     if (tid == 0 && (n & 1)) {
       const int64_t k = n - 1;
-      dst[k] = one(w[k], u[k], up ? up[k] : 0.0, q ? q[k] : 0.0);
+      dst[k] = one((double)w[k], u[k], up ? up[k] : 0.0, q ? q[k] : 0.0);
     }
   } else {
-    for (int64_t i = tid; i < n; i += step) dst[i] = one(w[i], u[i], up ? up[i] : 0.0, q ? q[i] : 0.0);
+    for (int64_t i = tid; i < n; i += step) dst[i] = one((double)w[i], u[i], up ? up[i] : 0.0, q ? q[i] : 0.0);
   }
   acc = block_sum(acc);
   finish(acc, partials, ticket, nrm, 1);
@@ -416,30 +425,50 @@ ctn_status lanczos_update_f64(double *w, const double *p1, const double *p0, int
 }
 static bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
-ctn_status dot2s_f64(const double *w, const double *a, const double *b, int64_t n, const double *s, double *out_a,
-                     double *out_b, double *ws2, cudaStream_t st) {
+template <typename WT>
+static ctn_status dot2s_any(const WT *w, const double *a, const double *b, int64_t n, const double *s, double *out_a,
+                            double *out_b, double *ws2, cudaStream_t st) {
   const int g = grid_stream(n);
   unsigned *ticket = reinterpret_cast<unsigned *>(ws2 + 2 * MAXCTA);
   if (aligned16(w) && aligned16(a) && aligned16(b))
-    k_dot2s<true><<<g, RT, 0, st>>>(w, a, b, n, s, ws2, ticket, out_a, out_b);
+    k_dot2s<true, WT><<<g, RT, 0, st>>>(w, a, b, n, s, ws2, ticket, out_a, out_b);
   else
-    k_dot2s<false><<<g, RT, 0, st>>>(w, a, b, n, s, ws2, ticket, out_a, out_b);
+    k_dot2s<false, WT><<<g, RT, 0, st>>>(w, a, b, n, s, ws2, ticket, out_a, out_b);
   CTN_CHECK_LAUNCH();
   return CTN_OK;
 }
+ctn_status dot2s_f64(const double *w, const double *a, const double *b, int64_t n, const double *s, double *out_a,
+                     double *out_b, double *ws2, cudaStream_t st) {
+  return dot2s_any(w, a, b, n, s, out_a, out_b, ws2, st);
+}
+ctn_status dot2s_f64(const float *w, const double *a, const double *b, int64_t n, const double *s, double *out_a,
+                     double *out_b, double *ws2, cudaStream_t st) {
+  return dot2s_any(w, a, b, n, s, out_a, out_b, ws2, st);
+}
 
-ctn_status lanczos_step_f64(const double *w, const double *u, const double *up, const double *q, double *dst,
-                            int64_t n, const double *alpha, const double *gamma, const double *s, const double *sp,
-                            double *nrm, double *ws, cudaStream_t st) {
+template <typename WT>
+static ctn_status lanczos_step_any(const WT *w, const double *u, const double *up, const double *q, double *dst,
+                                   int64_t n, const double *alpha, const double *gamma, const double *s,
+                                   const double *sp, double *nrm, double *ws, cudaStream_t st) {
   const int g = grid_stream(n);
   unsigned *ticket = reinterpret_cast<unsigned *>(ws + MAXCTA);
   const bool vec = aligned16(w) && aligned16(u) && aligned16(dst) && (!up || aligned16(up)) && (!q || aligned16(q));
   if (vec)
-    k_lanczos_step<true><<<g, RT, 0, st>>>(w, u, up, q, dst, n, alpha, gamma, s, sp, ws, ticket, nrm);
+    k_lanczos_step<true, WT><<<g, RT, 0, st>>>(w, u, up, q, dst, n, alpha, gamma, s, sp, ws, ticket, nrm);
   else
-    k_lanczos_step<false><<<g, RT, 0, st>>>(w, u, up, q, dst, n, alpha, gamma, s, sp, ws, ticket, nrm);
+    k_lanczos_step<false, WT><<<g, RT, 0, st>>>(w, u, up, q, dst, n, alpha, gamma, s, sp, ws, ticket, nrm);
   CTN_CHECK_LAUNCH();
   return CTN_OK;
+}
+ctn_status lanczos_step_f64(const double *w, const double *u, const double *up, const double *q, double *dst,
+                            int64_t n, const double *alpha, const double *gamma, const double *s, const double *sp,
+                            double *nrm, double *ws, cudaStream_t st) {
+  return lanczos_step_any(w, u, up, q, dst, n, alpha, gamma, s, sp, nrm, ws, st);
+}
+ctn_status lanczos_step_f64(const float *w, const double *u, const double *up, const double *q, double *dst,
+                            int64_t n, const double *alpha, const double *gamma, const double *s, const double *sp,
+                            double *nrm, double *ws, cudaStream_t st) {
+  return lanczos_step_any(w, u, up, q, dst, n, alpha, gamma, s, sp, nrm, ws, st);
 }
 
 ctn_status div_copy_f64(const double *x, double *y, int64_t n, const double *a, cudaStream_t st) {

@@ -17,8 +17,14 @@ ctn_status lanczos_update_f64(double *w, const double *p1, const double *p0, int
 //   out_a = <w, a> / s^2, out_b = <w, b> / s  (s null: no scaling)
 ctn_status dot2s_f64(const double *w, const double *a, const double *b, int64_t n, const double *s, double *out_a,
                      double *out_b, double *ws2, cudaStream_t st);
+// the same with an FP32 w (the split-precision matvec output)
+ctn_status dot2s_f64(const float *w, const double *a, const double *b, int64_t n, const double *s, double *out_a,
+                     double *out_b, double *ws2, cudaStream_t st);
 //   dst = (w - alpha u) / s - (s / sp) up - gamma q and ||dst|| -> nrm  (up, q may be null)
 ctn_status lanczos_step_f64(const double *w, const double *u, const double *up, const double *q, double *dst,
+                            int64_t n, const double *alpha, const double *gamma, const double *s, const double *sp,
+                            double *nrm, double *ws, cudaStream_t st);
+ctn_status lanczos_step_f64(const float *w, const double *u, const double *up, const double *q, double *dst,
                             int64_t n, const double *alpha, const double *gamma, const double *s, const double *sp,
                             double *nrm, double *ws, cudaStream_t st);
 ctn_status div_copy_f64(const double *x, double *y, int64_t n, const double *a, cudaStream_t st);

@@ -279,7 +279,7 @@ ctn_status lanczos_refined(int (*mv_lo)(void *, const double *, double *, void *
                            int (*mv_hi)(void *, const double *, double *, void *), void *u_hi, const double *psi0,
                            int64_t n, int krydim, int max_restarts, double tol, double *krylov, double *work,
                            double *eigvec, double *energy, double *residual, int *restarts, int64_t *counts,
-                           cudaStream_t st) {
+                           cudaStream_t st, bool w_f32) {
   CTN_REQUIRE(krydim >= 2 && max_restarts >= 1 && n > 0 && tol >= 0, "[Lanczos refined] bad argument");
   // work: [w n][scalars 8][reduction ws][two-sum ws][Ritz coefficients m][alpha m][beta m]
   double *w = work;
@@ -329,10 +329,16 @@ ctn_status lanczos_refined(int (*mv_lo)(void *, const double *, double *, void *
       const double *up = j >= 2 ? krylov + (int64_t)(j - 1) * n : nullptr;
       if (mv_lo(u_lo, uj, w, st) != 0) return CTN_ERR_CUDA;
       ++n_lo;
-      CTN_TRY(dot2s_f64(w, uj, q0, n, beta + j - 1, alpha + j, scal + 4, ws2, st));
-      if (j + 1 < krydim)
-        CTN_TRY(lanczos_step_f64(w, uj, up, q0, krylov + (int64_t)(j + 1) * n, n, alpha + j, scal + 4, beta + j - 1,
-                                 j >= 2 ? beta + j - 2 : nullptr, beta + j, ws, st));
+      auto step = [&](const auto *wv) -> ctn_status {
+        CTN_TRY(dot2s_f64(wv, uj, q0, n, beta + j - 1, alpha + j, scal + 4, ws2, st));
+        if (j + 1 < krydim)
+          CTN_TRY(lanczos_step_f64(wv, uj, up, q0, krylov + (int64_t)(j + 1) * n, n, alpha + j, scal + 4,
+                                   beta + j - 1, j >= 2 ? beta + j - 2 : nullptr, beta + j, ws, st));
+        return CTN_OK;
+      };
+      // w_f32: the low-precision matvec wrote w as n floats (its own error is far above FP32 rounding)
+      if (w_f32) CTN_TRY(step(reinterpret_cast<const float *>(w)));
+      else CTN_TRY(step(static_cast<const double *>(w)));
     }
     CTN_CUDA(cudaMemcpyAsync(As.data(), alpha, sizeof(double) * krydim, cudaMemcpyDeviceToHost, st));
     CTN_CUDA(cudaMemcpyAsync(Bs.data(), beta, sizeof(double) * krydim, cudaMemcpyDeviceToHost, st));
@@ -377,7 +383,8 @@ extern "C" ctn_status ctn_lanczos_refined(ctn_matvec_fn matvec_lo, void *user_lo
   CTN_REQUIRE(matvec_lo && matvec_hi && psi0 && krylov && work && eigvec && energy,
               "ctn_lanczos_refined: null argument");
   return ctn::lanczos_refined(matvec_lo, user_lo, matvec_hi, user_hi, psi0, n, krydim, max_restarts, tol, krylov,
-                              work, eigvec, energy, residual, restarts, matvecs, ctn::as_stream(stream));
+                              work, eigvec, energy, residual, restarts, matvecs, ctn::as_stream(stream),
+                              /*w_f32=*/false);
 }
 
 extern "C" ctn_status ctn_lanczos_gnd(ctn_matvec_fn matvec, void *user, const double *psi0, int64_t n, int maxiter,

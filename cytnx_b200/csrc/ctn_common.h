@@ -25,6 +25,12 @@ inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s
 ctn_status lanczos_gnd(int (*mv)(void *, const double *, double *, void *), void *user, const double *psi0,
                        int64_t n, int maxiter, double cvgcrit, double *krylov, double *work, double *eigvec,
                        double *energy, int *iters, cudaStream_t st, bool speculate);
+// restarted split-precision ground state (capi.cpp); w_f32: mv_lo writes its result as n floats
+ctn_status lanczos_refined(int (*mv_lo)(void *, const double *, double *, void *), void *u_lo,
+                           int (*mv_hi)(void *, const double *, double *, void *), void *u_hi, const double *psi0,
+                           int64_t n, int krydim, int max_restarts, double tol, double *krylov, double *work,
+                           double *eigvec, double *energy, double *residual, int *restarts, int64_t *counts,
+                           cudaStream_t st, bool w_f32);
 
 }  // namespace ctn
 

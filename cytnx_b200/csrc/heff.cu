@@ -452,6 +452,14 @@ int heff_mv(void *u, const double *x, double *y, void *stream) {
   HeffUser *h = (HeffUser *)u;
   return ctn_heff2_matvec(h->plan, x, y, h->precision, stream) == CTN_OK ? 0 : 1;
 }
+// split-precision matvec with its result rounded to FP32 into y (n floats)
+int heff_mv_f32(void *u, const double *x, double *y, void *stream) {
+  HeffUser *h = (HeffUser *)u;
+  return ctn::heff_split_matvec_f32out(h->plan, split_kind(h->precision), x, reinterpret_cast<float *>(y),
+                                       ctn::as_stream(stream)) == CTN_OK
+             ? 0
+             : 1;
+}
 }  // namespace
 
 extern "C" ctn_status ctn_heff2_lanczos_gnd(ctn_heff2_plan *plan, int precision, const double *psi0, int maxiter,
@@ -470,8 +478,16 @@ extern "C" ctn_status ctn_heff2_lanczos_refined(ctn_heff2_plan *plan, int precis
   CTN_REQUIRE(plan && plan->bound, "ctn_heff2_lanczos_refined: the FP64 environments must be bound (ctn_heff2_set_env "
                                    "with CTN_PREC_F64) for the refinement matvecs");
   HeffUser lo{plan, precision}, hi{plan, CTN_PREC_F64};
-  return ctn_lanczos_refined(heff_mv, &lo, heff_mv, &hi, psi0, plan->psi_elems, krydim, max_restarts, tol, krylov,
-                             work, eigvec, energy, residual, restarts, matvecs, stream);
+  // split-precision Krylov steps take the matvec result in FP32 (half the bytes through the
+  // step-4 epilogue and the two vector passes that read it)
+  const bool split = precision == CTN_PREC_3XTF32 || precision == CTN_PREC_BF16X3;
+  if (split)
+    CTN_REQUIRE(plan->split_bound[split_kind(precision)],
+                "ctn_heff2_lanczos_refined: environments not bound for this precision (ctn_heff2_set_env)");
+  CTN_REQUIRE(psi0 && krylov && work && eigvec && energy, "ctn_heff2_lanczos_refined: null argument");
+  return ctn::lanczos_refined(split ? heff_mv_f32 : heff_mv, &lo, heff_mv, &hi, psi0, plan->psi_elems, krydim,
+                              max_restarts, tol, krylov, work, eigvec, energy, residual, restarts, matvecs,
+                              ctn::as_stream(stream), /*w_f32=*/split);
 }
 
 extern "C" ctn_status ctn_heff2_profile(ctn_heff2_plan *p, const double *psi, double *out, int precision, int reps,

@@ -55,6 +55,9 @@ ctn_status heff_split_set_env(struct ::ctn_heff2_plan *p, int kind, const double
                               cudaStream_t st);
 ctn_status heff_split_matvec(struct ::ctn_heff2_plan *p, int kind, const double *psi, double *out, cudaStream_t st,
                              double *ms3);
+// the same with the result rounded to FP32 (n floats at out)
+ctn_status heff_split_matvec_f32out(struct ::ctn_heff2_plan *p, int kind, const double *psi, float *out,
+                                    cudaStream_t st);
 void heff_split_free(HeffSplit *s);
 double heff_split_gemm_flops(const struct ::ctn_heff2_plan *p, int kind, int step);
 void heff_split_apply_epilogue(struct ::ctn_heff2_plan *p, int kind);

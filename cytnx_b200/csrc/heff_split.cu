@@ -466,10 +466,11 @@ ctn_status heff_split_set_env(ctn_heff2_plan *p, int kind, const double *L, cons
   return split_set_env(p->split[kind], L, R, ws, st);
 }
 
-ctn_status split_matvec(HeffSplit *s, const void *psi, void *out, cudaStream_t st, double *ms4) {
+ctn_status split_matvec(HeffSplit *s, const void *psi, void *out, cudaStream_t st, double *ms4, bool f32_out) {
   CTN_REQUIRE(s && s->ws, "heff split: environments not bound");
   const int kind = s->kind;
-  const size_t oes = s->out_f32 ? 4 : 8;
+  const bool o32 = s->out_f32 || f32_out;
+  const size_t oes = o32 ? 4 : 8;
   uint8_t *w = s->ws;
   cudaEvent_t ev[5];
   if (ms4)
@@ -505,7 +506,7 @@ ctn_status split_matvec(HeffSplit *s, const void *psi, void *out, cudaStream_t s
     CTN_CHECK_LAUNCH();
   }
   if (ms4) CTN_CUDA(cudaEventRecord(ev[3], st));
-  if (s->out_f32)
+  if (o32)
     CTN_TRY(s->g4.run(w + s->o_a4h, w + s->o_a4l, w + s->o_b4h, w + s->o_b4l, (float *)out, nullptr, err, st));
   else
     CTN_TRY(s->g4.run(w + s->o_a4h, w + s->o_a4l, w + s->o_b4h, w + s->o_b4l, nullptr, (double *)out, err, st));
@@ -524,7 +525,11 @@ ctn_status split_matvec(HeffSplit *s, const void *psi, void *out, cudaStream_t s
 
 ctn_status heff_split_matvec(ctn_heff2_plan *p, int kind, const double *psi, double *out, cudaStream_t st,
                              double *ms4) {
-  return split_matvec(p->split[kind], psi, out, st, ms4);
+  return split_matvec(p->split[kind], psi, out, st, ms4, false);
+}
+
+ctn_status heff_split_matvec_f32out(ctn_heff2_plan *p, int kind, const double *psi, float *out, cudaStream_t st) {
+  return split_matvec(p->split[kind], psi, out, st, nullptr, true);
 }
 
 // ---------------------------------------------------------------- batches of independent problems
@@ -659,13 +664,13 @@ extern "C" ctn_status ctn_heff2_batch_set_env(ctn_heff2_batch *b, const void *L_
 }
 extern "C" ctn_status ctn_heff2_batch_matvec(ctn_heff2_batch *b, const void *psi_all, void *out_all, void *stream) {
   CTN_REQUIRE(b && psi_all && out_all, "ctn_heff2_batch_matvec: null argument");
-  return ctn::split_matvec(b->s, psi_all, out_all, ctn::as_stream(stream), nullptr);
+  return ctn::split_matvec(b->s, psi_all, out_all, ctn::as_stream(stream), nullptr, false);
 }
 extern "C" ctn_status ctn_heff2_batch_profile(ctn_heff2_batch *b, const void *psi_all, void *out_all, int reps,
                                               double *ms4, void *stream) {
   CTN_REQUIRE(b && psi_all && out_all && reps > 0 && ms4, "ctn_heff2_batch_profile: bad argument");
   double acc[4] = {0, 0, 0, 0};
-  for (int r = 0; r < reps; ++r) CTN_TRY(ctn::split_matvec(b->s, psi_all, out_all, ctn::as_stream(stream), acc));
+  for (int r = 0; r < reps; ++r) CTN_TRY(ctn::split_matvec(b->s, psi_all, out_all, ctn::as_stream(stream), acc, false));
   for (int i = 0; i < 4; ++i) ms4[i] = acc[i] / reps;
   return CTN_OK;
 }

@@ -374,6 +374,8 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
       // store; rows past M and columns past N are clipped by the tensor map.  The box is
       // reused once the previous store has read it (bulk-group wait on the read).
       const bool tma_out = p.cmaps != nullptr && g.mode == 0 && p.epi_staged;
+      // row-mapped FP64 groups launched with only an FP32 output go out as FP32 (mode 2)
+      const int mode = (g.mode == 1 && p.c64 == nullptr) ? 2 : g.mode;
       uint8_t *box = reinterpret_cast<uint8_t *>(smem + SM::EPI_OFF) + (warp - 2) * 4096;
 #pragma unroll 1
       for (int c0 = 0; c0 < BN && any_row; c0 += 32) {
@@ -405,9 +407,9 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
             asm volatile("cp.async.bulk.commit_group;" ::: "memory");
           }
         } else if (p.epi_staged) {
-          epi_store_piece(v, slab, lane, dst, cg0, ncol, g.mode, p.c32, p.c64);
+          epi_store_piece(v, slab, lane, dst, cg0, ncol, mode, p.c32, p.c64);
         } else if (dst >= 0) {
-          epi_store_direct(v, dst, cg0, ncol, g.mode, p.c32, p.c64);
+          epi_store_direct(v, dst, cg0, ncol, mode, p.c32, p.c64);
         }
       }
       tc_fence_before();
@@ -663,6 +665,8 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p, con
       const bool any_row = __any_sync(0xffffffffu, dst >= 0);  // warp-uniform: rows of this quarter inside M
       // row-strided FP32 output with a tensor map: TMA stores of 32 x 32 pieces (as in k_tc_gemm)
       const bool tma_out = p.cmaps != nullptr && g.mode == 0 && p.epi_staged;
+      // row-mapped FP64 groups launched with only an FP32 output go out as FP32 (mode 2)
+      const int mode = (g.mode == 1 && p.c64 == nullptr) ? 2 : g.mode;
       uint8_t *box = reinterpret_cast<uint8_t *>(smem + SM::EPI_OFF) + (warp - 2) * 4096;
 #pragma unroll 1
       for (int c0 = 0; c0 < BN && any_row; c0 += 32) {
@@ -694,9 +698,9 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p, con
             asm volatile("cp.async.bulk.commit_group;" ::: "memory");
           }
         } else if (p.epi_staged) {
-          epi_store_piece(v, slab, lane, dst, cg0, ncol, g.mode, p.c32, p.c64);
+          epi_store_piece(v, slab, lane, dst, cg0, ncol, mode, p.c32, p.c64);
         } else if (dst >= 0) {
-          epi_store_direct(v, dst, cg0, ncol, g.mode, p.c32, p.c64);
+          epi_store_direct(v, dst, cg0, ncol, mode, p.c32, p.c64);
         }
       }
       tc_fence_before();
