@@ -61,7 +61,18 @@ __device__ void finish(double part, double *partials, unsigned *ticket, double *
   }
 }
 
-__global__ void __launch_bounds__(RT) k_dot(const double *__restrict__ x, const double *__restrict__ y,
+// two consecutive elements (pair index i) of w as doubles: one 16-byte load for FP64, one
+// 8-byte load for FP32
+__device__ __forceinline__ double2 ld_pair(const double *w, int64_t i) {
+  return reinterpret_cast<const double2 *>(w)[i];
+}
+__device__ __forceinline__ double2 ld_pair(const float *w, int64_t i) {
+  const float2 v = reinterpret_cast<const float2 *>(w)[i];
+  return make_double2((double)v.x, (double)v.y);
+}
+
+template <typename XT>
+__global__ void __launch_bounds__(RT) k_dot(const XT *__restrict__ x, const double *__restrict__ y,
                                            int64_t n, double *partials, unsigned *ticket,
                                            double *out, int op) {
   double s = 0.0;
@@ -70,16 +81,15 @@ __global__ void __launch_bounds__(RT) k_dot(const double *__restrict__ x, const 
   const bool vec = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15) == 0;
   if (vec) {
     const int64_t n2 = n / 2;
-    const double2 *x2 = reinterpret_cast<const double2 *>(x);
     const double2 *y2 = reinterpret_cast<const double2 *>(y);
     for (int64_t i = tid; i < n2; i += step) {
-      double2 a = x2[i], b = y2[i];
+      const double2 a = ld_pair(x, i), b = y2[i];
       s = fma(a.x, b.x, s);
       s = fma(a.y, b.y, s);
     }
-    if (tid == 0 && (n & 1)) s = fma(x[n - 1], y[n - 1], s);
+    if (tid == 0 && (n & 1)) s = fma((double)x[n - 1], y[n - 1], s);
   } else {
-    for (int64_t i = tid; i < n; i += step) s = fma(x[i], y[i], s);
+    for (int64_t i = tid; i < n; i += step) s = fma((double)x[i], y[i], s);
   }
   s = block_sum(s);
   finish(s, partials, ticket, out, op);
@@ -109,24 +119,88 @@ __global__ void __launch_bounds__(RT) k_lanczos_update(double *__restrict__ w, c
   const double a = *alpha;
   const double b = p0 ? *beta : 0.0;
   double s = 0.0;
+  const int64_t tid = (int64_t)blockIdx.x * RT + threadIdx.x;
   const int64_t step = (int64_t)gridDim.x * RT;
-  for (int64_t i = (int64_t)blockIdx.x * RT + threadIdx.x; i < n; i += step) {
-    double v = w[i] - a * p1[i];
-    if (p0) v -= b * p0[i];
-    w[i] = v;
+  auto one = [&](double wv, double pv1, double pv0) -> double {
+    double v = wv - a * pv1;
+    if (p0) v -= b * pv0;
     s = fma(v, v, s);
+    return v;
+  };
+  const bool vec = ((reinterpret_cast<uintptr_t>(w) | reinterpret_cast<uintptr_t>(p1) |
+                     reinterpret_cast<uintptr_t>(p0)) & 15) == 0;
+  if (vec) {
+    const int64_t n2 = n / 2;
+    double2 *w2 = reinterpret_cast<double2 *>(w);
+    const double2 *a2 = reinterpret_cast<const double2 *>(p1), *b2 = reinterpret_cast<const double2 *>(p0);
+    const double2 z = make_double2(0.0, 0.0);
+    for (int64_t i = tid; i < n2; i += step) {
+      const double2 x = w2[i], y = a2[i], q = p0 ? b2[i] : z;
+      w2[i] = make_double2(one(x.x, y.x, q.x), one(x.y, y.y, q.y));
+    }
+    if (tid == 0 && (n & 1)) w[n - 1] = one(w[n - 1], p1[n - 1], p0 ? p0[n - 1] : 0.0);
+  } else {
+    for (int64_t i = tid; i < n; i += step) w[i] = one(w[i], p1[i], p0 ? p0[i] : 0.0);
+  }
+  s = block_sum(s);
+  finish(s, partials, ticket, nrm, 1);
+}
+
+// dst = w - alpha*p1 - beta*p0 (w FP32: the split-precision matvec's result) and ||dst||
+// in the same pass; dst is the next (unnormalised) Krylov slot
+__global__ void __launch_bounds__(RT) k_lanczos_update_to(const float *__restrict__ w, const double *__restrict__ p1,
+                                                         const double *__restrict__ p0, double *__restrict__ dst,
+                                                         int64_t n, const double *alpha, const double *beta,
+                                                         double *partials, unsigned *ticket, double *nrm) {
+  const double a = *alpha;
+  const double b = p0 ? *beta : 0.0;
+  double s = 0.0;
+  const int64_t tid = (int64_t)blockIdx.x * RT + threadIdx.x;
+  const int64_t step = (int64_t)gridDim.x * RT;
+  auto one = [&](double wv, double pv1, double pv0) -> double {
+    double v = wv - a * pv1;
+    if (p0) v -= b * pv0;
+    s = fma(v, v, s);
+    return v;
+  };
+  const bool vec = ((reinterpret_cast<uintptr_t>(w) | reinterpret_cast<uintptr_t>(p1) |
+                     reinterpret_cast<uintptr_t>(p0) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0;
+  if (vec) {
+    const int64_t n2 = n / 2;
+    double2 *d2 = reinterpret_cast<double2 *>(dst);
+    const double2 *a2 = reinterpret_cast<const double2 *>(p1), *b2 = reinterpret_cast<const double2 *>(p0);
+    const double2 z = make_double2(0.0, 0.0);
+    for (int64_t i = tid; i < n2; i += step) {
+      const double2 x = ld_pair(w, i), y = a2[i], q = p0 ? b2[i] : z;
+      d2[i] = make_double2(one(x.x, y.x, q.x), one(x.y, y.y, q.y));
+    }
+    if (tid == 0 && (n & 1)) dst[n - 1] = one((double)w[n - 1], p1[n - 1], p0 ? p0[n - 1] : 0.0);
+  } else {
+    for (int64_t i = tid; i < n; i += step) dst[i] = one((double)w[i], p1[i], p0 ? p0[i] : 0.0);
   }
   s = block_sum(s);
   finish(s, partials, ticket, nrm, 1);
 }
 
 // y = x / *a (y = 0 when *a is zero: a Lanczos breakdown leaves the next vector empty)
-__global__ void __launch_bounds__(RT) k_div_copy(const double *__restrict__ x, double *__restrict__ y,
-                                                int64_t n, const double *a) {
+// (x == y allowed: each element is read, then written, by the same thread)
+__global__ void __launch_bounds__(RT) k_div_copy(const double *x, double *y, int64_t n, const double *a) {
   const double al = *a;
   const bool zero = al == 0.0;
+  const int64_t tid = (int64_t)blockIdx.x * RT + threadIdx.x;
   const int64_t step = (int64_t)gridDim.x * RT;
-  for (int64_t i = (int64_t)blockIdx.x * RT + threadIdx.x; i < n; i += step) y[i] = zero ? 0.0 : x[i] / al;
+  if (((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15) == 0) {
+    const int64_t n2 = n / 2;
+    const double2 *x2 = reinterpret_cast<const double2 *>(x);
+    double2 *y2 = reinterpret_cast<double2 *>(y);
+    for (int64_t i = tid; i < n2; i += step) {
+      const double2 v = x2[i];
+      y2[i] = zero ? make_double2(0.0, 0.0) : make_double2(v.x / al, v.y / al);
+    }
+    if (tid == 0 && (n & 1)) y[n - 1] = zero ? 0.0 : x[n - 1] / al;
+  } else {
+    for (int64_t i = tid; i < n; i += step) y[i] = zero ? 0.0 : x[i] / al;
+  }
 }
 
 // ---- Krylov steps on unnormalised storage.  The restarted Lanczos keeps u_j = s_j q_j
@@ -137,15 +211,6 @@ __global__ void __launch_bounds__(RT) k_div_copy(const double *__restrict__ x, d
 
 __device__ __forceinline__ double safe_inv(double s) { return s != 0.0 ? 1.0 / s : 0.0; }
 
-// two consecutive elements (pair index i) of w as doubles: one 16-byte load for FP64, one
-// 8-byte load for FP32
-__device__ __forceinline__ double2 ld_pair(const double *w, int64_t i) {
-  return reinterpret_cast<const double2 *>(w)[i];
-}
-__device__ __forceinline__ double2 ld_pair(const float *w, int64_t i) {
-  const float2 v = reinterpret_cast<const float2 *>(w)[i];
-  return make_double2((double)v.x, (double)v.y);
-}
 
 // <w, a> / s^2 and <w, b> / s in one pass (s = *s_ptr, 1 when s_ptr is null; a zero s
 // gives zeros: the vector behind it is empty after a breakdown)
@@ -394,15 +459,29 @@ size_t reduce2_ws_bytes() { return (2 * MAXCTA + 8) * sizeof(double); }
 
 // ws2 layout (dot2s_f64): [2 * MAXCTA partials][ticket]
 // ws layout: [partials MAXCTA doubles][ticket (8 bytes)]
+ctn_status dot_f64(const float *x, const double *y, int64_t n, double *out, double *ws, cudaStream_t st) {
+  int g = grid_for(n);
+  k_dot<float><<<g, RT, 0, st>>>(x, y, n, ws, reinterpret_cast<unsigned *>(ws + MAXCTA), out, 0);
+  CTN_CHECK_LAUNCH();
+  return CTN_OK;
+}
+ctn_status lanczos_update_to_f64(const float *w, const double *p1, const double *p0, double *dst, int64_t n,
+                                 const double *alpha, const double *beta, double *nrm, double *ws, cudaStream_t st) {
+  int g = grid_for(n);
+  k_lanczos_update_to<<<g, RT, 0, st>>>(w, p1, p0, dst, n, alpha, beta, ws, reinterpret_cast<unsigned *>(ws + MAXCTA),
+                                        nrm);
+  CTN_CHECK_LAUNCH();
+  return CTN_OK;
+}
 ctn_status dot_f64(const double *x, const double *y, int64_t n, double *out, double *ws, cudaStream_t st) {
   int g = grid_for(n);
-  k_dot<<<g, RT, 0, st>>>(x, y, n, ws, reinterpret_cast<unsigned *>(ws + MAXCTA), out, 0);
+  k_dot<double><<<g, RT, 0, st>>>(x, y, n, ws, reinterpret_cast<unsigned *>(ws + MAXCTA), out, 0);
   CTN_CHECK_LAUNCH();
   return CTN_OK;
 }
 ctn_status nrm2_f64(const double *x, int64_t n, double *out, double *ws, cudaStream_t st) {
   int g = grid_for(n);
-  k_dot<<<g, RT, 0, st>>>(x, x, n, ws, reinterpret_cast<unsigned *>(ws + MAXCTA), out, 1);
+  k_dot<double><<<g, RT, 0, st>>>(x, x, n, ws, reinterpret_cast<unsigned *>(ws + MAXCTA), out, 1);
   CTN_CHECK_LAUNCH();
   return CTN_OK;
 }

@@ -8,6 +8,11 @@ size_t reduce_ws_bytes();
 // the same for dot2s_f64 (two reductions in one pass)
 size_t reduce2_ws_bytes();
 ctn_status dot_f64(const double *x, const double *y, int64_t n, double *out, double *ws, cudaStream_t st);
+// FP32 x (the split-precision matvec's result) against an FP64 y
+ctn_status dot_f64(const float *x, const double *y, int64_t n, double *out, double *ws, cudaStream_t st);
+// dst = w - alpha p1 - beta p0 with an FP32 w, ||dst|| -> *nrm (dst: the next Krylov slot)
+ctn_status lanczos_update_to_f64(const float *w, const double *p1, const double *p0, double *dst, int64_t n,
+                                 const double *alpha, const double *beta, double *nrm, double *ws, cudaStream_t st);
 ctn_status nrm2_f64(const double *x, int64_t n, double *out, double *ws, cudaStream_t st);
 ctn_status axpy_f64(const double *x, double *y, int64_t n, const double *a, double a_scale, cudaStream_t st);
 ctn_status scal_f64(double *x, int64_t n, const double *a, int invert, cudaStream_t st);

@@ -178,7 +178,7 @@ static ctn_status pinned_scalars(double **out) {
 // without side effects.
 ctn_status lanczos_gnd(int (*mv)(void *, const double *, double *, void *), void *user, const double *psi0,
                        int64_t n, int maxiter, double cvgcrit, double *krylov, double *work, double *eigvec,
-                       double *energy, int *iters, cudaStream_t st, bool speculate) {
+                       double *energy, int *iters, cudaStream_t st, bool speculate, bool w_f32) {
   CTN_REQUIRE(maxiter >= 2, "[Lanczos] Maxiter must >1");
   CTN_REQUIRE(cvgcrit > 0, "[Lanczos] converge criteria must >0");
   CTN_REQUIRE(n > 0, "[Lanczos] empty vector");
@@ -209,14 +209,22 @@ ctn_status lanczos_gnd(int (*mv)(void *, const double *, double *, void *), void
   CTN_TRY(div_copy_f64(psi0, krylov, n, scal + 0, st));
   // iteration i on the device: (i >= 1) psi_i = w / beta_{i-1}; w = H psi_i; alpha_i = <w, psi_i>;
   // w -= alpha_i psi_i + beta_{i-1} psi_{i-1}; beta_i = |w|; alpha_i, beta_i -> pinned slot i & 1
+  // w_f32 (split-precision matvecs): mv writes w as n floats, the update writes its FP64 result
+  // straight into the next Krylov slot, which the next iteration scales in place
   auto queue = [&](int i) -> ctn_status {
     double *pi = krylov + (int64_t)i * n;
     double *b_new = scal + 2 + (i & 1);
     const double *b_old = i ? scal + 2 + ((i - 1) & 1) : nullptr;
-    if (i) CTN_TRY(div_copy_f64(w, pi, n, b_old, st));
+    if (i) CTN_TRY(div_copy_f64(w_f32 ? pi : w, pi, n, b_old, st));
     if (mv(user, pi, w, st) != 0) return CTN_ERR_CUDA;
-    CTN_TRY(dot_f64(w, pi, n, scal + 1, ws, st));
-    CTN_TRY(lanczos_update_f64(w, pi, i ? pi - n : nullptr, n, scal + 1, b_old, b_new, ws, st));
+    if (w_f32) {
+      const float *wf = reinterpret_cast<const float *>(w);
+      CTN_TRY(dot_f64(wf, pi, n, scal + 1, ws, st));
+      CTN_TRY(lanczos_update_to_f64(wf, pi, i ? pi - n : nullptr, pi + n, n, scal + 1, b_old, b_new, ws, st));
+    } else {
+      CTN_TRY(dot_f64(w, pi, n, scal + 1, ws, st));
+      CTN_TRY(lanczos_update_f64(w, pi, i ? pi - n : nullptr, n, scal + 1, b_old, b_new, ws, st));
+    }
     CTN_CUDA(cudaMemcpyAsync(pin + 4 * (i & 1), scal + 1, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     CTN_CUDA(cudaEventRecord(ev[i & 1], st));
     return CTN_OK;
@@ -391,7 +399,7 @@ extern "C" ctn_status ctn_lanczos_gnd(ctn_matvec_fn matvec, void *user, const do
                                       double cvgcrit, double *krylov, double *work, double *eigvec, double *energy,
                                       int *iters, void *stream) {
   return ctn::lanczos_gnd(matvec, user, psi0, n, maxiter, cvgcrit, krylov, work, eigvec, energy, iters,
-                          ctn::as_stream(stream), /*speculate=*/false);
+                          ctn::as_stream(stream), /*speculate=*/false, /*w_f32=*/false);
 }
 
 namespace ctn {

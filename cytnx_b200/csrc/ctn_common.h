@@ -21,10 +21,11 @@ inline ctn_status cuda_fail(cudaError_t e, const char *what, const char *file, i
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
 // ground-state Lanczos (capi.cpp); speculate queues each next iteration before the host
-// solve of the current one (matvecs without side effects only: one extra call at the end)
+// solve of the current one (matvecs without side effects only: one extra call at the end);
+// w_f32: mv writes its result as n floats
 ctn_status lanczos_gnd(int (*mv)(void *, const double *, double *, void *), void *user, const double *psi0,
                        int64_t n, int maxiter, double cvgcrit, double *krylov, double *work, double *eigvec,
-                       double *energy, int *iters, cudaStream_t st, bool speculate);
+                       double *energy, int *iters, cudaStream_t st, bool speculate, bool w_f32);
 // restarted split-precision ground state (capi.cpp); w_f32: mv_lo writes its result as n floats
 ctn_status lanczos_refined(int (*mv_lo)(void *, const double *, double *, void *), void *u_lo,
                            int (*mv_hi)(void *, const double *, double *, void *), void *u_hi, const double *psi0,

@@ -467,8 +467,13 @@ extern "C" ctn_status ctn_heff2_lanczos_gnd(ctn_heff2_plan *plan, int precision,
                                             double *energy, int *iters, void *stream) {
   CTN_REQUIRE(plan && psi0 && krylov && work && eigvec && energy && iters, "ctn_heff2_lanczos_gnd: null argument");
   HeffUser u{plan, precision};
-  return ctn::lanczos_gnd(heff_mv, &u, psi0, plan->psi_elems, maxiter, cvgcrit, krylov, work, eigvec, energy, iters,
-                          ctn::as_stream(stream), /*speculate=*/true);
+  // split-precision matvecs hand their result over in FP32 (the matvec's own error is far above it)
+  const bool split = precision == CTN_PREC_3XTF32 || precision == CTN_PREC_BF16X3;
+  if (split)
+    CTN_REQUIRE(plan->split_bound[split_kind(precision)],
+                "ctn_heff2_lanczos_gnd: environments not bound for this precision (ctn_heff2_set_env)");
+  return ctn::lanczos_gnd(split ? heff_mv_f32 : heff_mv, &u, psi0, plan->psi_elems, maxiter, cvgcrit, krylov, work,
+                          eigvec, energy, iters, ctn::as_stream(stream), /*speculate=*/true, /*w_f32=*/split);
 }
 
 extern "C" ctn_status ctn_heff2_lanczos_refined(ctn_heff2_plan *plan, int precision, const double *psi0, int krydim,

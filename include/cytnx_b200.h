@@ -347,8 +347,10 @@ ctn_status ctn_heff2_lanczos_refined(ctn_heff2_plan *plan, int precision, const 
                                      int64_t *matvecs, void *stream);
 /* the same driver on a planned H_eff (no callback).  Each next iteration is queued on the
  * device before the host solves the current tridiagonal, so the host solve overlaps the next
- * matvec; after the last iteration one queued matvec is discarded (results are those of
- * ctn_lanczos_gnd with the same matvec, bit for bit). */
+ * matvec; after the last iteration one queued matvec is discarded.  CTN_PREC_F64: the results
+ * are those of ctn_lanczos_gnd with the same matvec, bit for bit.  Split precisions: the
+ * matvec hands its result to the recurrence in FP32 (its own error, ~1e-5, is far above the
+ * FP32 rounding); the recurrence itself is FP64. */
 ctn_status ctn_heff2_lanczos_gnd(ctn_heff2_plan *plan, int precision, const double *psi0,
                                  int maxiter, double cvgcrit, double *krylov, double *work,
                                  double *eigvec, double *energy, int *iters, void *stream);
