@@ -7,6 +7,10 @@
 
 namespace ctn {
 
+#ifndef F64_NARROW_BELOW
+#define F64_NARROW_BELOW 6  // 64 x 32 tiles when a plan has fewer 64 x 64 tiles than this many per SM
+#endif
+
 struct GemmTaskD {
   int64_t c_off;
   int32_t m, n, ldc;
@@ -41,11 +45,11 @@ struct GroupedGemmF64 {
   bool mixed = false;     // pairs disagree on the orientation (rejected at run time)
 
   void finalize() {
-    // fewer than two 64 x 64 tiles per SM (148 SMs): 64 x 32 tiles, twice as many CTAs and
-    // less padding on narrow groups
+    // fewer than six 64 x 64 tiles per SM (148 SMs; about 1.5 waves of four resident CTAs):
+    // 64 x 32 tiles, twice as many CTAs, less padding on narrow groups and a fuller last wave
     bn = 64;
     build_tiles_f64(tasks, pairs, tiles, bn);
-    if (tiles.size() < 2 * 148) {
+    if (tiles.size() < F64_NARROW_BELOW * 148) {
       bn = 32;
       build_tiles_f64(tasks, pairs, tiles, bn);
     }
