@@ -140,8 +140,8 @@ PAIR_DT = np.dtype([("a_off", "<i8"), ("b_off", "<i8"), ("k", "<i4"), ("lda", "<
 @pytest.mark.parametrize("shapes", ["wide", "narrow"])
 def test_grouped_gemm_tile_widths(flags, shapes):
     """ctn_gemm_grouped_f64 (the Gemm_Batch replacement) against FP64 torch matmuls.  'wide':
-    five 512 x 512 tasks (320 tiles of 64 x 64, the 64-wide kernel); 'narrow': ragged small
-    tasks (fewer than two tiles per SM, the 64 x 32 kernel).  Two pairs per task with k not a
+    four 1024 x 1024 tasks (1024 tiles of 64 x 64, above six per SM: the 64-wide kernel);
+    'narrow': ragged small tasks (the 64 x 32 kernel).  Two pairs per task with k not a
     multiple of 16, every operand orientation, one task without pairs (zeros)."""
     import ctypes
 
@@ -149,7 +149,7 @@ def test_grouped_gemm_tile_widths(flags, shapes):
 
     g = torch.Generator().manual_seed(11 + flags)
     if shapes == "wide":
-        mn = [(512, 512)] * 5
+        mn = [(1024, 1024)] * 4
     else:
         mn = [(70, 70), (130, 6), (5, 200), (64, 33), (1, 1)]
     ks = [40, 23]
