@@ -46,17 +46,31 @@ __global__ void __launch_bounds__(256) k_mpo_apply(const double *__restrict__ X1
                                                    const MpoTask *__restrict__ tasks,
                                                    const MpoTerm *__restrict__ terms,
                                                    const MpoChunk *__restrict__ chunks, int64_t nchunks) {
+  // each thread owns MPO_CHUNK / 256 elements of the chunk, 256 apart; the terms run outside
+  // so a term's loads for all of them are in flight together (per element the sum order over
+  // the terms is unchanged)
+  constexpr int PER = MPO_CHUNK / 256;
   for (int64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
     const MpoChunk ch = chunks[c];
     const MpoTask tk = tasks[ch.task];
     const int64_t end = tk.size < ch.start + MPO_CHUNK ? tk.size : ch.start + MPO_CHUNK;
-    for (int64_t e = ch.start + threadIdx.x; e < end; e += blockDim.x) {
-      double s = 0.0;
-      for (int t = 0; t < tk.term_count; ++t) {
-        const MpoTerm tm = terms[tk.term_begin + t];
-        s = fma(tm.coef, X1[tm.x1_off + e], s);
+    const int64_t e0 = ch.start + threadIdx.x;
+    double s[PER];
+#pragma unroll
+    for (int j = 0; j < PER; ++j) s[j] = 0.0;
+    for (int t = 0; t < tk.term_count; ++t) {
+      const MpoTerm tm = terms[tk.term_begin + t];
+      const double *src = X1 + tm.x1_off;
+#pragma unroll
+      for (int j = 0; j < PER; ++j) {
+        const int64_t e = e0 + (int64_t)j * 256;
+        if (e < end) s[j] = fma(tm.coef, __ldg(src + e), s[j]);
       }
-      X3[tk.x3_off + e] = s;
+    }
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      const int64_t e = e0 + (int64_t)j * 256;
+      if (e < end) X3[tk.x3_off + e] = s[j];
     }
   }
 }
