@@ -116,6 +116,9 @@ struct MpoSParams {
 constexpr int MPO_THREADS = 256;
 constexpr int MPO_UNROLL = 1;
 constexpr int MPO_ITEM = MPO_THREADS * MPO_UNROLL;  // chunks per work item
+#ifndef MPO_TERMS
+#define MPO_TERMS 1  // terms whose X1 loads are issued together (most X3 chunks have one or two)
+#endif
 
 // round-to-nearest (ties away) to TF32 / round-to-nearest-even to BF16 with integer ops
 // (ALU pipe; the conversion unit is the bottleneck of a cvt-based version)
@@ -168,8 +171,10 @@ __device__ __forceinline__ void mpo_store(const float (&x)[8], const MpoSegS &s,
 // thread finds its block by a binary search over the blocks the item overlaps).  Blocks
 // are ordered by (a', b), so the blocks that read the same X1 inputs run together and
 // share them in L2.  X1 block rows start on 16-byte boundaries (padded step-1 columns),
-// so full chunks load as float4.  Each thread computes MPO_UNROLL chunks together, four
-// terms per round: up to 2 x 4 x 2 independent 16-byte loads are in flight per thread.
+// so full chunks load as float4.  Each thread computes MPO_UNROLL chunks together, MPO_TERMS
+// terms per round (one: the kernel is close to issue-bound, and with 1.4 terms per chunk on
+// average wider rounds mostly issue predicated-off loads and multiplies by zero; 0.0386 ->
+// 0.0371 ms at D=4096 BF16x3 against four).
 // Six CTAs per SM (40 registers): occupancy over registers, the loads are latency-bound
 // (39 vs 43 us at D=4096 BF16x3 against the unconstrained 44-register build).
 template <int KIND>
@@ -207,13 +212,13 @@ __global__ void __launch_bounds__(MPO_THREADS, 6) k_mpo_split(MpoSParams p) {
     int tmax = 0;
 #pragma unroll
     for (int j = 0; j < U; ++j) tmax = max(tmax, nv[j] == E ? nt[j] : 0);
-    for (int t0 = 0; t0 < tmax; t0 += 4) {
-      float4 v[U][4], w[U][4];
-      float cf[U][4];
+    for (int t0 = 0; t0 < tmax; t0 += MPO_TERMS) {
+      float4 v[U][MPO_TERMS], w[U][MPO_TERMS];
+      float cf[U][MPO_TERMS];
 #pragma unroll
       for (int j = 0; j < U; ++j)
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < MPO_TERMS; ++u) {
           v[j][u] = w[j][u] = make_float4(0.f, 0.f, 0.f, 0.f);
           cf[j][u] = 0.f;
           if (nv[j] == E && t0 + u < nt[j]) {
@@ -227,7 +232,7 @@ __global__ void __launch_bounds__(MPO_THREADS, 6) k_mpo_split(MpoSParams p) {
 #pragma unroll
       for (int j = 0; j < U; ++j)
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < MPO_TERMS; ++u) {
           x[j][0] = fmaf(cf[j][u], v[j][u].x, x[j][0]);
           x[j][1] = fmaf(cf[j][u], v[j][u].y, x[j][1]);
           x[j][2] = fmaf(cf[j][u], v[j][u].z, x[j][2]);
