@@ -14,6 +14,8 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <numeric>
+#include <queue>
 #include <cstring>
 
 #include "tc_gemm.cuh"
@@ -1121,6 +1123,43 @@ void TcGemm::finalize() {
   for (auto &x : tmp) tiles.push_back(x.second);
 }
 
+// Order of the uploaded tile table.  The kernels hand tiles to their W persistent workers
+// round-robin (worker w takes positions w, w + W, ...), so worker w gets R + 1 tiles when
+// w < n mod W and R = n / W otherwise.  Within those counts the tiles are assigned largest
+// first to the least-loaded worker (work = tile width x K slices), then laid out so that the
+// round-robin walk visits that assignment.  The first round is the largest-first order itself.
+static std::vector<TcTile> balance_tiles(const std::vector<TcTile> &tiles, const std::vector<TcGroup> &groups,
+                                         int bn, int64_t W) {
+  const int64_t n = (int64_t)tiles.size();
+  if (W <= 0 || n <= W) return tiles;
+  const int64_t R = n / W, rem = n % W;
+  std::vector<double> work(n);
+  for (int64_t i = 0; i < n; ++i) {
+    const TcTile &t = tiles[i];
+    const TcGroup &g = groups[t.group];
+    const int neff = t.nt == g.nt - 1 ? (g.N - t.nt * bn + 15) / 16 * 16 : bn;
+    work[i] = (double)neff * g.kb;
+  }
+  std::vector<int64_t> idx(n);
+  std::iota(idx.begin(), idx.end(), 0);
+  std::stable_sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) { return work[a] > work[b]; });
+  using Slot = std::pair<double, int64_t>;
+  std::priority_queue<Slot, std::vector<Slot>, std::greater<Slot>> heap;
+  for (int64_t w = 0; w < W; ++w) heap.push({0.0, w});
+  std::vector<std::vector<int64_t>> lists(W);
+  for (int64_t i : idx) {
+    const Slot sl = heap.top();
+    heap.pop();
+    lists[sl.second].push_back(i);
+    const int64_t cap = R + (sl.second < rem ? 1 : 0);
+    if ((int64_t)lists[sl.second].size() < cap) heap.push({sl.first + work[i], sl.second});
+  }
+  std::vector<TcTile> out(n);
+  for (int64_t w = 0; w < W; ++w)
+    for (size_t k = 0; k < lists[w].size(); ++k) out[(int64_t)k * W + w] = tiles[lists[w][k]];
+  return out;
+}
+
 ctn_status TcGemm::upload(cudaStream_t st) {
   int dev = 0;
   CTN_CUDA(cudaGetDevice(&dev));
@@ -1134,10 +1173,13 @@ ctn_status TcGemm::upload(cudaStream_t st) {
   char *q = (char *)d_mem;
   if (!groups.empty()) CTN_CUDA(cudaMemcpyAsync(q, groups.data(), groups.size() * sizeof(TcGroup), cudaMemcpyHostToDevice, st));
   q += groups.size() * sizeof(TcGroup);
-  if (!tiles.empty()) CTN_CUDA(cudaMemcpyAsync(q, tiles.data(), tiles.size() * sizeof(TcTile), cudaMemcpyHostToDevice, st));
+  // the workers of the launch: CTAs (1-CTA form) or CTA pairs (2-CTA form)
+  const int64_t workers = std::min<int64_t>((int64_t)tiles.size(), pair ? nsm_count() / 2 : nsm_count());
+  const std::vector<TcTile> order = balance_tiles(tiles, groups, bn, workers);
+  if (!order.empty()) CTN_CUDA(cudaMemcpyAsync(q, order.data(), order.size() * sizeof(TcTile), cudaMemcpyHostToDevice, st));
   q += tiles.size() * sizeof(TcTile);
   if (!rowmap.empty()) CTN_CUDA(cudaMemcpyAsync(q, rowmap.data(), rowmap.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
-  CTN_CUDA(cudaStreamSynchronize(st));
+  CTN_CUDA(cudaStreamSynchronize(st));  // the host vectors (order among them) must outlive the copies
   return CTN_OK;
 }
 
