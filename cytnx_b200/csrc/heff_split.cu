@@ -549,6 +549,7 @@ HeffSplit *split_batch(std::vector<ctn_heff2_plan *> &plans, const int64_t *psi_
   B->g1.kind = B->g4.kind = kind;
   B->g1.set_width(bn1);
   B->g4.set_width(bn4);
+  B->g1.balance = B->g4.balance = false;
   B->pk_L.kind = B->pk_P.kind = B->pk_R.kind = kind;
   B->in_f32 = fp32_io;
   B->out_f32 = fp32_io;

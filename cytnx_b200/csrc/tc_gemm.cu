@@ -1175,7 +1175,7 @@ ctn_status TcGemm::upload(cudaStream_t st) {
   q += groups.size() * sizeof(TcGroup);
   // the workers of the launch: CTAs (1-CTA form) or CTA pairs (2-CTA form)
   const int64_t workers = std::min<int64_t>((int64_t)tiles.size(), pair ? nsm_count() / 2 : nsm_count());
-  const std::vector<TcTile> order = balance_tiles(tiles, groups, bn, workers);
+  const std::vector<TcTile> order = balance ? balance_tiles(tiles, groups, bn, workers) : tiles;
   if (!order.empty()) CTN_CUDA(cudaMemcpyAsync(q, order.data(), order.size() * sizeof(TcTile), cudaMemcpyHostToDevice, st));
   q += tiles.size() * sizeof(TcTile);
   if (!rowmap.empty()) CTN_CUDA(cudaMemcpyAsync(q, rowmap.data(), rowmap.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));

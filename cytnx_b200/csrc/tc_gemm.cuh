@@ -75,6 +75,9 @@ struct TcGemm {
   int kind = TC_TF32;
   int bn = 128;
   bool pair = false;  // 2-CTA (cta_group::2) tiles of 256 rows
+  // upload the tiles in a load-balanced round-robin order (off for the DRAM-bound batched
+  // plans, whose panels stay in L2 longer when a group's tiles run together)
+  bool balance = true;
   // signed width: bn for 1-CTA tiles, -bn for 2-CTA tiles
   void set_width(int w) {
     pair = w < 0;
