@@ -160,7 +160,8 @@ extern "C" ctn_status ctn_tridiag_eigh(int n, const double *d, const double *e, 
 namespace ctn {
 // per-thread pinned landing slots for the per-iteration scalars: a device-to-host copy into
 // pageable memory returns only when it has completed, which would hold the host at every
-// queued read; into pinned memory it is queued like a kernel
+// queued read; into pinned memory it is queued like a kernel.  128 bytes per calling thread,
+// allocated on first use and left to the process exit (no CUDA call from thread teardown)
 static ctn_status pinned_scalars(double **out) {
   static thread_local double *buf = nullptr;
   if (!buf) CTN_CUDA(cudaHostAlloc((void **)&buf, 16 * sizeof(double), cudaHostAllocPortable));
