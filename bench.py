@@ -161,41 +161,78 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
-def cpu_baseline_matvec(spec, mpo_vals, seed, sample_s, threads):
+def cpu_baseline_matvec(D, seed, sample_s, threads):
     """Reference CPU algorithm (oracle restatement of BlockUniTensor::contract, OpenBLAS
-    dgemm) on the host cores: matvecs in the order L -> M1 -> M2 -> R until sample_s."""
+    dgemm) on the host cores: whole matvecs in the order L -> M1 -> M2 -> R until
+    sample_s.  Inputs come from the oracle's own builder (no product code)."""
     import oracle as O
-    from cytnx_b200 import workloads as W
+    from oracle import workloads as OW
 
     O.set_threads(threads)
-    psi, L, M1, M2, R = W.build_two_site(spec, mpo_vals, seed=seed, device=-1)
-
-    def to_o(u, labels):
-        bonds = [O.Bond(b.type(), b._qnums, b._degs) for b in u.bonds()]
-        lay = u._layout
-        data = u._data.numpy()
-        blocks = [data[o:o + s].reshape(sh) for o, s, sh in zip(lay.offs, lay.sizes, lay.shapes)]
-        return O.BlockTensor(bonds, labels, u.rowrank(), lay.itoi, blocks)
-
-    ops = {"psi": to_o(psi, ["-1", "-2", "-3", "-4"]), "L": to_o(L, ["-5", "-1", "0"]),
-           "R": to_o(R, ["-7", "-4", "3"]), "M1": to_o(M1, ["-5", "-6", "-2", "1"]),
-           "M2": to_o(M2, ["-6", "-7", "-3", "2"])}
-
-    def mv():
-        t = ops["L"].contract(ops["psi"])
-        t = t.contract(ops["M1"])
-        t = t.contract(ops["M2"])
-        return t.contract(ops["R"])
-
-    mv()  # warm
+    ops = OW.xxz_two_site(D, seed=seed)
+    outs = OW.heff_chain(ops)  # warm; its results are the step buffers
     n, t0 = 0, time.perf_counter()
     while True:
-        mv()
+        OW.heff_chain(ops, outs=outs)
         n += 1
         el = time.perf_counter() - t0
         if el >= sample_s or n >= 50:
             break
-    return el / n, n
+    return el / n, n, OW.heff_flops(ops)
+
+
+def config_for(D, nsec, world):
+    """The workload description shared by both arms (the arithmetic form is in ``dtype``)."""
+    return {"workload": f"u1_xxz_two_site_heff_D{D}", "D": D, "sectors": nsec, "mpo_bond": 5, "d": 2,
+            "order": "L->M1->M2->R", "l2": "inputs larger than L2 (operands + intermediates > 126 MB)",
+            "parallelism": f"replicas{world}"}
+
+
+def run_reference(args, world, rank):
+    """The reference's CPU algorithm for the H_eff matvec (the oracle's restatement of
+    BlockUniTensor::contract with OpenBLAS dgemm per block pair, all host threads), on
+    the same workload, metric and JSON keys as this arm.  A step is one whole matvec
+    when --warmup + --steps of them fit in about 150 s; otherwise each step multiplies
+    every s-th block pair of all four contractions (s fixed so the run fits, steps
+    cycling through the s offsets), i.e. a bounded sample of the matvec, and the flops
+    are those of the pairs multiplied.  Imports nothing from the product package."""
+    import oracle as O
+    from oracle import workloads as OW
+
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    ops = OW.xxz_two_site(args.D, seed=0)
+    nsec = len(OW.u1_sector_sizes(args.D)[0])
+    t0 = time.perf_counter()
+    outs = OW.heff_chain(ops)  # one untimed whole matvec: sizes the sample, buffers for the steps
+    t_full = time.perf_counter() - t0
+    stride = max(1, int(np.ceil((args.steps + args.warmup) * t_full / 150.0)))
+    for i in range(args.warmup):
+        OW.heff_chain(ops, stride=stride, offset=i % stride, outs=outs)
+    fl = []
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        OW.heff_chain(ops, stride=stride, offset=(args.warmup + i) % stride, outs=outs, flops=fl)
+    el = time.perf_counter() - t0
+    val = sum(fl) / el / 1e12
+    sample = (f"{args.steps} whole H_eff matvecs at D={args.D}" if stride == 1 else
+              f"{args.steps} steps at D={args.D}, each the block pairs p = offset mod {stride} of the four "
+              f"contractions ({sum(fl) / args.steps:.3e} flops per step, a whole matvec is "
+              f"{OW.heff_flops(ops):.3e})")
+    line = {"metric": METRIC, "impl": "reference", "value": val, "unit": "TFLOP/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded numpy PCG64)", "config": config_for(args.D, nsec, world),
+            "cpu_baseline": {"value": val, "unit": "TFLOP/s", "cores": threads, "kind": "port",
+                             "sample": sample + " (oracle restatement of BlockUniTensor::contract, per-pair "
+                                                "permute + OpenBLAS dgemm, as the reference's non-MKL path)"},
+            "e2e": {"value": val, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+METRIC = "U(1) H_eff matvec TFLOP/s & Lanczos s/step, split-prec vs FP64, dE<=1e-9"
 
 
 def main():
@@ -211,6 +248,12 @@ def main():
         from datetime import timedelta
 
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     from cytnx_b200 import workloads as W
 
@@ -239,35 +282,7 @@ def main():
 
     spec = W.xxz_spec(args.D)
     mpo_vals = W.xxz_mpo_values(1.0, 1.0, 0.0)
-    workload = f"u1_xxz_two_site_heff_D{args.D}"
-    config_base = {"workload": workload, "D": args.D, "sectors": int(len(spec.dv)), "mpo_bond": 5, "d": 2,
-                   "order": "L->M1->M2->R", "l2": "inputs larger than L2 (operands + intermediates > 126 MB)"}
-
-    if args.impl == "reference":
-        if rank != 0:
-            if world > 1:
-                dist.destroy_process_group()
-            return
-        threads = os.cpu_count() or 1
-        # algorithmic flops from the block structure (host only)
-        import cytnx_b200 as c
-
-        sec, n = cpu_baseline_matvec(spec, mpo_vals, 0, max(2.0, min(args.cpu_sample_s, 60.0)), threads)
-        flops = _algo_flops_host(spec, mpo_vals)
-        val = flops / sec / 1e12
-        line = {"metric": "U(1) H_eff matvec TFLOP/s & Lanczos s/step, split-prec vs FP64, dE<=1e-9",
-                "impl": "reference", "value": val, "unit": "TFLOP/s", "n_gpus": args.gpus, "steps": n,
-                "steps_requested": args.steps, "warmup": 1, "ms_per_step": sec * 1e3, "higher_is_better": True,
-                "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded numpy PCG64)",
-                "config": dict(config_base, parallelism="cpu"),
-                "cpu_baseline": {"value": val, "unit": "TFLOP/s", "cores": threads, "kind": "port",
-                                 "sample": f"{n} whole matvecs at D={args.D} after one untimed one (oracle "
-                                           f"restatement, OpenBLAS dgemm; one matvec takes seconds on the host, so "
-                                           f"the run is bounded by time, not by --steps)"},
-                "e2e": {"value": val, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
-        return
+    config_base = config_for(args.D, int(len(spec.dv)), world)
 
     import ctypes
 
@@ -435,7 +450,7 @@ def main():
 
     # ---- ground state to convergence: restarted Lanczos, Krylov steps in each form, one FP64
     # refinement matvec per restart; energies are FP64 Rayleigh quotients of the returned vectors
-    refined = {}
+    refined, ground = {}, {}
     for form in forms:
         # warm at the same Krylov dimension (its buffers come from the caching allocator afterwards)
         H.lanczos_refined(psi, precision=form, krylov_dim=32, max_restarts=2, tol=0.0)
@@ -449,6 +464,7 @@ def main():
                          "residual_rel": r["residual"] / abs(r["energy"]), "restarts": r["restarts"],
                          "matvecs_split_or_form": r["matvecs_lo"], "matvecs_fp64": r["matvecs_fp64"],
                          "time_to_solution_s": dt, "s_per_step": dt / max(nmv, 1)}
+        ground[form] = r["vec"].flat_view().cpu().numpy()
     e64 = refined["fp64"]["energy"]
     for form in forms:
         refined[form]["dE_rel_vs_fp64"] = abs(refined[form]["energy"] - e64) / abs(e64)
@@ -505,25 +521,32 @@ def main():
     batched = run_batched(args, world, rank, dev, st) if args.batch_problems > 0 else None
     mps_ad = run_mps_autograd(args, dev) if args.mps_lbfgs_steps > 0 else None
     if rank == 0:
+        ora = None
+        if os.environ.get("CTN_BENCH_NO_ORACLE") != "1":
+            ora = oracle_checks(args.D, {f: r["y"].cpu().numpy() for f, r in results.items()}, ground,
+                                {f: refined[f]["energy"] for f in forms})
         cpu = None
         if world == 1 and os.environ.get("CTN_BENCH_NO_CPU") != "1":
             threads = os.cpu_count() or 1
-            sec, n = cpu_baseline_matvec(spec, mpo_vals, 0, args.cpu_sample_s, threads)
-            cpu = {"value": flops / sec / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": "port",
+            sec, n, oflops = cpu_baseline_matvec(args.D, 0, args.cpu_sample_s, threads)
+            cpu = {"value": oflops / sec / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": "port",
                    "sample": f"{n} H_eff matvecs at D={args.D} on the host (oracle restatement of "
                              f"BlockUniTensor::contract, OpenBLAS dgemm), {sec:.3f} s each"}
         forms_out = {f: {k: v for k, v in r.items() if k != "y"} for f, r in results.items()}
         line = {
-            "metric": "U(1) H_eff matvec TFLOP/s & Lanczos s/step, split-prec vs FP64, dE<=1e-9",
-            "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": head["ms_per_matvec"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": args.precision, "data": "synthetic (seeded numpy PCG64)",
-            "config": dict(config_base, parallelism=f"replicas{world}", precision=args.precision),
+            "config": config_base,
             "algorithmic_flops_per_matvec": flops,
             "autotuned_tiles": tiles,
             "forms": forms_out,
             "speedup_vs_fp64": results["fp64"]["ms_per_matvec"] / head["ms_per_matvec"],
             "matvec_rel_err_vs_fp64": mv_err,
+            "matvec_rel_err_vs_oracle": ora["matvec_rel_err_vs_oracle"][args.precision] if ora else None,
+            "dE_rel_vs_oracle": ora["refined"][args.precision]["dE_rel_vs_oracle"] if ora else None,
+            "residual_rel_vs_oracle": ora["refined"][args.precision]["residual_rel_oracle"] if ora else None,
+            "oracle_checks": ora,
             "lanczos": lanczos,
             "lanczos_refined": refined,
             "lanczos_s_per_step": refined[args.precision]["s_per_step"],
@@ -546,6 +569,38 @@ def main():
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def oracle_checks(D, ys, ground, energies):
+    """Errors against the oracle's FP64 matvec, computed on the host outside every timed
+    region: each form's matvec output against the oracle's matvec of the same input, and
+    each form's refined ground state v checked with the oracle's matvec (Rayleigh quotient
+    E_o(v) and eigen-residual |H v - E_o v| / (|E_o| |v|); by the symmetric residual bound an
+    exact eigenvalue of the oracle's operator lies within that residual of E_o).  The
+    energies' dE is taken against E_o of the FP64 run's ground state."""
+    import oracle as O
+    from oracle import workloads as OW
+
+    t0 = time.perf_counter()
+    O.set_threads(os.cpu_count() or 1)
+    ops = OW.xxz_two_site(D, seed=0)
+    ref = OW.heff_matvec(ops)
+    nref = float(np.linalg.norm(ref))
+    out = {"matvec_rel_err_vs_oracle": {f: float(np.linalg.norm(y - ref) / nref) for f, y in ys.items()},
+           "refined": {}}
+    eo = {}
+    for f, v in ground.items():
+        hv = OW.heff_matvec(ops, v)
+        e = float(np.dot(v, hv) / np.dot(v, v))
+        eo[f] = e
+        out["refined"][f] = {"E_oracle_rayleigh": e,
+                             "residual_rel_oracle": float(np.linalg.norm(hv - e * v) / (abs(e) * np.linalg.norm(v))),
+                             "E_reported_minus_E_oracle_rel": abs(energies[f] - e) / abs(e)}
+    e_ref = eo.get("fp64")
+    for f in out["refined"]:
+        out["refined"][f]["dE_rel_vs_oracle"] = abs(energies[f] - e_ref) / abs(e_ref) if e_ref else None
+    out["host_seconds"] = time.perf_counter() - t0
+    return out
 
 
 def run_batched(args, world, rank, dev, st):
@@ -613,6 +668,20 @@ def run_batched(args, world, rank, dev, st):
             got = rec["_B"].slice(rec["_y"], i).double()
             errs[f].append(float((torch.linalg.vector_norm(got - ref) / nref).item()))
         del H
+    # a sample of the problems against the oracle's FP64 matvec (host, untimed, rank 0's shard)
+    from oracle import workloads as OW
+
+    pick = list(range(0, len(probs), max(1, len(probs) // 8)))[:8]
+    oerr = {f: [] for f in out["forms"]}
+    for i in pick:
+        ref = OW.heff_matvec(OW.hubbard_two_site(dims[mine[i]], 1000 + mine[i]))
+        nref = np.linalg.norm(ref)
+        for f, rec in out["forms"].items():
+            got = rec["_B"].slice(rec["_y"], i).double().cpu().numpy()
+            oerr[f].append(float(np.linalg.norm(got - ref) / nref))
+    for f, rec in out["forms"].items():
+        rec["rel_err_vs_oracle_sample"] = {"problems": [int(mine[i]) for i in pick],
+                                           "D": [int(dims[mine[i]]) for i in pick], "max": max(oerr[f])}
     for f, rec in out["forms"].items():
         e = torch.tensor(errs[f], dtype=torch.float64, device=dev)
         mx = e.max().clone()
@@ -770,11 +839,20 @@ def run_mps_autograd(args, dev):
     out["fd_check"] = {"entries": 64, "h": h, "max_abs_err": worst, "max_abs_grad": float(flat_g.abs().max())}
     num = mps.energy(checkpoint_every=4, numerator_only=True)
     gnum = torch.autograd.grad(num, mps.params)
+    # 2 H_eff,k A_k from the oracle's contractions (environments included), host, untimed
+    import oracle as O
+    from oracle import workloads as OW
+
+    O.set_threads(os.cpu_count() or 1)
+    bq = [b._qnums[:, 0].copy() for b in mps.bonds]
+    bd = [b._degs.copy() for b in mps.bonds]
+    flats = [p.detach().cpu().numpy() for p in mps.params]
     errs = []
     for k in (0, L // 2, L - 1):
-        ref = 2.0 * mps.heff_times_site(k)
-        errs.append(float(torch.linalg.vector_norm(gnum[k] - ref) / torch.linalg.vector_norm(ref)))
-    out["grad_vs_2HeffA_rel_err_max"] = max(errs)
+        ref = 2.0 * OW.mps_heff_times_site(bq, bd, flats, k)
+        errs.append(float(np.linalg.norm(gnum[k].cpu().numpy() - ref) / np.linalg.norm(ref)))
+    out["grad_vs_oracle_2HeffA_rel_err_max"] = max(errs)
+    out["grad_vs_oracle_2HeffA_sites"] = [0, L // 2, L - 1]
     if args.mps_lbfgs_steps > 0:
         x = torch.cat([p.detach().reshape(-1) for p in mps.params]).clone().requires_grad_(True)
         opt = torch.optim.LBFGS([x], lr=1.0, max_iter=args.mps_lbfgs_steps, history_size=30,
@@ -798,33 +876,6 @@ def run_mps_autograd(args, dev):
                         "trace_every_20": hist[::20]}
     out["setup_and_checks_s"] = time.perf_counter() - t_setup
     return out
-
-
-def _algo_flops_host(spec, mpo_vals):
-    """Algorithmic flops without a GPU: the planner counts block pairs on the host."""
-    from cytnx_b200.unitensor import contract_plan_flops, structure_only
-    from cytnx_b200 import workloads as W
-    from cytnx_b200.core import BD_KET, Bond
-
-    Vl = Bond(BD_KET, spec.qv.reshape(-1, 1), spec.dv)
-    Vr = Bond(BD_KET, spec.qv_r.reshape(-1, 1), spec.dv_r)
-    phys = Bond(BD_KET, np.array(spec.phys_q).reshape(-1, 1), [1] * len(spec.phys_q))
-    inner = Bond(BD_KET, np.array(spec.inner_q).reshape(-1, 1), [1] * len(spec.inner_q))
-    P = structure_only([Vl, phys.redirect(), phys.redirect(), Vr.redirect()], ["a", "s1", "s2", "b"])
-    L = structure_only([inner.redirect(), Vl.redirect(), Vl], ["w", "a", "ap"])
-    M1 = structure_only([inner, inner.redirect(), phys, phys.redirect()], ["w", "w1", "s1", "s1p"])
-    M2 = structure_only([inner, inner.redirect(), phys, phys.redirect()], ["w1", "w2", "s2", "s2p"])
-    R = structure_only([inner, Vr, Vr.redirect()], ["w2", "b", "bp"])
-    from cytnx_b200.heff import _struct_contract
-
-    f = contract_plan_flops(L, P)
-    T1 = _struct_contract(L, P)
-    f += contract_plan_flops(T1, M1)
-    T2 = _struct_contract(T1, M1)
-    f += contract_plan_flops(T2, M2)
-    T3 = _struct_contract(T2, M2)
-    f += contract_plan_flops(T3, R)
-    return f
 
 
 if __name__ == "__main__":

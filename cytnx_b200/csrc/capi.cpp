@@ -36,79 +36,82 @@ static ctn_status device_ws(double **ws) {
   return CTN_OK;
 }
 
-// Symmetric tridiagonal eigenproblem by the implicit QL algorithm with Wilkinson-type
-// shifts (the EISPACK tql2 / "tqli" scheme: Bowdler, Martin, Reinsch & Wilkinson,
-// Numer. Math. 11 (1968) 293-306).  d: diagonal (n), e: sub-diagonal (n-1).
-// Eigenvalues ascending; z (n x n, row-major) receives eigenvectors as ROWS, which is
-// the is_row=true layout linalg::Tridiag returns (src/linalg/Tridiag.cpp:83-95).
-// With zrows == nullptr the rotations are not accumulated (O(n^2) instead of O(n^3)); the
-// eigenvalues do not depend on the accumulation and come out bit-identical.
+// Symmetric tridiagonal eigenproblem by the implicit symmetric QR algorithm with
+// Wilkinson shifts (Golub & Van Loan, Matrix Computations, 4th ed., Algorithms 8.3.2
+// "implicit symmetric QR step" and 8.3.3 "symmetric QR"): the trailing unreduced window
+// [lo, hi] of T is swept by Givens rotations that chase the shift's bulge down the band,
+// and off-diagonals below eps * (|d_i| + |d_i+1|) split the problem.  d: diagonal (n),
+// e: off-diagonal (n-1).  Eigenvalues ascending; z (n x n, row-major) receives the
+// eigenvectors as ROWS, the is_row=true layout linalg::Tridiag returns
+// (src/linalg/Tridiag.cpp:83-95).  With zrows == nullptr no rotation is accumulated
+// (O(n^2) instead of O(n^3)); the eigenvalues do not depend on it and are bit-identical.
 static ctn_status tql(int n, const double *din, const double *ein, double *w, double *zrows) {
-  std::vector<double> d(din, din + n), e(n, 0.0);
+  std::vector<double> d(din, din + n), e(n > 1 ? n - 1 : 1, 0.0);
   for (int i = 0; i + 1 < n; ++i) e[i] = ein[i];
-  // column-major accumulation: z[k + n*i] = comp k of vec i
-  std::vector<double> z(zrows ? (size_t)n * n : 0, 0.0);
+  // vec[j * n + k]: component k of the j-th column of the accumulated rotation product V
+  // (T_input = V T_current V^T), so the two columns a rotation touches are contiguous
+  std::vector<double> vec(zrows ? (size_t)n * n : 0, 0.0);
   if (zrows)
-    for (int i = 0; i < n; ++i) z[(size_t)i * n + i] = 1.0;
-  for (int l = 0; l < n; ++l) {
-    int iter = 0;
-    int m;
-    do {
-      for (m = l; m < n - 1; ++m) {
-        const double dd = std::fabs(d[m]) + std::fabs(d[m + 1]);
-        if (std::fabs(e[m]) <= 1e-300 || std::fabs(e[m]) + dd == dd) break;
+    for (int j = 0; j < n; ++j) vec[(size_t)j * n + j] = 1.0;
+  const double eps = std::numeric_limits<double>::epsilon();
+  auto negligible = [&](int i) {
+    return std::fabs(e[i]) <= eps * (std::fabs(d[i]) + std::fabs(d[i + 1])) || std::fabs(e[i]) < 1e-300;
+  };
+  // rotation R = [[c, s], [-s, c]] on coordinates (k, k+1): T <- R T R^T, V <- V R^T
+  auto rotate_vectors = [&](int k, double c, double s) {
+    if (!zrows) return;
+    double *u = &vec[(size_t)k * n], *v = &vec[(size_t)(k + 1) * n];
+    for (int i = 0; i < n; ++i) {
+      const double a = u[i], b = v[i];
+      u[i] = c * a + s * b;
+      v[i] = c * b - s * a;
+    }
+  };
+  long long budget = 60ll * std::max(n, 1);
+  int hi = n - 1;
+  while (hi > 0) {
+    if (negligible(hi - 1)) {
+      e[hi - 1] = 0.0;
+      --hi;
+      continue;
+    }
+    int lo = hi - 1;
+    while (lo > 0 && !negligible(lo - 1)) --lo;
+    if (--budget < 0) {
+      set_error("ctn_tridiag_eigh: QR iteration did not converge");
+      return CTN_ERR_NUMERIC;
+    }
+    // Wilkinson shift: the eigenvalue of the trailing 2 x 2 block closer to d[hi]
+    const double half = 0.5 * (d[hi - 1] - d[hi]);
+    const double off = e[hi - 1];
+    const double den = half + (half >= 0.0 ? 1.0 : -1.0) * std::hypot(half, off);
+    const double mu = d[hi] - (den != 0.0 ? off * off / den : 0.0);
+    // implicit QR step: the first rotation comes from the shifted first column, each
+    // later one removes the bulge the previous one created below the band
+    double x = d[lo] - mu, z = e[lo];
+    for (int k = lo; k < hi; ++k) {
+      const double r = std::hypot(x, z);
+      const double c = r != 0.0 ? x / r : 1.0, s = r != 0.0 ? z / r : 0.0;
+      if (k > lo) e[k - 1] = r;
+      const double p = d[k], q = e[k], t = d[k + 1];
+      const double cc = c * c, ss = s * s, cs = c * s;
+      d[k] = cc * p + 2.0 * cs * q + ss * t;
+      d[k + 1] = ss * p - 2.0 * cs * q + cc * t;
+      e[k] = cs * (t - p) + (cc - ss) * q;
+      rotate_vectors(k, c, s);
+      if (k + 1 < hi) {
+        z = s * e[k + 1];  // the new bulge at (k + 2, k)
+        e[k + 1] *= c;
+        x = e[k];
       }
-      if (m != l) {
-        if (++iter > 200) {
-          set_error("ctn_tridiag_eigh: QL iteration did not converge");
-          return CTN_ERR_NUMERIC;
-        }
-        double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-        double r = std::hypot(g, 1.0);
-        g = d[m] - d[l] + e[l] / (g + (g >= 0 ? std::fabs(r) : -std::fabs(r)));
-        double s = 1.0, c = 1.0, p = 0.0;
-        int i;
-        bool early = false;
-        for (i = m - 1; i >= l; --i) {
-          double f = s * e[i];
-          const double b = c * e[i];
-          r = std::hypot(f, g);
-          e[i + 1] = r;
-          if (r == 0.0) {
-            d[i + 1] -= p;
-            e[m] = 0.0;
-            early = true;
-            break;
-          }
-          s = f / r;
-          c = g / r;
-          g = d[i + 1] - p;
-          r = (d[i] - g) * s + 2.0 * c * b;
-          p = s * r;
-          d[i + 1] = g + p;
-          g = c * r - b;
-          if (zrows) {
-            double *zi = &z[(size_t)i * n], *zi1 = &z[(size_t)(i + 1) * n];
-            for (int k = 0; k < n; ++k) {
-              f = zi1[k];
-              zi1[k] = s * zi[k] + c * f;
-              zi[k] = c * zi[k] - s * f;
-            }
-          }
-        }
-        if (early) continue;
-        d[l] -= p;
-        e[l] = g;
-        e[m] = 0.0;
-      }
-    } while (m != l);
+    }
   }
   std::vector<int> idx(n);
   std::iota(idx.begin(), idx.end(), 0);
   std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return d[a] < d[b]; });
   for (int j = 0; j < n; ++j) {
     w[j] = d[idx[j]];
-    if (zrows) std::memcpy(zrows + (size_t)j * n, &z[(size_t)idx[j] * n], sizeof(double) * n);
+    if (zrows) std::memcpy(zrows + (size_t)j * n, &vec[(size_t)idx[j] * n], sizeof(double) * n);
   }
   return CTN_OK;
 }

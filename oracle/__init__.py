@@ -80,6 +80,7 @@ def lib():
         _lib.orc_permute.restype = ctypes.c_int
         _lib.orc_blocks_enumerate.restype = ctypes.c_int64
         _lib.orc_bs_contract.restype = ctypes.c_int
+        _lib.orc_bs_contract_ex.restype = ctypes.c_int
     return _lib
 
 
@@ -204,7 +205,11 @@ class BlockTensor:
                            self.itoi[:, mapper] if len(self.itoi) else self.itoi,
                            [permute(b, mapper) for b in self.blocks])
 
-    def contract(self, rhs: "BlockTensor") -> "BlockTensor":
+    def contract(self, rhs: "BlockTensor", stride: int = 1, offset: int = 0, out: "BlockTensor" = None,
+                 flops: list = None) -> "BlockTensor":
+        """BlockUniTensor::contract.  ``stride`` > 1 multiplies only every stride-th block
+        pair (from ``offset``) into ``out`` (a bounded sample of the work for CPU timings);
+        ``stride`` 0 only counts.  ``flops`` (a list) receives 2*M*N*K of the pairs taken."""
         comm = sorted(set(self.labels) & set(rhs.labels))
         c1 = [self.labels.index(l) for l in comm]
         c2 = [rhs.labels.index(l) for l in comm]
@@ -230,23 +235,67 @@ class BlockTensor:
         out_labels = [self.labels[i] for i in n1] + [rhs.labels[i] for i in n2]
         rowrank = self.rowrank + rhs.rowrank - sum(1 for i in c1 if i < self.rowrank) \
             - sum(1 for i in c2 if i < rhs.rowrank)
-        out = BlockTensor(out_bonds, out_labels, rowrank, dtype=dt)
+        reuse = out is not None
+        if not reuse:
+            out = BlockTensor(out_bonds, out_labels, rowrank, dtype=dt)
         code = {np.dtype(np.float64): 3, np.dtype(np.complex128): 1}[np.dtype(dt)]
         L = self if self.dtype == dt else self.astype(dt)
         R = rhs if rhs.dtype == dt else rhs.astype(dt)
         keep = []
-        ldat, rdat = np.ascontiguousarray(L.flat()), np.ascontiguousarray(R.flat())
-        odat = np.zeros(sum(b.size for b in out.blocks), dtype=dt)
-        rc = lib().orc_bs_contract(ctypes.c_int(code), L._layout(keep), _p(ldat),
-                                   R._layout(keep), _p(rdat), ctypes.c_int(len(comm)),
-                                   _p(_i64(c1)), _p(_i64(c2)), out._layout(keep), _p(odat))
+        ldat = self._flat_cache(L)
+        rdat = rhs._flat_cache(R)
+        if reuse:
+            odat = out._odat
+        else:
+            odat = np.zeros(sum(b.size for b in out.blocks), dtype=dt)
+        fl = ctypes.c_double(0.0)
+        rc = lib().orc_bs_contract_ex(ctypes.c_int(code), L._layout(keep), _p(ldat),
+                                      R._layout(keep), _p(rdat), ctypes.c_int(len(comm)),
+                                      _p(_i64(c1)), _p(_i64(c2)), out._layout(keep), _p(odat),
+                                      ctypes.c_int64(stride), ctypes.c_int64(offset), ctypes.byref(fl))
         if rc:
             raise RuntimeError(f"orc_bs_contract failed ({rc})")
-        pos = 0
-        for i, b in enumerate(out.blocks):
-            out.blocks[i] = odat[pos:pos + b.size].reshape(b.shape)
-            pos += b.size
+        if flops is not None:
+            flops.append(fl.value)
+        if not reuse:
+            pos = 0
+            for i, b in enumerate(out.blocks):
+                out.blocks[i] = odat[pos:pos + b.size].reshape(b.shape)
+                pos += b.size
+            out._odat = odat
         return out
+
+    def contract_flops(self, rhs: "BlockTensor") -> float:
+        """2*M*N*K summed over the block pairs BlockUniTensor::contract multiplies."""
+        fl = []
+        self.contract(rhs, stride=0, flops=fl)
+        return fl[0]
+
+    def _flat_cache(self, conv):
+        """Contiguous flat data of ``conv`` (this tensor or its dtype conversion).  When
+        every block is still a view into the one buffer it was made from (a contract
+        result, or ``from_flat``), that buffer is used as it is."""
+        od = getattr(self, "_odat", None)
+        if conv is self and od is not None and all(b.base is od for b in self.blocks):
+            return od
+        return np.ascontiguousarray(conv.flat())
+
+    @classmethod
+    def from_flat(cls, bonds, labels, rowrank, itoi, flat) -> "BlockTensor":
+        """Blocks as views into ``flat`` (back to back in ``itoi`` order, row-major)."""
+        t = cls(bonds, labels, rowrank, itoi, blocks=[])
+        flat = np.ascontiguousarray(flat)
+        blocks, pos = [], 0
+        for tup in t.itoi:
+            shp = t.block_shape(tup)
+            n = int(np.prod(shp))
+            blocks.append(flat[pos:pos + n].reshape(shp))
+            pos += n
+        if pos != flat.size:
+            raise ValueError("flat data size does not match the blocks")
+        t.blocks = blocks
+        t._odat = flat
+        return t
 
     def astype(self, dt):
         return BlockTensor(self.bonds, self.labels, self.rowrank, self.itoi,

@@ -200,10 +200,15 @@ static int64_t tmap_find(const tmap *m, const int64_t *itoi, int rank, const int
   return -1;
 }
 
-/* dtype: 3 = float64, 1 = complex128 (reference dtype ids). */
-int orc_bs_contract(int dtype, orc_layout L, const void *Ldata, orc_layout R, const void *Rdata,
-                    int ncomm, const int64_t *comm1, const int64_t *comm2, orc_layout O,
-                    void *Odata) {
+/* dtype: 3 = float64, 1 = complex128 (reference dtype ids).
+ * Pair sampling (for bounded CPU timings): the block pairs are numbered in the order the
+ * loops below meet them; with stride >= 1 only pairs p with p % stride == offset are
+ * multiplied (stride 1: every pair, the reference's contract), and the output is cleared
+ * only when offset == 0.  stride <= 0 counts without computing or touching Odata.
+ * *flops (if not NULL) receives 2*M*N*K summed over the pairs taken. */
+int orc_bs_contract_ex(int dtype, orc_layout L, const void *Ldata, orc_layout R, const void *Rdata,
+                       int ncomm, const int64_t *comm1, const int64_t *comm2, orc_layout O,
+                       void *Odata, int64_t stride, int64_t offset, double *flops) {
   const int64_t es = (dtype == 1) ? 16 : 8;
   int rl = L.rank, rr = R.rank;
   int ncl = rl - ncomm, ncr = rr - ncomm;
@@ -234,8 +239,11 @@ int orc_bs_contract(int dtype, orc_layout L, const void *Ldata, orc_layout R, co
   for (int i = 0; i < rl; i++) invL[mapL[i]] = i;
   for (int i = 0; i < rr; i++) invR[mapR[i]] = i;
 
+  const int count_only = stride <= 0;
+  double fl = 0.0;
+  int64_t pair = -1;
   /* Init() allocates every output block as zeros (BlockUniTensor.cpp:213-216). */
-  {
+  if (!count_only && offset == 0) {
     int64_t tot = 0;
     for (int64_t b = 0; b < O.nblocks; b++) {
       int64_t sz = 1;
@@ -257,7 +265,7 @@ int orc_bs_contract(int dtype, orc_layout L, const void *Ldata, orc_layout R, co
     int64_t comm_dim = 1, lsz = 1;
     for (int k = 0; k < ncomm; k++) comm_dim *= shl[comm1[k]];
     for (int i = 0; i < rl; i++) lsz *= shl[i];
-    if (lsz > lcap) {
+    if (!count_only && lsz > lcap) {
       free(Lbuf);
       Lbuf = (char *)malloc(lsz * es);
       lcap = lsz;
@@ -265,7 +273,13 @@ int orc_bs_contract(int dtype, orc_layout L, const void *Ldata, orc_layout R, co
     /* Lmat = block[a].permute(mapperL).reshape({-1, comm_dim}) */
     uint64_t oshape[32];
     for (int i = 0; i < rl; i++) oshape[i] = shl[i];
-    orc_permute((const char *)Ldata + L.offs[a] * es, Lbuf, es, rl, oshape, mapL, invL);
+    /* Lmat is built up front like the reference; a sampled call builds it on the first
+     * pair it takes for this left block */
+    int l_done = 0;
+    if (!count_only && stride <= 1) {
+      orc_permute((const char *)Ldata + L.offs[a] * es, Lbuf, es, rl, oshape, mapL, invL);
+      l_done = 1;
+    }
     int64_t mrows = comm_dim ? lsz / comm_dim : 0;
     for (int k = 0; k < ncomm; k++) ktup[k] = itl[comm1[k]];
     /* right blocks whose common qindices match, in ascending b (the hash-map push order) */
@@ -277,13 +291,26 @@ int orc_bs_contract(int dtype, orc_layout L, const void *Ldata, orc_layout R, co
       const int64_t *shr = R.shapes + b * rr;
       int64_t rsz = 1;
       for (int i = 0; i < rr; i++) rsz *= shr[i];
+      ++pair;
+      const int take = count_only || stride <= 1 || (pair % stride) == offset;
+      if (!take) continue;
+      if (count_only) {
+        const int64_t nc = comm_dim ? rsz / comm_dim : 0;
+        if (mrows && nc && comm_dim) fl += 2.0 * (double)mrows * (double)nc * (double)comm_dim;
+        continue;
+      }
+      if (!l_done) {
+        orc_permute((const char *)Ldata + L.offs[a] * es, Lbuf, es, rl, oshape, mapL, invL);
+        l_done = 1;
+      }
       if (rsz > rcap) {
         free(Rbuf);
         Rbuf = (char *)malloc(rsz * es);
         rcap = rsz;
       }
-      for (int i = 0; i < rr; i++) oshape[i] = shr[i];
-      orc_permute((const char *)Rdata + R.offs[b] * es, Rbuf, es, rr, oshape, mapR, invR);
+      uint64_t rshape[32];
+      for (int i = 0; i < rr; i++) rshape[i] = shr[i];
+      orc_permute((const char *)Rdata + R.offs[b] * es, Rbuf, es, rr, rshape, mapR, invR);
       int64_t ncols = comm_dim ? rsz / comm_dim : 0;
       /* Lgbuffer: output qindex tuple = nonc of a ++ nonc of b */
       for (int i = 0; i < ncl; i++) gbuf[i] = itl[nonc1[i]];
@@ -300,6 +327,7 @@ int orc_bs_contract(int dtype, orc_layout L, const void *Ldata, orc_layout R, co
       int M = (int)mrows, N = (int)ncols, K = (int)comm_dim;
       char *C = (char *)Odata + O.offs[targ] * es;
       if (K == 0) continue;
+      fl += 2.0 * (double)M * (double)N * (double)K;
       if (dtype == 3) {
         double one = 1.0;
         g_dgemm("N", "N", &N, &M, &K, &one, (double *)Rbuf, &N, (double *)Lbuf, &K, &one,
@@ -313,5 +341,12 @@ int orc_bs_contract(int dtype, orc_layout L, const void *Ldata, orc_layout R, co
   free(Lbuf);
   free(Rbuf);
   free(mpC.slot);
+  if (flops) *flops = fl;
   return 0;
+}
+
+int orc_bs_contract(int dtype, orc_layout L, const void *Ldata, orc_layout R, const void *Rdata,
+                    int ncomm, const int64_t *comm1, const int64_t *comm2, orc_layout O,
+                    void *Odata) {
+  return orc_bs_contract_ex(dtype, L, Ldata, R, Rdata, ncomm, comm1, comm2, O, Odata, 1, 0, NULL);
 }

@@ -1,7 +1,8 @@
 """Convert the reference's binary test fixtures for the hot path into small .npz files.
 
-Run in a container where the reference checkout exists (default
-/root/reference); the GPU-side tests only read the .npz files written here.
+Run where a checkout of the reference exists, giving its root as the argument (or in
+the environment variable CYTNX_REFERENCE_ROOT); the GPU-side tests only read the .npz
+files written here.
 
 Fixtures converted (the reference tests that use them):
 
@@ -72,4 +73,7 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CYTNX_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: python tests/golden/make_golden.py <reference_root> (or set CYTNX_REFERENCE_ROOT)")
+    main(root)

@@ -127,3 +127,25 @@ def test_autotune_keeps_results():
     for i, ref in enumerate(refs):
         got = y[B.psi_offsets[i]: B.psi_offsets[i] + B.psi_sizes[i]]
         assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 2e-5
+
+
+def test_batched_problems_match_oracle():
+    """Eight Hubbard problems of different D (17 .. 256): the FP64 planned matvec to
+    1e-12 and every split form's slice of the batched launch against the oracle's FP64
+    matvec of the same FP32-valued inputs (built by the oracle's own generator)."""
+    from cytnx_b200.batch import BatchedTwoSiteHeff
+    from oracle import workloads as OW
+
+    probs, data = _problems()
+    refs = [OW.heff_matvec(OW.hubbard_two_site(D, 11 + i)) for i, D in enumerate(DIMS)]
+    for got, ref in zip(_fp64_reference(probs, data), refs):
+        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-12
+    for precision, bound in (("bf16x3", 2e-5), ("3xtf32", 3e-6)):
+        B = BatchedTwoSiteHeff(probs, precision, fp32=True)
+        B.set_env(B.gather([d[0] for d in data], "L"), B.gather([d[1] for d in data], "R"))
+        x_all = B.gather([d[2] for d in data], "psi")
+        y = B.matvec(x_all, torch.zeros_like(x_all)).double().cpu().numpy()
+        for i, ref in enumerate(refs):
+            got = y[B.psi_offsets[i]: B.psi_offsets[i] + B.psi_sizes[i]]
+            err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+            assert err <= bound, (precision, DIMS[i], err)

@@ -148,11 +148,15 @@ def test_fileio_roundtrip(tmp_path):
         assert np.array_equal(a, b)
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/tests/test_data_base"), reason="reference tree absent")
+REF_ROOT = os.environ.get("CYTNX_REFERENCE_ROOT", "")
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REF_ROOT, "tests", "test_data_base")) or not REF_ROOT,
+                    reason="reference checkout not given (CYTNX_REFERENCE_ROOT)")
 def test_fileio_reads_reference_files():
     from cytnx_b200 import fileio
 
-    base = "/root/reference/tests/test_data_base/common/BlockUniTensor"
+    base = os.path.join(REF_ROOT, "tests", "test_data_base", "common", "BlockUniTensor")
     e = fileio.read_unitensor(os.path.join(base, "contract_ans3.cytnx"))
     z = load_golden("block_contract_ans3")
     assert np.array_equal(e["itoi"], z["itoi"])
