@@ -45,9 +45,16 @@ static ctn_status device_ws(double **ws) {
 // eigenvectors as ROWS, the is_row=true layout linalg::Tridiag returns
 // (src/linalg/Tridiag.cpp:83-95).  With zrows == nullptr no rotation is accumulated
 // (O(n^2) instead of O(n^3)); the eigenvalues do not depend on it and are bit-identical.
+// The sweeps run on the reversed matrix J T J (J the exchange matrix), i.e. the bulge moves
+// from the last row towards the first and rows deflate from the top: on Lanczos
+// tridiagonals this keeps the leading eigenvector components, which the Lanczos drivers
+// combine (exp(tau T) e_1, the Ritz vectors), accurate to rounding; the top-down order
+// lost up to two digits there (the stopping value |exp(tau T)[i][0]| of Lanczos_Exp then
+// stalled above 1e-14).
 static ctn_status tql(int n, const double *din, const double *ein, double *w, double *zrows) {
-  std::vector<double> d(din, din + n), e(n > 1 ? n - 1 : 1, 0.0);
-  for (int i = 0; i + 1 < n; ++i) e[i] = ein[i];
+  std::vector<double> d(n), e(n > 1 ? n - 1 : 1, 0.0);
+  for (int i = 0; i < n; ++i) d[i] = din[n - 1 - i];
+  for (int i = 0; i + 1 < n; ++i) e[i] = ein[n - 2 - i];
   // vec[j * n + k]: component k of the j-th column of the accumulated rotation product V
   // (T_input = V T_current V^T), so the two columns a rotation touches are contiguous
   std::vector<double> vec(zrows ? (size_t)n * n : 0, 0.0);
@@ -111,7 +118,10 @@ static ctn_status tql(int n, const double *din, const double *ein, double *w, do
   std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return d[a] < d[b]; });
   for (int j = 0; j < n; ++j) {
     w[j] = d[idx[j]];
-    if (zrows) std::memcpy(zrows + (size_t)j * n, &vec[(size_t)idx[j] * n], sizeof(double) * n);
+    if (zrows) {
+      const double *src = &vec[(size_t)idx[j] * n];
+      for (int k = 0; k < n; ++k) zrows[(size_t)j * n + k] = src[n - 1 - k];  // undo the reversal
+    }
   }
   return CTN_OK;
 }
