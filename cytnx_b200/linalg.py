@@ -19,7 +19,7 @@ import torch
 from . import _lib
 from ._lib import CytnxError
 from .core import Device, Tensor, Type, require_cuda
-from .svd import Gesvd, Svd, Svd_truncate  # noqa: F401
+from .svd import Gesvd, Gesvd_truncate, Svd, Svd_truncate  # noqa: F401
 from .unitensor import Contract, UniTensor, UTenType
 
 

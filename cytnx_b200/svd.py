@@ -44,23 +44,23 @@ def _row_charge(u: UniTensor, tup: Sequence[int]) -> Tuple[int, ...]:
 
 
 def _sectors(u: UniTensor):
-    """Group the blocks of a contiguous BlockUniTensor by row charge."""
+    """Group the blocks of a contiguous BlockUniTensor by row charge: sectors in ascending
+    charge order, rows and columns of a sector in ascending qindex-tuple order (the std::map
+    and vec_sort orders of Gesvd_BlockUT_internal, src/linalg/Gesvd.cpp:238-262)."""
     r = u.rowrank()
     itoi = u._layout.itoi.tolist()
     sec: Dict[tuple, dict] = {}
-    order: List[tuple] = []
     for b, t in enumerate(itoi):
         q = _row_charge(u, t)
-        if q not in sec:
-            sec[q] = {"rows": [], "cols": [], "blocks": []}
-            order.append(q)
-        s = sec[q]
+        s = sec.setdefault(q, {"rows": set(), "cols": set(), "blocks": []})
         rt, ct = tuple(t[:r]), tuple(t[r:])
-        if rt not in s["rows"]:
-            s["rows"].append(rt)
-        if ct not in s["cols"]:
-            s["cols"].append(ct)
+        s["rows"].add(rt)
+        s["cols"].add(ct)
         s["blocks"].append((b, rt, ct))
+    order = sorted(sec)
+    for q in order:
+        sec[q]["rows"] = sorted(sec[q]["rows"])
+        sec[q]["cols"] = sorted(sec[q]["cols"])
     return order, sec
 
 
@@ -152,6 +152,89 @@ def Gesvd(Tin: UniTensor, is_U: bool = True, is_vT: bool = True) -> List[UniTens
 Svd = Gesvd
 
 
+def _cut(Sall: np.ndarray, keep_dim: int, err: float, floor: int):
+    """Cut value Smin on ascending singular values: keep_dim from the top, raised past values
+    below err while more than `floor` stay (Svd_truncate.cpp:166-191); None keeps nothing."""
+    n = len(Sall)
+    if keep_dim < n:
+        smidx = n - keep_dim
+    else:
+        keep_dim, smidx = n, 0
+    smin = Sall[smidx]
+    while smin < err and keep_dim > floor:
+        keep_dim -= 1
+        if keep_dim == 0:
+            return None
+        smidx += 1
+        smin = Sall[smidx]
+    return smin
+
+
+def Gesvd_truncate(Tin: UniTensor, keepdim: int, *args, err: float = 0.0, is_U: bool = True, is_vT: bool = True,
+                   return_err: int = 0, mindim: int = 1, min_blockdim=None):
+    """linalg::Gesvd_truncate (src/linalg/Gesvd_truncate.cpp): ``Gesvd_truncate(T, keepdim, err,
+    is_U, is_vT, return_err, mindim)`` or, with a per-sector floor, ``Gesvd_truncate(T, keepdim,
+    min_blockdim, err, is_U, is_vT, return_err, mindim)`` (:430-560): the first min_blockdim[b]
+    values of sector b are kept outside the global ranking (one entry applies to every sector)."""
+    args = list(args)
+    if args and isinstance(args[0], (list, tuple, np.ndarray)):
+        min_blockdim = list(args.pop(0))
+    names = ["err", "is_U", "is_vT", "return_err", "mindim"]
+    vals = dict(err=err, is_U=is_U, is_vT=is_vT, return_err=return_err, mindim=mindim)
+    for n_, v in zip(names, args):
+        vals[n_] = v
+    err, is_U, is_vT, return_err, mindim = (vals[n_] for n_ in names)
+    if min_blockdim is None:
+        res = Svd_truncate(Tin, keepdim, err, True, return_err, mindim)
+        S, U, Vt = res[:3]
+        out = [S] + ([U] if is_U else []) + ([Vt] if is_vT else [])
+        return out + res[3:]
+    u, parts = _svd_blocks(Tin)
+    nb = len(parts)
+    mb = [int(x) for x in min_blockdim]
+    if len(mb) == 1:
+        mb = mb * nb
+    if len(mb) != nb:
+        raise CytnxError("[ERROR][Gesvd_truncate] min_blockdim must have the same number of elements as blocks "
+                         "in the singular value UniTensor")
+    keep_dim, min_dim = int(keepdim), max(1, int(mindim))
+    rest, any_mb = [], False
+    for b, p in enumerate(parts):
+        v = p[7].cpu().numpy()
+        if mb[b] < 1:
+            rest.append(v)
+            continue
+        any_mb = True
+        if len(v) <= mb[b]:
+            keep_dim -= len(v)
+            min_dim -= len(v)
+            continue
+        rest.append(v[mb[b]:])
+        keep_dim -= mb[b]
+        min_dim -= mb[b]
+    smin = None
+    Srest = np.sort(np.concatenate(rest)) if rest else np.zeros(0)
+    if rest and keep_dim > 0:
+        min_dim = max(1, min_dim) if not any_mb else max(0, min_dim)
+        smin = _cut(Srest, keep_dim, err, min_dim)
+    keep = []
+    for b, p in enumerate(parts):
+        v = p[7].cpu().numpy()
+        k = min(mb[b], len(v))
+        if smin is not None:
+            above = np.nonzero(v[mb[b]:] >= smin)[0]
+            if len(above):
+                k = mb[b] + int(above[-1]) + 1
+        keep.append(k)
+    res = _assemble(u, parts, keep, is_U, is_vT)
+    if return_err:
+        dropped = np.sort(np.concatenate([p[7].cpu().numpy()[k:] for p, k in zip(parts, keep)])) \
+            if parts else np.zeros(0)
+        e = float(dropped.max()) if return_err == 1 and len(dropped) else 0.0
+        res.append(Tensor.from_numpy(np.array([e]), -1) if return_err == 1 else Tensor.from_numpy(dropped[::-1], -1))
+    return res
+
+
 def Svd_truncate(Tin: UniTensor, keepdim: int, err: float = 0.0, is_UvT: bool = True, return_err: int = 0,
                  mindim: int = 1):
     """Truncated block SVD keeping the ``keepdim`` largest singular values overall."""
@@ -169,7 +252,7 @@ def Svd_truncate(Tin: UniTensor, keepdim: int, err: float = 0.0, is_UvT: bool = 
         keep_dim -= 1
         smidx += 1
         Smin = Sall[smidx]
-    keep = [int((p[7] >= Smin).sum().item()) for p in parts]
+    keep = [int((p[7] >= float(Smin)).sum().item()) for p in parts]
     # an exact degeneracy at the cut stays whole (values >= Smin are kept)
     res = _assemble(u, parts, keep, is_UvT, is_UvT)
     if return_err:

@@ -11,6 +11,9 @@ Fixtures converted (the reference tests that use them):
 * DenseUniTensor denseutensor{1,2}, densecontres{1,2,3}, densepermu{1,2}
                                                -- tests/DenseUniTensor_test.cpp:2594-2619
 * linalg/Lanczos_Gnd lan_block_{A,B,C}         -- tests/linalg_test/Lanczos_Gnd_test.cpp:102-125,392-445
+* linalg/Svd_truncate Svd_truncate1 + S_truncate1 -- tests/linalg_test/linalg_test.h:78-83, linalg_test.cpp:57-67
+* common/sym_UT_U1_exp_Svals_F64 with its linalg/Svd_truncate answers (singular values, reconstructed
+  tensor, and the min_blockdim variants)       -- tests/linalg_test/Gesvd_truncate_test.cpp:107-135, 187-270
 
 Usage:  python tests/golden/make_golden.py [reference_root]
 """
@@ -66,6 +69,18 @@ def main(ref_root: str) -> None:
         u = fileio.read_unitensor(src)
         np.savez_compressed(os.path.join(HERE, dst + ".npz"), **pack_unitensor(u))
         print("wrote", dst)
+    sdir = os.path.join(base, "linalg", "Svd_truncate")
+    jobs_svd = [(os.path.join(sdir, "Svd_truncate1.cytnx"), "svd_truncate1_T"),
+                (os.path.join(base, "common", "sym_UT_U1_exp_Svals_F64.cytnx"), "svd_u1_exp_src")]
+    for suffix in ["", "_reconstructed", "_minblockdim", "_minblockdim_reconstructed"]:
+        jobs_svd.append((os.path.join(sdir, f"sym_UT_U1_exp_Svals_F64{suffix}.cytnx"), f"svd_u1_exp_ans{suffix}"))
+    for src, dst in jobs_svd:
+        u = fileio.read_unitensor(src)
+        np.savez_compressed(os.path.join(HERE, dst + ".npz"), **pack_unitensor(u))
+        print("wrote", dst)
+    np.savez_compressed(os.path.join(HERE, "svd_truncate1_S.npz"),
+                        S=fileio.read_tensor(os.path.join(sdir, "S_truncate1.cytn")))
+    print("wrote svd_truncate1_S")
     ldir = os.path.join(base, "linalg", "Lanczos_Gnd")
     lan = {k: fileio.read_tensor(os.path.join(ldir, f"lan_block_{k}.cytn")) for k in "ABC"}
     np.savez_compressed(os.path.join(HERE, "lanczos_blocks.npz"), **lan)
