@@ -517,7 +517,8 @@ def main():
                  "kernel_flops_per_matvec": g_flops, "kernel_ms_per_matvec": g_ms})
     clocks = sampler.summary()
     permute = run_permute(args, dev, st, pk.get("hbm_gbs"))
-    fp64_d1024 = run_fp64_d1024(args, dev, st)
+    fp64_d1024 = run_fp64_d1024(args, dev, st, dgemm_tflops, rank)
+    config1 = run_config1(args, dev, st, dgemm_tflops) if rank == 0 else None
     batched = run_batched(args, world, rank, dev, st) if args.batch_problems > 0 else None
     mps_ad = run_mps_autograd(args, dev) if args.mps_lbfgs_steps > 0 else None
     if rank == 0:
@@ -561,6 +562,7 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cpu,
             "permute": permute,
+            "dense_single_site_D64": config1,
             "fp64_D1024": fp64_d1024,
             "batched_hubbard": batched,
             "autograd_mps": mps_ad,
@@ -653,10 +655,28 @@ def run_batched(args, world, rank, dev, st):
         gf = torch.tensor([B.gemm_flops()], dtype=torch.float64, device=dev)
         if world > 1:
             dist.all_reduce(gf)
+        gst = B.gemm_stats()
+        # algorithmic bytes: every problem's FP32 environments and vector read once, the result
+        # written once; the GEMM panels (hi + lo) are the implementation's operand traffic
+        alg_bytes = 4.0 * sum(L_._layout.nelem + R_._layout.nelem + 2 * P_._layout.nelem
+                              for (L_, _, _, R_, P_) in probs)
         out["forms"][form] = {"ms_per_batch": ms, "matvecs_per_s": args.batch_problems / (ms * 1e-3),
                               "useful_tflops": float(gf.item()) / (ms * 1e-3) / 1e12, "phase_ms": ph,
                               "tiles": [tune["step1"], tune["step4"]], "graph_replay": True,
-                              "launches_per_batch": 4, "workspace_gb": B.workspace_bytes() / 1e9, "_B": B, "_y": y}
+                              "launches_per_batch": 4, "workspace_gb": B.workspace_bytes() / 1e9,
+                              "gemm_stats_rank0": gst,
+                              "roofline": {
+                                  "algorithmic_bytes_per_batch_rank0": alg_bytes,
+                                  "step4_panel_bytes_over_operand_bytes":
+                                      gst["step4"]["panel_bytes"] / max(1.0, gst["step4"]["operand_bytes"]),
+                                  "step1_panel_bytes_over_operand_bytes":
+                                      gst["step1"]["panel_bytes"] / max(1.0, gst["step1"]["operand_bytes"]),
+                                  "executed_over_useful_flops": (gst["step1"]["executed_flops"] +
+                                                                 gst["step4"]["executed_flops"]) /
+                                                                (gst["step1"]["useful_flops"] +
+                                                                 gst["step4"]["useful_flops"]),
+                                  "step4_ms": ph[3], "step4_panel_GB_s": gst["step4"]["panel_bytes"] / (ph[3] * 1e-3) / 1e9},
+                              "_B": B, "_y": y}
     # per-problem error of each form against the FP64 planned matvec of the same (FP32-valued) inputs
     errs = {f: [] for f in out["forms"]}
     for i, ((L, M1, M2, R, psi), (l, r, x)) in enumerate(zip(probs, data)):
@@ -690,17 +710,47 @@ def run_batched(args, world, rank, dev, st):
         rec["rel_err_vs_fp64_max"] = float(mx.item())
         rec["rel_err_vs_fp64_median_rank0"] = float(e.median().item())
         del rec["_B"], rec["_y"]
+    if rank == 0 and os.environ.get("CTN_BENCH_NO_CPU") != "1":
+        # CPU baseline: the oracle's FP64 matvec (BlockUniTensor::contract restated, OpenBLAS, all
+        # host threads) looping over problems of this batch for ~10 s; the batch time is the
+        # sampled time scaled by the batch's algorithmic flops over the sample's
+        import oracle as O
+        from oracle import workloads as OW
+
+        O.set_threads(os.cpu_count() or 1)
+        t_c, f_c, done, t0 = 0.0, 0.0, [], time.perf_counter()
+        for i in range(len(mine)):
+            ops = OW.hubbard_two_site(dims[mine[i]], 1000 + mine[i])
+            ta = time.perf_counter()
+            OW.heff_matvec(ops)
+            t_c += time.perf_counter() - ta
+            f_c += OW.heff_flops(ops)
+            done.append(int(mine[i]))
+            if time.perf_counter() - t0 > 10.0:
+                break
+        out["cpu_baseline"] = {"matvecs_per_s": len(done) / t_c, "tflops": f_c / t_c / 1e12,
+                               "sampled_problems": done, "sampled_D": [int(dims[i]) for i in done],
+                               "batch_mean_D": float(np.mean(dims)), "seconds": t_c, "flops": f_c,
+                               "cores": os.cpu_count() or 1, "kind": "port",
+                               "sample": "oracle FP64 matvecs (BlockUniTensor::contract restated, OpenBLAS dgemm) "
+                                         "over the first problems of the batch for about 10 s"}
     out["setup_s"] = time.perf_counter() - t_setup
     return out
 
 
-def run_fp64_d1024(args, dev, st):
+def run_fp64_d1024(args, dev, st, dgemm_tflops, rank):
     """Plain FP64 U(1) configuration: two-site XXZ H_eff at D=1024, 40 Lanczos iterations
     (the reference's Gnd recurrence) and the block SVD truncation of the ground state back
-    to D (Svd_truncate, rowrank 2: (a, s1) | (s2, b))."""
+    to D (Svd_truncate, rowrank 2: (a, s1) | (s2, b)).  Roofline: the grouped FP64 DMMA GEMMs
+    of steps 1 and 4 against the measured cuBLAS DGEMM.  CPU baseline (rank 0): the oracle's
+    matvec (BlockUniTensor::contract restated, OpenBLAS), its Lanczos_Gnd_Ut and its block
+    Svd_truncate on all host threads."""
+    import ctypes
+
     import torch
 
     import cytnx_b200 as c
+    from cytnx_b200 import _lib
     from cytnx_b200 import workloads as W
 
     spec = W.xxz_spec(1024)
@@ -721,6 +771,12 @@ def run_fp64_d1024(args, dev, st):
     e1.record(st)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / reps
+    ph = (ctypes.c_double * 4)()
+    nl = ctypes.c_int()
+    _lib.check(_lib.lib().ctn_heff2_profile(H._h, x.data_ptr(), y.data_ptr(), 0, 20, ph, ctypes.byref(nl),
+                                           _lib.stream_ptr()), "profile")
+    g_flops = _lib.lib().ctn_heff2_gemm_flops(H._h, 1) + _lib.lib().ctn_heff2_gemm_flops(H._h, 4)
+    g_ms = ph[1] + ph[3]
     H.lanczos(psi, maxiter=4, cvgcrit=1e-300)  # warm
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -736,10 +792,143 @@ def run_fp64_d1024(args, dev, st):
     t_svd = time.perf_counter() - t0
     s = S.flat_view()
     kept = int(S.shape()[0])
-    return {"workload": "u1_xxz_two_site_heff_D1024_fp64", "algorithmic_flops_per_matvec": flops,
-            "matvec_ms": ms, "matvec_tflops": flops / (ms * 1e-3) / 1e12, "lanczos_iters": it,
-            "lanczos_s_per_step": t_lan / max(it, 1), "energy_40": E, "svd_truncate_s": t_svd,
-            "svd_kept": kept, "svd_norm2_kept": float((s * s).sum().item())}
+    out = {"workload": "u1_xxz_two_site_heff_D1024_fp64", "algorithmic_flops_per_matvec": flops,
+           "matvec_ms": ms, "matvec_tflops": flops / (ms * 1e-3) / 1e12, "phase_ms": [ph[i] for i in range(4)],
+           "lanczos_iters": it, "lanczos_s_per_step": t_lan / max(it, 1), "energy_40": E,
+           "svd_truncate_s": t_svd, "svd_kept": kept, "svd_norm2_kept": float((s * s).sum().item()),
+           "roofline": {"bound": "fp64 tensor (DMMA)", "kernel": "k_gemm_grouped_f64 (steps 1 and 4)",
+                        "achieved": g_flops / (g_ms * 1e-3) / 1e12, "peak": dgemm_tflops, "unit": "TFLOP/s",
+                        "frac": g_flops / (g_ms * 1e-3) / 1e12 / dgemm_tflops,
+                        "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                        "kernel_flops_per_matvec": g_flops, "kernel_ms_per_matvec": g_ms}}
+    if rank == 0 and os.environ.get("CTN_BENCH_NO_CPU") != "1":
+        import oracle as O
+        from oracle import svd as OS
+        from oracle import workloads as OW
+
+        O.set_threads(os.cpu_count() or 1)
+        ops = OW.xxz_two_site(1024, seed=0)
+        outs = OW.heff_chain(ops)
+        n, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < 3.0:
+            OW.heff_chain(ops, outs=outs)
+            n += 1
+        cpu_mv = (time.perf_counter() - t0) / n
+        t0 = time.perf_counter()
+        E_o, v_o, it_o = O.lanczos_gnd_ut(lambda z: OW.heff_matvec(ops, z), ops["psi"].flat(), 1e-300, 40)
+        cpu_lan = (time.perf_counter() - t0) / it_o
+        vo = OW.with_psi(ops, v_o)["psi"]
+        vo = O.BlockTensor(vo.bonds, vo.labels, 2, vo.itoi, vo.blocks)
+        t0 = time.perf_counter()
+        So, _, _, _ = OS.svd_truncate(vo, 1024)
+        cpu_svd = time.perf_counter() - t0
+        out["energy_40_oracle"] = E_o
+        out["dE_rel_vs_oracle"] = abs(E - E_o) / abs(E_o)
+        out["cpu_baseline"] = {"matvec_ms": cpu_mv * 1e3, "matvec_tflops": flops / cpu_mv / 1e12,
+                               "lanczos_s_per_step": cpu_lan, "svd_truncate_s": cpu_svd,
+                               "cores": os.cpu_count() or 1, "kind": "port",
+                               "sample": f"{n} oracle matvecs (3 s), 40 oracle Lanczos_Gnd_Ut iterations, one "
+                                         "oracle block Svd_truncate (numpy LAPACK per sector)"}
+    return out
+
+
+def run_config1(args, dev, st, dgemm_tflops):
+    """Plain dense FP64 single-site configuration: L[64,5,64], R[64,5,64] (symmetrised over the
+    two bond indices), the XXZ MPO W[5,5,2,2], A[64,2,64]; the matvec through Network / LinOp
+    (the drop-in path) and 30 iterations of linalg.Lanczos("Gnd").  CPU baseline: the same
+    matvec as three oracle Tensordot calls (Tensordot.cpp:29-110, OpenBLAS dgemm, all host
+    threads) inside the oracle's Lanczos_Gnd_Ut restatement."""
+    import torch
+
+    import cytnx_b200 as c
+    import oracle as O
+    from cytnx_b200 import workloads as W
+
+    D = 64
+    rng = np.random.default_rng(0)
+    L = rng.standard_normal((D, 5, D))
+    L = 0.5 * (L + L.transpose(2, 1, 0))
+    R = rng.standard_normal((D, 5, D))
+    R = 0.5 * (R + R.transpose(2, 1, 0))
+    Wm = np.zeros((5, 5, 2, 2))
+    for (a, b, s_, sp), v in W.xxz_mpo_values(1.0, 1.0, 0.0).items():
+        Wm[a, b, s_, sp] = v
+    A = rng.standard_normal((D, 2, D))
+    A /= np.linalg.norm(A)
+    Lu = c.UniTensor(c.Tensor.from_torch(torch.from_numpy(L).to(dev)), False, -1, ["a", "w", "ap"])
+    Ru = c.UniTensor(c.Tensor.from_torch(torch.from_numpy(R).to(dev)), False, -1, ["b", "w2", "bp"])
+    Wu = c.UniTensor(c.Tensor.from_torch(torch.from_numpy(Wm).to(dev)), False, -1, ["w", "w2", "s", "sp"])
+    Au = c.UniTensor(c.Tensor.from_torch(torch.from_numpy(A).to(dev)), False, -1, ["a", "s", "b"])
+
+    class OneSite(c.LinOp):
+        def __init__(self):
+            super().__init__("mv", A.size, c.Type.Double, c.Device.cuda)
+            self.net = c.Network()
+            self.net.FromString(["A: a,s,b", "L: a,w,ap", "W: w,w2,s,sp", "R: b,w2,bp", "TOUT: ap,sp,bp"])
+            self.net.PutUniTensors(["L", "W", "R"], [Lu, Wu, Ru])
+
+        def matvec(self, v):
+            lbl = v.labels()
+            self.net.PutUniTensor("A", v)
+            out = self.net.Launch()
+            out.relabel_(lbl)
+            return out
+
+    H = OneSite()
+    # flops of the three pairwise contractions (L.A over a; .W over (w, s); .R over (b, w2))
+    flops = 2.0 * (5 * D) * (2 * D) * D + 2.0 * (D * D) * (5 * 2) * (5 * 2) + 2.0 * (D * 2) * D * (D * 5)
+    for _ in range(5):
+        H.matvec(Au)
+    torch.cuda.synchronize()
+    reps = 200
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(st)
+    for _ in range(reps):
+        H.matvec(Au)
+    e1.record(st)
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) / reps
+    dev_ms = e0.elapsed_time(e1) / reps
+    c.linalg.Lanczos(Hop=H, Tin=Au, method="Gnd", Maxiter=30, CvgCrit=1e-300)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    E, _ = c.linalg.Lanczos(Hop=H, Tin=Au, method="Gnd", Maxiter=30, CvgCrit=1e-300)
+    torch.cuda.synchronize()
+    lan_s = (time.perf_counter() - t0) / 30
+    # CPU: the reference's dense path (three Tensordot calls) and its Lanczos
+    O.set_threads(os.cpu_count() or 1)
+
+    def mv(x):
+        a = x.reshape(D, 2, D)
+        t = O.tensordot(L, a, [0], [0])            # [w, ap, s, b]
+        t = O.tensordot(t, Wm, [0, 2], [0, 2])      # [ap, b, w2, sp]
+        t = O.tensordot(t, R, [1, 2], [0, 1])       # [ap, sp, bp]
+        return t.reshape(-1)
+
+    mv(A.reshape(-1))
+    n, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < 2.0:
+        mv(A.reshape(-1))
+        n += 1
+    cpu_mv = (time.perf_counter() - t0) / n
+    t0 = time.perf_counter()
+    E_ref, _, it = O.lanczos_gnd_ut(mv, A.reshape(-1), 1e-300, 30)
+    cpu_lan = (time.perf_counter() - t0) / it
+    return {"workload": "dense_fp64_single_site_D64", "algorithmic_flops_per_matvec": flops,
+            "matvec_ms_wall": wall * 1e3, "matvec_ms_device": dev_ms,
+            "matvec_gflops_wall": flops / wall / 1e9,
+            "lanczos_iters": 30, "lanczos_s_per_step": lan_s, "energy_30": float(E.item()),
+            "energy_30_oracle": float(E_ref), "dE_rel_vs_oracle": abs(float(E.item()) - E_ref) / abs(E_ref),
+            "roofline": {"bound": "launch / host latency (1.1e7 flops per matvec through three "
+                                  "Network contractions)",
+                         "achieved_tflops": flops / (dev_ms * 1e-3) / 1e12, "peak_tflops": dgemm_tflops,
+                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                         "frac": flops / (dev_ms * 1e-3) / 1e12 / dgemm_tflops},
+            "cpu_baseline": {"matvec_ms": cpu_mv * 1e3, "matvec_gflops": flops / cpu_mv / 1e9,
+                             "lanczos_s_per_step": cpu_lan, "cores": os.cpu_count() or 1, "kind": "port",
+                             "sample": "the matvec as three oracle Tensordot calls (permute + OpenBLAS dgemm) "
+                                       "for 2 s, then 30 iterations of the oracle Lanczos_Gnd_Ut"}}
 
 
 def run_permute(args, dev, st, hbm_peak, reps=None, small=True):
@@ -782,8 +971,57 @@ def run_permute(args, dev, st, hbm_peak, reps=None, small=True):
     for perm in itertools.permutations(range(4)) if small else ():
         ms, _ = timed(x, perm, reps or 200)
         tot += ms
+    if small:
+        # device-only time of the 24 launches: the same calls captured once in a CUDA graph
+        ys = [torch.empty_like(x) for _ in range(24)]
+        osh = np.array(x.shape, dtype=np.uint64)
+        mps_ = [np.array(p, dtype=np.uint64) for p in itertools.permutations(range(4))]
+        gs = torch.cuda.Stream()
+        gs.wait_stream(torch.cuda.current_stream())
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(gs):
+            for y, mp in zip(ys, mps_):  # warm outside the capture
+                _lib.check(lib.ctn_permute(x.data_ptr(), y.data_ptr(), 3, 4, osh.ctypes.data_as(_lib.P_u64),
+                                           mp.ctypes.data_as(_lib.P_u64), _lib.stream_ptr()), "permute")
+            with torch.cuda.graph(graph, stream=gs):
+                for y, mp in zip(ys, mps_):
+                    _lib.check(lib.ctn_permute(x.data_ptr(), y.data_ptr(), 3, 4, osh.ctypes.data_as(_lib.P_u64),
+                                               mp.ctypes.data_as(_lib.P_u64), _lib.stream_ptr()), "permute")
+        torch.cuda.synchronize()
+        for _ in range(3):
+            graph.replay()
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        nrep = 50
+        g0.record(st)
+        for _ in range(nrep):
+            graph.replay()
+        g1.record(st)
+        torch.cuda.synchronize()
+        dev_us = g0.elapsed_time(g1) / nrep / 24 * 1e3
+        for y, mp in zip(ys, mps_):
+            if not torch.equal(y.reshape(-1), x.permute(*[int(v) for v in mp]).contiguous().reshape(-1)):
+                raise RuntimeError("graph-replayed permute mismatch")
+        del graph
+        # CPU baseline: the oracle's Movemem_cpu loop on the same 24 permutations
+        import oracle as O
+
+        xh = x.cpu().numpy()
+        t0 = time.perf_counter()
+        nrep_c = 20
+        for _ in range(nrep_c):
+            for p in itertools.permutations(range(4)):
+                O.permute(xh, p)
+        cpu_us = (time.perf_counter() - t0) / (nrep_c * 24) * 1e6
     out["small"] = {"shape": [64, 2, 2, 64], "dtype": "f64", "perms": 24, "total_ms_24": tot,
                     "mean_us_per_perm": tot / 24 * 1e3, "bytes_per_perm": 2 * x.numel() * 8}
+    if small:
+        out["small"].update({"device_us_per_perm_graph": dev_us,
+                             "device_GB_s_graph": 2 * x.numel() * 8 / (dev_us * 1e-6) / 1e9,
+                             "note": "mean_us_per_perm is host-issued (ctypes call + launch each); the graph "
+                                     "figure is the same 24 launches replayed from one CUDA graph",
+                             "cpu_baseline_us_per_perm": cpu_us,
+                             "cpu_baseline": "oracle restatement of Movemem_cpu.cpp:152-191 (1 thread)"})
     for shape, perm, dt in (((2048, 4, 4, 2048), (3, 1, 2, 0), torch.float64),
                             ((2048, 4, 4, 2048), (0, 2, 1, 3), torch.float64),
                             ((2048, 4, 4, 2048), (1, 0, 3, 2), torch.float64),

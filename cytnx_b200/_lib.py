@@ -76,6 +76,7 @@ _SIGS = {
     "ctn_split_gemm_workspace_bytes": (c_size, [c_i64, c_i64, c_i64, c_int]),
     "ctn_split_gemm_f64": (c_int, [c_i64, c_i64, c_i64, c_vp, c_vp, c_vp, c_int, c_vp, c_vp]),
     "ctn_split_gemm_f64_noalloc": (c_int, [c_i64, c_i64, c_i64, c_vp, c_vp, c_vp, c_int, c_vp]),
+    "ctn_selftest_wait_timeout": (c_int, [c_int, ctypes.c_longlong, c_vp]),
     "ctn_dot_f64": (c_int, [c_vp, c_vp, c_i64, c_vp, c_vp]),
     "ctn_nrm2_f64": (c_int, [c_vp, c_i64, c_vp, c_vp]),
     "ctn_axpy_f64": (c_int, [c_vp, c_vp, c_i64, c_vp, c_dbl, c_vp]),
@@ -93,10 +94,12 @@ _SIGS = {
     "ctn_heff2_profile": (c_int, [c_vp, c_vp, c_vp, c_int, c_int, P_dbl, ctypes.POINTER(c_int), c_vp]),
     "ctn_heff2_gemm_flops": (c_dbl, [c_vp, c_int]),
     "ctn_heff2_split_gemm_flops": (c_dbl, [c_vp, c_int, c_int]),
+    "ctn_heff2_split_stats": (c_int, [c_vp, c_int, ctypes.POINTER(c_dbl)]),
     "ctn_heff2_batch_create": (c_int, [ctypes.POINTER(c_vp), c_int, P_i64, P_i64, P_i64, c_int, c_int, c_int, c_int,
                                        ctypes.POINTER(c_vp)]),
     "ctn_heff2_batch_workspace_bytes": (c_size, [c_vp]),
     "ctn_heff2_batch_gemm_flops": (c_dbl, [c_vp]),
+    "ctn_heff2_batch_stats": (c_int, [c_vp, ctypes.POINTER(c_dbl)]),
     "ctn_heff2_batch_set_env": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp]),
     "ctn_heff2_batch_matvec": (c_int, [c_vp, c_vp, c_vp, c_vp]),
     "ctn_heff2_batch_profile": (c_int, [c_vp, c_vp, c_vp, c_int, P_dbl, c_vp]),

@@ -137,6 +137,15 @@ class BatchedTwoSiteHeff:
         """Useful flops (2*M*N*K over every problem's stacked GEMM groups) of one batched matvec."""
         return float(_lib.lib().ctn_heff2_batch_gemm_flops(self._b))
 
+    def gemm_stats(self) -> dict:
+        """Work accounting of the two batched GEMMs (ctn_heff2_batch_stats): useful flops,
+        executed MMA flops of the tiles (padding included, one product each) and the operand
+        panel bytes the tiles copy into shared memory per matvec."""
+        out = (ctypes.c_double * 8)()
+        _lib.check(_lib.lib().ctn_heff2_batch_stats(self._b, out), "BatchedTwoSiteHeff.gemm_stats")
+        return {f"step{s}": {"useful_flops": out[i], "executed_flops": out[i + 1], "panel_bytes": out[i + 2],
+                             "operand_bytes": out[i + 3]} for s, i in ((1, 0), (4, 4))}
+
     def plan(self, i: int) -> int:
         return self._plans[i]
 

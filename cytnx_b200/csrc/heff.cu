@@ -560,6 +560,12 @@ extern "C" double ctn_heff2_gemm_flops(const ctn_heff2_plan *p, int step) {
   return step == 1 ? p->g1.flops : step == 4 ? p->g4.flops : 0.0;
 }
 
+extern "C" ctn_status ctn_heff2_split_stats(ctn_heff2_plan *p, int precision, double *out) {
+  CTN_REQUIRE(p && out, "ctn_heff2_split_stats: null argument");
+  const int k = split_kind(precision);
+  CTN_TRY(ctn::heff_split_prepare(p, k));
+  return ctn::heff_split_stats(p, k, out);
+}
 extern "C" double ctn_heff2_split_gemm_flops(ctn_heff2_plan *p, int precision, int step) {
   const int k = split_kind(precision);
   if (ctn::heff_split_prepare(p, k) != CTN_OK) return 0.0;

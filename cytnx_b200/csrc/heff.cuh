@@ -60,6 +60,7 @@ ctn_status heff_split_matvec_f32out(struct ::ctn_heff2_plan *p, int kind, const 
                                     cudaStream_t st);
 void heff_split_free(HeffSplit *s);
 double heff_split_gemm_flops(const struct ::ctn_heff2_plan *p, int kind, int step);
+ctn_status heff_split_stats(const struct ::ctn_heff2_plan *p, int kind, double *out);
 void heff_split_apply_epilogue(struct ::ctn_heff2_plan *p, int kind);
 }  // namespace ctn
 

@@ -45,6 +45,7 @@ struct WorkItem {
   int64_t chunk0;      // global chunk index of the item's first chunk
 };
 
+
 struct HeffSplit {
   int kind = TC_TF32;
   std::vector<WorkItem> items;
@@ -58,7 +59,7 @@ struct HeffSplit {
   int d_dev = -1;
   int64_t x1_elems = 0;
   // workspace layout (bytes)
-  int64_t o_a1h, o_a1l, o_b1h, o_b1l, o_x1, o_a4h, o_a4l, o_b4h, o_b4l, o_err, total;
+  int64_t o_a1, o_b1, o_x1, o_a4, o_b4, o_err, total;  // panels hold hi and lo tiles interleaved
   std::vector<std::pair<int64_t, int64_t>> uncovered;  // out ranges no group writes (zero them)
   uint8_t *ws = nullptr;
   int in_f32 = 0;   // psi / L / R given in FP32 (batched form) instead of FP64
@@ -75,7 +76,7 @@ constexpr int KALIGN = 8;
 
 int64_t up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
-// workspace layout (bytes): [A1 hi|lo][B1 hi|lo][X1 f32][A4 hi|lo][B4 hi|lo][error word]
+// workspace layout (bytes): [A1 panel][B1 panel][X1 f32][A4 panel][B4 panel][error word]
 void split_layout(HeffSplit *s) {
   int64_t o = 0;
   auto take = [&](int64_t bytes) {
@@ -83,15 +84,11 @@ void split_layout(HeffSplit *s) {
     o = up(o + bytes, 1024);
     return at;
   };
-  s->o_a1h = take(s->g1.a_bytes);
-  s->o_a1l = take(s->g1.a_bytes);
-  s->o_b1h = take(s->g1.b_bytes);
-  s->o_b1l = take(s->g1.b_bytes);
+  s->o_a1 = take(s->g1.a_bytes);
+  s->o_b1 = take(s->g1.b_bytes);
   s->o_x1 = take(s->x1_elems * 4);
-  s->o_a4h = take(s->g4.a_bytes);
-  s->o_a4l = take(s->g4.a_bytes);
-  s->o_b4h = take(s->g4.b_bytes);
-  s->o_b4l = take(s->g4.b_bytes);
+  s->o_a4 = take(s->g4.a_bytes);
+  s->o_b4 = take(s->g4.b_bytes);
   s->o_err = take(256);
   s->total = o;
 }
@@ -140,8 +137,8 @@ __device__ __forceinline__ void mpo_store(const float (&x)[8], const MpoSegS &s,
   const int rr = row & (TC_BM - 1);
   const int kslice = TF ? (kabs >> 5) : (kabs >> 6);
   const int byte = TF ? ((kabs & 31) << 2) : ((kabs & 63) << 1);
-  const int64_t off = s.panel_off + ((int64_t)(row >> 7) * s.kb + kslice) * TC_A_TILE + (rr >> 3) * 1024 +
-                      (rr & 7) * 128 + (((byte >> 4) ^ (rr & 7)) << 4);
+  const int64_t off = s.panel_off + ((int64_t)(row >> 7) * s.kb + kslice) * (2 * TC_A_TILE) + (rr >> 3) * 1024 +
+                      (rr & 7) * 128 + (((byte >> 4) ^ (rr & 7)) << 4);  // hi tile; lo = hi + TC_A_TILE
   if (TF) {
     float h[4], l[4];
 #pragma unroll
@@ -423,6 +420,14 @@ void heff_split_apply_epilogue(ctn_heff2_plan *p, int kind) {
   s->g4.epi_staged = p->split_epi[kind][1] < 0 ? s->g4.epi_auto : p->split_epi[kind][1] != 0;
 }
 
+ctn_status heff_split_stats(const ctn_heff2_plan *p, int kind, double *out) {
+  const HeffSplit *s = p->split[kind];
+  CTN_REQUIRE(s, "ctn_heff2_split_stats: precision not prepared");
+  s->g1.stats(out);
+  s->g4.stats(out + 4);
+  return CTN_OK;
+}
+
 double heff_split_gemm_flops(const ctn_heff2_plan *p, int kind, int step) {
   const HeffSplit *s = p->split[kind];
   if (!s) return 0.0;
@@ -437,8 +442,8 @@ ctn_status split_set_env(HeffSplit *s, const void *L, const void *R, void *ws, c
   CTN_REQUIRE(s, "heff split: not prepared");
   s->ws = (uint8_t *)ws;
   CTN_CUDA(cudaMemsetAsync(ws, 0, s->total, st));
-  CTN_TRY(s->pk_L.run(L, s->in_f32, s->ws + s->o_a1h, s->ws + s->o_a1l, st));
-  CTN_TRY(s->pk_R.run(R, s->in_f32, s->ws + s->o_b4h, s->ws + s->o_b4l, st));
+  CTN_TRY(s->pk_L.run(L, s->in_f32, s->ws + s->o_a1, st));
+  CTN_TRY(s->pk_R.run(R, s->in_f32, s->ws + s->o_b4, st));
   // device copy of the MPO segment tables
   int dev = 0;
   CTN_CUDA(cudaGetDevice(&dev));
@@ -482,10 +487,10 @@ ctn_status split_matvec(HeffSplit *s, const void *psi, void *out, cudaStream_t s
     for (auto &e : ev) CTN_CUDA(cudaEventCreate(&e));
   if (ms4) CTN_CUDA(cudaEventRecord(ev[0], st));
   for (auto &u : s->uncovered) CTN_CUDA(cudaMemsetAsync((char *)out + u.first * oes, 0, u.second * oes, st));
-  CTN_TRY(s->pk_P.run(psi, s->in_f32, w + s->o_b1h, w + s->o_b1l, st));
+  CTN_TRY(s->pk_P.run(psi, s->in_f32, w + s->o_b1, st));
   if (ms4) CTN_CUDA(cudaEventRecord(ev[1], st));
   int *err = (int *)(w + s->o_err);
-  CTN_TRY(s->g1.run(w + s->o_a1h, w + s->o_a1l, w + s->o_b1h, w + s->o_b1l, (float *)(w + s->o_x1), nullptr, err, st));
+  CTN_TRY(s->g1.run(w + s->o_a1, w + s->o_b1, (float *)(w + s->o_x1), nullptr, err, st));
   if (ms4) CTN_CUDA(cudaEventRecord(ev[2], st));
   if (!s->items.empty()) {
     MpoSParams prm;
@@ -499,8 +504,8 @@ ctn_status split_matvec(HeffSplit *s, const void *psi, void *out, cudaStream_t s
     prm.nchunks = s->nchunks;
     prm.kind = kind;
     prm.x1 = (const float *)(w + s->o_x1);
-    prm.hi = w + s->o_a4h;
-    prm.lo = w + s->o_a4l;
+    prm.hi = w + s->o_a4;
+    prm.lo = w + s->o_a4 + tc_lo_delta(TC_BM);
     // four waves of resident CTAs: items of uneven size balance through the CTA scheduler
     auto launch = [&](auto kern) -> void {
       const int64_t grid = std::min<int64_t>(prm.nitems, (int64_t)nsm_count() * resident_ctas(kern, MPO_THREADS) * 4);
@@ -512,9 +517,9 @@ ctn_status split_matvec(HeffSplit *s, const void *psi, void *out, cudaStream_t s
   }
   if (ms4) CTN_CUDA(cudaEventRecord(ev[3], st));
   if (o32)
-    CTN_TRY(s->g4.run(w + s->o_a4h, w + s->o_a4l, w + s->o_b4h, w + s->o_b4l, (float *)out, nullptr, err, st));
+    CTN_TRY(s->g4.run(w + s->o_a4, w + s->o_b4, (float *)out, nullptr, err, st));
   else
-    CTN_TRY(s->g4.run(w + s->o_a4h, w + s->o_a4l, w + s->o_b4h, w + s->o_b4l, nullptr, (double *)out, err, st));
+    CTN_TRY(s->g4.run(w + s->o_a4, w + s->o_b4, nullptr, (double *)out, err, st));
   if (ms4) {
     CTN_CUDA(cudaEventRecord(ev[4], st));
     CTN_CUDA(cudaEventSynchronize(ev[4]));
@@ -660,6 +665,12 @@ extern "C" ctn_status ctn_heff2_batch_create(ctn_heff2_plan *const *plans, int n
   return CTN_OK;
 }
 extern "C" size_t ctn_heff2_batch_workspace_bytes(const ctn_heff2_batch *b) { return b ? (size_t)b->s->total : 0; }
+extern "C" ctn_status ctn_heff2_batch_stats(const ctn_heff2_batch *b, double *out) {
+  CTN_REQUIRE(b && out, "ctn_heff2_batch_stats: null argument");
+  b->s->g1.stats(out);
+  b->s->g4.stats(out + 4);
+  return CTN_OK;
+}
 extern "C" double ctn_heff2_batch_gemm_flops(const ctn_heff2_batch *b) {
   return b ? b->s->g1.flops + b->s->g4.flops : 0.0;
 }

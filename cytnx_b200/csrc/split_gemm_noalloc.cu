@@ -14,7 +14,9 @@
 //    library, from module load until process exit;
 //  * the first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (once per device, with that device current); make that first
-//    call before any stream capture on that device;
+//    call before any stream capture on that device.  The address is kept for the
+//    process: a device reset (cudaDeviceReset) or a new primary context on that device
+//    is not supported afterwards;
 //  * every call on a device uses the same array and leaves its contents behind; the call
 //    clears the regions that must start at zero itself.  Calls whose work overlaps on
 //    the GPU (different streams, or host threads without ordering) race on the array:
@@ -71,17 +73,13 @@ extern "C" ctn_status ctn_split_gemm_f64_noalloc(int64_t M, int64_t N, int64_t K
   const int bn = 128;
   const int64_t ks = ctn::tc_k_per_slice(kind);
   const int64_t kb = (K + ks - 1) / ks, mt = (M + ctn::TC_BM - 1) / ctn::TC_BM, nt = (N + bn - 1) / bn;
-  const size_t a_bytes = (size_t)(mt * kb) * ctn::TC_A_TILE;
-  const size_t b_bytes = (size_t)(nt * kb) * bn * ctn::TC_ROW_BYTES;
-  // scratch layout: [A_hi][A_lo][B_hi][B_lo][err][group][tiles][rowmap][pack segs][pack prefixes]
+  const size_t a_bytes = (size_t)(mt * kb) * 2 * ctn::TC_A_TILE;         // hi and lo tiles interleaved
+  const size_t b_bytes = (size_t)(nt * kb) * 2 * bn * ctn::TC_ROW_BYTES;
+  // scratch layout: [A panel][B panel][err][group][tiles][rowmap][pack segs][pack prefixes]
   size_t o = 0;
-  const size_t o_ah = o;
+  const size_t o_a = o;
   o += a_bytes;
-  const size_t o_al = o;
-  o += a_bytes;
-  const size_t o_bh = o;
-  o += b_bytes;
-  const size_t o_bl = o;
+  const size_t o_b = o;
   o += b_bytes;
   const size_t o_err = o;
   o = align_up(o + 256, 256);
@@ -142,12 +140,12 @@ extern "C" ctn_status ctn_split_gemm_f64_noalloc(int64_t M, int64_t N, int64_t K
   CTN_CUDA(cudaMemcpyAsync(S + o_begin, begin, sizeof(begin), cudaMemcpyHostToDevice, st));
   const ctn::PackSeg *dsegs = (const ctn::PackSeg *)(S + o_segs);
   const int64_t *dbeg = (const int64_t *)(S + o_begin);
-  CTN_TRY(ctn::pack_launch_tables(kind, dsegs, dbeg, 1, ca, A, 0, S + o_ah, S + o_al, st));
-  CTN_TRY(ctn::pack_launch_tables(kind, dsegs + 1, dbeg + 2, 1, cb, B, 0, S + o_bh, S + o_bl, st));
+  CTN_TRY(ctn::pack_launch_tables(kind, dsegs, dbeg, 1, ca, A, 0, S + o_a, ctn::TC_BM, st));
+  CTN_TRY(ctn::pack_launch_tables(kind, dsegs + 1, dbeg + 2, 1, cb, B, 0, S + o_b, bn, st));
   int *err = (int *)(S + o_err);
   CTN_TRY(ctn::tc_launch_tables(kind, bn, (const ctn::TcGroup *)(S + o_grp), (const ctn::TcTile *)(S + o_tiles),
-                                (int64_t)tiles.size(), (const int64_t *)(S + o_rows), S + o_ah, S + o_al, S + o_bh,
-                                S + o_bl, nullptr, C, err, st));
+                                (int64_t)tiles.size(), (const int64_t *)(S + o_rows), S + o_a, S + o_b, nullptr, C,
+                                err, st));
   int herr = 0;
   CTN_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
   CTN_CUDA(cudaStreamSynchronize(st));

@@ -35,7 +35,6 @@ int nsm_count() {
 namespace {
 
 constexpr int NTHREADS_TC = 192;
-constexpr long long SPIN_LIMIT = 1ll << 24;  // try_wait probes before giving up (~seconds)
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -60,9 +59,10 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// bounded wait; returns false (and records `code`) when the limit is reached
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code) {
-  for (long long i = 0; i < SPIN_LIMIT; ++i) {
+// bounded wait; returns false (and records `code`) when `limit` probes found the phase
+// incomplete, or early once another role has recorded an error
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code, long long limit) {
+  for (long long i = 0; i < limit; ++i) {
     if (mbar_try(bar, parity)) return true;
     if ((i & 1023) == 1023 && *(volatile int *)err != 0) return false;  // another role gave up
   }
@@ -210,7 +210,11 @@ struct TcSmem {
   static constexpr int RING = STAGES * STAGE_BYTES;
   static constexpr int BAR_OFF = RING;                 // full[S], empty[S], tfull[2], tempty[2], drain
   static constexpr int EPI_OFF = RING + 1024;  // four warps' epilogue slabs (1024-aligned: TMA store boxes)
-  static constexpr int TOTAL = EPI_OFF + EPI_BYTES;
+  // two 4 KB TMA store boxes per epilogue warp when they fit beside the ring (a piece is
+  // written into one box while the previous piece's store still reads the other)
+  static constexpr int EPI_DB_BYTES = 4 * 2 * 4096;
+  static constexpr bool EPI_DB = EPI_OFF + EPI_DB_BYTES + 1024 <= 227 * 1024;
+  static constexpr int TOTAL = EPI_OFF + (EPI_DB ? EPI_DB_BYTES : EPI_BYTES);
 };
 
 template <int KIND, int BN, int STAGES>
@@ -273,18 +277,29 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
       const TcGroup g = p.groups[tl.group];
       const uint32_t b_bytes = (uint32_t)tile_n(g, tl) * TC_ROW_BYTES;  // the tile's B rows only
       for (int kb = 0; kb < g.kb; ++kb) {
-        if (!mbar_wait(&empty[stage], phase ^ 1, p.err, 1)) {
+        if (!mbar_wait(&empty[stage], phase ^ 1, p.err, 1, p.spin_limit)) {
           ok = false;
           break;
         }
+        if (p.skip_copies) {  // self-test of the error path: nothing arrives on this stage
+          if (++stage == STAGES) {
+            stage = 0;
+            phase ^= 1;
+          }
+          continue;
+        }
         uint8_t *st = smem + stage * SM::STAGE_BYTES;
         mbar_expect_tx(&full[stage], 2 * SM::A_BYTES + 2 * b_bytes);
-        const int64_t ao = g.a_off + ((int64_t)tl.mt * g.kb + kb) * SM::A_BYTES;
-        const int64_t bo = g.b_off + ((int64_t)tl.nt * g.kb + kb) * SM::B_BYTES;
-        bulk_g2s(st, p.a_hi + ao, SM::A_BYTES, &full[stage]);
-        bulk_g2s(st + SM::A_BYTES, p.a_lo + ao, SM::A_BYTES, &full[stage]);
-        bulk_g2s(st + 2 * SM::A_BYTES, p.b_hi + bo, b_bytes, &full[stage]);
-        bulk_g2s(st + 2 * SM::A_BYTES + SM::B_BYTES, p.b_lo + bo, b_bytes, &full[stage]);
+        // tiles are stored hi then lo: A's pair is one copy, B's too when the tile is full width
+        const int64_t ao = g.a_off + ((int64_t)tl.mt * g.kb + kb) * (2 * SM::A_BYTES);
+        const int64_t bo = g.b_off + ((int64_t)tl.nt * g.kb + kb) * (2 * SM::B_BYTES);
+        bulk_g2s(st, p.a + ao, 2 * SM::A_BYTES, &full[stage]);
+        if (b_bytes == (uint32_t)SM::B_BYTES) {
+          bulk_g2s(st + 2 * SM::A_BYTES, p.b + bo, 2 * SM::B_BYTES, &full[stage]);
+        } else {
+          bulk_g2s(st + 2 * SM::A_BYTES, p.b + bo, b_bytes, &full[stage]);
+          bulk_g2s(st + 2 * SM::A_BYTES + SM::B_BYTES, p.b + bo + SM::B_BYTES, b_bytes, &full[stage]);
+        }
         filled[stage]++;
         if (++stage == STAGES) {
           stage = 0;
@@ -294,7 +309,7 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
     }
     // drain: every issued fill must have landed before the CTA may exit
     for (int s = 0; s < STAGES; ++s)
-      if (filled[s]) mbar_wait(&full[s], (filled[s] - 1) & 1, p.err, 5);
+      if (filled[s]) mbar_wait(&full[s], (filled[s] - 1) & 1, p.err, 5, p.spin_limit);
   } else if (warp == 1 && lane == 0) {
     // ---------------------------------------------------------------- MMA issuer
     int stage = 0;
@@ -307,11 +322,11 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
       const TcTile tl = p.tiles[t];
       const TcGroup g = p.groups[tl.group];
       const uint32_t idesc = IDESC0 | ((uint32_t)(tile_n(g, tl) >> 3) << 17);
-      if (!mbar_wait(&tempty[acc], acc_phase ^ 1, p.err, 2)) break;
+      if (!mbar_wait(&tempty[acc], acc_phase ^ 1, p.err, 2, p.spin_limit)) break;
       tc_fence_after();
       const uint32_t d = tmem_base + (uint32_t)(acc * BN);
       for (int kb = 0; kb < g.kb; ++kb) {
-        if (!mbar_wait(&full[stage], phase, p.err, 3)) {
+        if (!mbar_wait(&full[stage], phase, p.err, 3, p.spin_limit)) {
           ok = false;
           break;
         }
@@ -343,7 +358,7 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
     // all MMAs of this CTA complete before TMEM is released
     if (issued) {
       tc_commit(drain);
-      mbar_wait(drain, 0, p.err, 6);
+      mbar_wait(drain, 0, p.err, 6, p.spin_limit);
     }
   } else if (warp >= 2) {
     // ---------------------------------------------------------------- epilogue
@@ -351,12 +366,13 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
     float *slab = reinterpret_cast<float *>(smem + SM::EPI_OFF) + (warp - 2) * EPI_WARP_FLOATS;
     int acc = 0;
     uint32_t acc_phase = 0;
+    uint32_t pieces = 0;  // TMA-stored pieces of this warp (alternates the store boxes)
     for (int64_t t = blockIdx.x; t < p.ntiles; t += gridDim.x) {
       const TcTile tl = p.tiles[t];
       const TcGroup g = p.groups[tl.group];
       // warp-uniform bounded wait (the TMEM loads below are .sync.aligned)
       int okw = 0;
-      if (lane == 0) okw = mbar_wait(&tfull[acc], acc_phase, p.err, 4) ? 1 : 0;
+      if (lane == 0) okw = mbar_wait(&tfull[acc], acc_phase, p.err, 4, p.spin_limit) ? 1 : 0;
       okw = __shfl_sync(0xffffffffu, okw, 0);
       __syncwarp();
       if (!okw) break;
@@ -378,7 +394,6 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
       const bool tma_out = p.cmaps != nullptr && g.mode == 0 && p.epi_staged;
       // row-mapped FP64 groups launched with only an FP32 output go out as FP32 (mode 2)
       const int mode = (g.mode == 1 && p.c64 == nullptr) ? 2 : g.mode;
-      uint8_t *box = reinterpret_cast<uint8_t *>(smem + SM::EPI_OFF) + (warp - 2) * 4096;
 #pragma unroll 1
       for (int c0 = 0; c0 < BN && any_row; c0 += 32) {
         uint32_t v[32];
@@ -389,7 +404,15 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
         if (cg0 >= g.N) continue;  // warp-uniform: the whole piece is past the tile edge
         const int ncol = min(min(32, BN - c0), g.N - cg0);  // a 32-column piece may pass the tile edge
         if (tma_out) {
-          if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+          uint8_t *box = reinterpret_cast<uint8_t *>(smem + SM::EPI_OFF) +
+                         (SM::EPI_DB ? (warp - 2) * 8192 + (pieces & 1) * 4096 : (warp - 2) * 4096);
+          if (lane == 0) {
+            if (SM::EPI_DB)
+              asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");  // the other box may still be read
+            else
+              asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+          }
+          ++pieces;
           __syncwarp();
 #pragma unroll
           for (int j = 0; j < 8; ++j)
@@ -512,10 +535,8 @@ struct TcSmem2 {
 };
 
 template <int KIND, int BN, int STAGES>
-__global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p, const __grid_constant__ CUtensorMap ta_hi,
-                                                                  const __grid_constant__ CUtensorMap ta_lo,
-                                                                  const __grid_constant__ CUtensorMap tb_hi,
-                                                                  const __grid_constant__ CUtensorMap tb_lo) {
+__global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p, const __grid_constant__ CUtensorMap ta,
+                                                                  const __grid_constant__ CUtensorMap tb) {
   using SM = TcSmem2<KIND, BN, STAGES>;
   static_assert(BN % 16 == 0 && BN >= 32 && BN <= 256, "2-CTA tile width");
   extern __shared__ uint8_t smem_raw[];
@@ -570,21 +591,22 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p, con
       const TcGroup g = p.groups[tl.group];
       const int mt128 = 2 * tl.mt + (int)rank;  // this CTA's 128-row A tile (panels hold an even count)
       for (int kb = 0; kb < g.kb; ++kb) {
-        if (!mbar_wait(&empty[stage], phase ^ 1, p.err, 1)) {
+        if (!mbar_wait(&empty[stage], phase ^ 1, p.err, 1, p.spin_limit)) {
           ok = false;
           break;
         }
         uint8_t *st = smem + stage * SM::STAGE_BYTES;
         if (rank == 0) mbar_expect_tx(&full[stage], 2 * SM::STAGE_BYTES);
         const uint32_t fb = peer_addr(&full[stage], 0);
-        // panel rows of 128 bytes: A tile (mt128, kb) and this CTA's half of B tile (nt, kb)
-        const int ya = (int)((g.a_off + ((int64_t)mt128 * g.kb + kb) * SM::A_BYTES) / TC_ROW_BYTES);
-        const int yb = (int)((g.b_off + ((int64_t)tl.nt * g.kb + kb) * (2 * SM::B_BYTES) + (int64_t)rank * SM::B_BYTES) /
+        // panel rows of 128 bytes: A tile (mt128, kb) hi + lo (256 rows, one box) and this
+        // CTA's half of the hi and of the lo B tile (nt, kb); a full B tile is BN rows hi then
+        // BN rows lo (SM::B_BYTES is half a tile)
+        const int ya = (int)((g.a_off + ((int64_t)mt128 * g.kb + kb) * (2 * SM::A_BYTES)) / TC_ROW_BYTES);
+        const int yb = (int)((g.b_off + ((int64_t)tl.nt * g.kb + kb) * (4 * SM::B_BYTES) + (int64_t)rank * SM::B_BYTES) /
                              TC_ROW_BYTES);
-        tma_rows_pair(st, &ta_hi, ya, fb);
-        tma_rows_pair(st + SM::A_BYTES, &ta_lo, ya, fb);
-        tma_rows_pair(st + 2 * SM::A_BYTES, &tb_hi, yb, fb);
-        tma_rows_pair(st + 2 * SM::A_BYTES + SM::B_BYTES, &tb_lo, yb, fb);
+        tma_rows_pair(st, &ta, ya, fb);
+        tma_rows_pair(st + 2 * SM::A_BYTES, &tb, yb, fb);
+        tma_rows_pair(st + 2 * SM::A_BYTES + SM::B_BYTES, &tb, yb + 2 * SM::B_BYTES / TC_ROW_BYTES, fb);
         filled[stage]++;
         if (++stage == STAGES) {
           stage = 0;
@@ -596,7 +618,7 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p, con
     // for every issued fill; the follower is held at the final cluster barrier meanwhile
     if (rank == 0)
       for (int s = 0; s < STAGES; ++s)
-        if (filled[s]) mbar_wait(&full[s], (filled[s] - 1) & 1, p.err, 5);
+        if (filled[s]) mbar_wait(&full[s], (filled[s] - 1) & 1, p.err, 5, p.spin_limit);
   } else if (warp == 1 && lane == 0 && rank == 0) {
     // ---------------------------------------------------------------- MMA issuer (leader)
     int stage = 0;
@@ -607,11 +629,11 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p, con
     bool issued = false;
     for (int64_t t = pair; t < p.ntiles && ok; t += npairs) {
       const TcGroup g = p.groups[p.tiles[t].group];
-      if (!mbar_wait(&tempty[acc], acc_phase ^ 1, p.err, 2)) break;
+      if (!mbar_wait(&tempty[acc], acc_phase ^ 1, p.err, 2, p.spin_limit)) break;
       tc_fence_after();
       const uint32_t d = tmem_base + (uint32_t)(acc * BN);
       for (int kb = 0; kb < g.kb; ++kb) {
-        if (!mbar_wait(&full[stage], phase, p.err, 3)) {
+        if (!mbar_wait(&full[stage], phase, p.err, 3, p.spin_limit)) {
           ok = false;
           break;
         }
@@ -642,7 +664,7 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p, con
     }
     if (issued) {
       tc_commit2_local(drain);
-      mbar_wait(drain, 0, p.err, 6);
+      mbar_wait(drain, 0, p.err, 6, p.spin_limit);
     }
   } else if (warp >= 2) {
     // ---------------------------------------------------------------- epilogue (both CTAs)
@@ -655,7 +677,7 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p, con
       const TcTile tl = p.tiles[t];
       const TcGroup g = p.groups[tl.group];
       int okw = 0;
-      if (lane == 0) okw = mbar_wait(&tfull[acc], acc_phase, p.err, 4) ? 1 : 0;
+      if (lane == 0) okw = mbar_wait(&tfull[acc], acc_phase, p.err, 4, p.spin_limit) ? 1 : 0;
       okw = __shfl_sync(0xffffffffu, okw, 0);
       __syncwarp();
       if (!okw) break;
@@ -1023,14 +1045,12 @@ ctn_status launch_tc_pair(const TcParams &prm, int64_t ntiles, cudaStream_t st) 
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  CUtensorMap ma_hi, ma_lo, mb_hi, mb_lo;
+  CUtensorMap ma, mb;
   CTN_REQUIRE(prm.a_bytes > 0 && prm.b_bytes > 0 && prm.a_bytes % 128 == 0 && prm.b_bytes % 128 == 0,
               "tcgen05 2-CTA GEMM: panel sizes unknown");
-  CTN_TRY(encode_rows_map(&ma_hi, prm.a_hi, prm.a_bytes, TC_BM));
-  CTN_TRY(encode_rows_map(&ma_lo, prm.a_lo, prm.a_bytes, TC_BM));
-  CTN_TRY(encode_rows_map(&mb_hi, prm.b_hi, prm.b_bytes, BN / 2));
-  CTN_TRY(encode_rows_map(&mb_lo, prm.b_lo, prm.b_bytes, BN / 2));
-  CTN_CUDA(cudaLaunchKernelEx(&cfg, k_tc_gemm_pair<KIND, BN, STAGES>, prm, ma_hi, ma_lo, mb_hi, mb_lo));
+  CTN_TRY(encode_rows_map(&ma, prm.a, prm.a_bytes, 2 * TC_BM));  // hi + lo of one A tile per box
+  CTN_TRY(encode_rows_map(&mb, prm.b, prm.b_bytes, BN / 2));
+  CTN_CUDA(cudaLaunchKernelEx(&cfg, k_tc_gemm_pair<KIND, BN, STAGES>, prm, ma, mb));
   return CTN_OK;
 }
 
@@ -1094,11 +1114,32 @@ int TcGemm::add_group(int M, int N, int K, int mode, int64_t c_off, int ldc, int
   g.rm_off = rm_off;
   g.a_off = a_bytes;
   g.b_off = b_bytes;
-  a_bytes += (int64_t)mt_alloc * g.kb * TC_A_TILE;
-  b_bytes += (int64_t)g.nt * g.kb * bn * TC_ROW_BYTES;
+  a_bytes += (int64_t)mt_alloc * g.kb * 2 * TC_A_TILE;     // hi + lo tiles
+  b_bytes += (int64_t)g.nt * g.kb * 2 * bn * TC_ROW_BYTES;
   groups.push_back(g);
   flops += 2.0 * M * (double)N * K;
   return (int)groups.size() - 1;
+}
+
+void TcGemm::stats(double *out) const {
+  const int ks = tc_k_per_slice(kind);
+  const int rows = pair ? 2 * TC_BM : TC_BM;
+  double exec = 0.0, bytes = 0.0, own = 0.0;
+  for (const TcGroup &g : groups) {
+    if (g.kb == 0) continue;
+    own += 2.0 * tc_elem_bytes(kind) * ((double)g.M * g.K + (double)g.N * g.K);
+    const int mtiles = pair ? (g.mt + 1) / 2 : g.mt;
+    for (int n = 0; n < g.nt; ++n) {
+      const int rem = g.N - n * bn;
+      const int neff = rem >= bn ? bn : (rem + 15) / 16 * 16;
+      exec += 2.0 * mtiles * rows * (double)neff * g.kb * ks;
+      bytes += (double)mtiles * g.kb * 2.0 * ((double)rows * TC_ROW_BYTES + (double)neff * TC_ROW_BYTES);
+    }
+  }
+  out[0] = flops;
+  out[1] = exec;
+  out[2] = bytes;
+  out[3] = own;
 }
 
 void TcGemm::finalize() {
@@ -1221,8 +1262,7 @@ ctn_status TcGemm::bind_c32(float *c32, cudaStream_t st) {
   return CTN_OK;
 }
 
-ctn_status TcGemm::run(const uint8_t *a_hi, const uint8_t *a_lo, const uint8_t *b_hi, const uint8_t *b_lo,
-                       float *c32, double *c64, int *err, cudaStream_t st) {
+ctn_status TcGemm::run(const uint8_t *a, const uint8_t *b, float *c32, double *c64, int *err, cudaStream_t st) {
   if (tiles.empty()) return CTN_OK;
   CTN_TRY(upload(st));
   TcParams prm;
@@ -1237,10 +1277,10 @@ ctn_status TcGemm::run(const uint8_t *a_hi, const uint8_t *a_lo, const uint8_t *
   prm.epi_staged = epi_staged ? 1 : 0;
   prm.a_bytes = a_bytes;
   prm.b_bytes = b_bytes;
-  prm.a_hi = a_hi;
-  prm.a_lo = a_lo;
-  prm.b_hi = b_hi;
-  prm.b_lo = b_lo;
+  prm.a = a;
+  prm.b = b;
+  prm.spin_limit = spin_limit;
+  prm.skip_copies = skip_copies;
   prm.c32 = c32;
   prm.c64 = c64;
   prm.err = err;
@@ -1248,8 +1288,8 @@ ctn_status TcGemm::run(const uint8_t *a_hi, const uint8_t *a_lo, const uint8_t *
 }
 
 ctn_status tc_launch_tables(int kind, int bn, const TcGroup *d_groups, const TcTile *d_tiles, int64_t ntiles,
-                            const int64_t *d_rowmap, const uint8_t *a_hi, const uint8_t *a_lo, const uint8_t *b_hi,
-                            const uint8_t *b_lo, float *c32, double *c64, int *err, cudaStream_t st) {
+                            const int64_t *d_rowmap, const uint8_t *a, const uint8_t *b, float *c32, double *c64,
+                            int *err, cudaStream_t st) {
   if (ntiles == 0) return CTN_OK;
   TcParams prm;
   prm.cmaps = nullptr;
@@ -1260,10 +1300,10 @@ ctn_status tc_launch_tables(int kind, int bn, const TcGroup *d_groups, const TcT
   prm.epi_staged = 0;
   prm.a_bytes = 0;
   prm.b_bytes = 0;
-  prm.a_hi = a_hi;
-  prm.a_lo = a_lo;
-  prm.b_hi = b_hi;
-  prm.b_lo = b_lo;
+  prm.a = a;
+  prm.b = b;
+  prm.spin_limit = TC_SPIN_LIMIT;
+  prm.skip_copies = 0;
   prm.c32 = c32;
   prm.c64 = c64;
   prm.err = err;
@@ -1271,8 +1311,9 @@ ctn_status tc_launch_tables(int kind, int bn, const TcGroup *d_groups, const TcT
 }
 
 ctn_status pack_launch_tables(int kind, const PackSeg *d_segs, const int64_t *d_begin, int nseg, int64_t nchunks,
-                              const void *src, int src_is_f32, uint8_t *hi, uint8_t *lo, cudaStream_t st) {
+                              const void *src, int src_is_f32, uint8_t *panel, int tile_rows, cudaStream_t st) {
   if (nchunks == 0) return CTN_OK;
+  uint8_t *hi = panel, *lo = panel + tc_lo_delta(tile_rows);
   PackParams prm;
   prm.segs = d_segs;
   prm.begin = d_begin;
@@ -1358,9 +1399,13 @@ ctn_status Packer::upload(cudaStream_t st) {
   return CTN_OK;
 }
 
-ctn_status Packer::run(const void *src, int src_is_f32, uint8_t *hi, uint8_t *lo, cudaStream_t st) {
+ctn_status Packer::run(const void *src, int src_is_f32, uint8_t *panel, cudaStream_t st) {
   if (nchunks == 0) return CTN_OK;
   CTN_TRY(upload(st));
+  // every segment of one packer fills the same panel: one tile height
+  if (transposing ? tile_items.empty() : segs.empty()) return CTN_OK;
+  const int rows = transposing ? tile_items[0].tile_rows : segs[0].tile_rows;
+  uint8_t *hi = panel, *lo = panel + tc_lo_delta(rows);
   if (transposing) {
     PackTileParams tp;
     tp.segs = (const PackSeg *)d_mem;
@@ -1443,6 +1488,45 @@ extern "C" size_t ctn_split_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K
   return (size_t)(2 * a + 2 * b + 256 + 64);
 }
 
+extern "C" ctn_status ctn_selftest_wait_timeout(int precision, long long spin_limit, void *stream) {
+  CTN_REQUIRE(precision == CTN_PREC_3XTF32 || precision == CTN_PREC_BF16X3,
+              "ctn_selftest_wait_timeout: precision must be split");
+  CTN_REQUIRE(spin_limit > 0, "ctn_selftest_wait_timeout: spin_limit must be positive");
+  cudaStream_t st = ctn::as_stream(stream);
+  SplitDense s;
+  const int kind = precision == CTN_PREC_BF16X3 ? ctn::TC_BF16 : ctn::TC_TF32;
+  s.g.kind = kind;
+  s.g.bn = 128;
+  const int64_t n = 128;
+  std::vector<int64_t> rows(n);
+  for (int64_t r = 0; r < n; ++r) rows[r] = r * n;
+  s.g.rowmap = rows;
+  s.g.add_group((int)n, (int)n, (int)n, 1, 0, (int)n, 0);
+  s.g.finalize();
+  s.g.spin_limit = spin_limit;
+  s.g.skip_copies = 1;  // the producer issues nothing: the MMA warp's first wait runs out
+  uint8_t *ws = nullptr;
+  const size_t bytes = (size_t)(s.g.a_bytes + s.g.b_bytes + 64 + (int64_t)n * n * 8);
+  CTN_CUDA(cudaMalloc(&ws, bytes));
+  CTN_CUDA(cudaMemsetAsync(ws, 0, bytes, st));
+  int *err = (int *)(ws + s.g.a_bytes + s.g.b_bytes);
+  double *C = (double *)(ws + s.g.a_bytes + s.g.b_bytes + 64);
+  ctn_status rc = s.g.run(ws, ws + s.g.a_bytes, nullptr, C, err, st);
+  int herr = 0;
+  if (rc == CTN_OK) {
+    if (cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) rc = CTN_ERR_CUDA;
+  }
+  cudaFree(ws);
+  if (rc != CTN_OK) return rc;
+  if (herr) {
+    ctn::set_error("tcgen05 GEMM: a bounded wait expired (code %d)", herr);
+    return CTN_ERR_TIMEOUT;
+  }
+  ctn::set_error("ctn_selftest_wait_timeout: the kernel finished without a timeout");
+  return CTN_ERR_INVALID;
+}
+
 extern "C" ctn_status ctn_split_gemm_f64(int64_t M, int64_t N, int64_t K, const double *A, const double *B, double *C,
                                          int precision, void *workspace, void *stream) {
   CTN_REQUIRE(M > 0 && N > 0 && K > 0 && A && B && C && workspace, "ctn_split_gemm_f64: bad argument");
@@ -1467,12 +1551,12 @@ extern "C" ctn_status ctn_split_gemm_f64(int64_t M, int64_t N, int64_t K, const 
   s.pa.finalize();
   s.pb.finalize();
   uint8_t *ws = (uint8_t *)workspace;
-  uint8_t *a_hi = ws, *a_lo = a_hi + s.g.a_bytes, *b_hi = a_lo + s.g.a_bytes, *b_lo = b_hi + s.g.b_bytes;
-  int *err = (int *)(b_lo + s.g.b_bytes);
-  CTN_CUDA(cudaMemsetAsync(ws, 0, 2 * s.g.a_bytes + 2 * s.g.b_bytes + 64, st));
-  CTN_TRY(s.pa.run(A, 0, a_hi, a_lo, st));
-  CTN_TRY(s.pb.run(B, 0, b_hi, b_lo, st));
-  CTN_TRY(s.g.run(a_hi, a_lo, b_hi, b_lo, nullptr, C, err, st));
+  uint8_t *pa = ws, *pb = pa + s.g.a_bytes;  // panels (hi and lo tiles interleaved)
+  int *err = (int *)(pb + s.g.b_bytes);
+  CTN_CUDA(cudaMemsetAsync(ws, 0, s.g.a_bytes + s.g.b_bytes + 64, st));
+  CTN_TRY(s.pa.run(A, 0, pa, st));
+  CTN_TRY(s.pb.run(B, 0, pb, st));
+  CTN_TRY(s.g.run(pa, pb, nullptr, C, err, st));
   int herr = 0;
   CTN_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
   CTN_CUDA(cudaStreamSynchronize(st));

@@ -4,11 +4,13 @@
 // cut into tiles of 128 (A) or BN (B) rows by one 128-byte K slice (32 TF32 or 64 BF16
 // values), each tile laid out exactly as the UMMA K-major SWIZZLE_128B canonical layout
 // expects in shared memory (8-row x 128-byte atoms, 16-byte chunk index XOR row % 8).
-// A tile therefore moves global -> shared with ONE contiguous bulk copy (TMA engine,
-// cp.async.bulk + mbarrier complete_tx), no tensor map needed, for any block shape;
-// padding rows/columns are zeros written once.  Each operand is split into a "hi" and a
-// "lo" panel (x = hi + lo, both exactly representable in TF32 or BF16) and every K slice
-// issues three MMAs lo*hi + hi*lo + hi*hi into one FP32 TMEM accumulator.
+// Each operand is split as x = hi + lo (both exactly representable in TF32 or BF16), and a
+// tile is stored as its hi half followed by its lo half: the hi and lo tiles of one K slice
+// move global -> shared with ONE contiguous bulk copy (TMA engine, cp.async.bulk +
+// mbarrier complete_tx), no tensor map needed, for any block shape.  (Bulk copies of 32 KB
+// and more stream from L2 at ~1.4x the rate of 16 KB ones on B200.)  Padding rows/columns
+// are zeros written once.  Every K slice issues three MMAs lo*hi + hi*lo + hi*hi into one
+// FP32 TMEM accumulator.
 #pragma once
 #include <cstdint>
 #include <algorithm>
@@ -21,6 +23,7 @@ namespace ctn {
 constexpr int TC_BM = 128;            // UMMA M (rows of an A tile, TMEM lanes)
 constexpr int TC_ROW_BYTES = 128;     // one swizzle row = one K slice
 constexpr int TC_A_TILE = TC_BM * TC_ROW_BYTES;  // 16 KiB
+constexpr long long TC_SPIN_LIMIT = 1ll << 24;   // try_wait probes of a bounded wait (~seconds)
 
 enum TcKind { TC_TF32 = 0, TC_BF16 = 1 };
 
@@ -46,20 +49,24 @@ struct TcParams {
   const TcGroup *groups;
   const TcTile *tiles;
   int64_t ntiles;
-  const uint8_t *a_hi, *a_lo, *b_hi, *b_lo;
+  const uint8_t *a, *b;  // operand panels (hi/lo interleaved per tile)
   float *c32;
   double *c64;
   const int64_t *rowmap;
   int *err;  // device error word: 0 ok, else the code of the wait that gave up
   int epi_staged;  // 1: epilogue through the shared-memory slab (whole row segments), 0: direct
-  int64_t a_bytes, b_bytes;  // panel sizes (2-CTA form: extents of its TMA views)
+  int64_t a_bytes, b_bytes;  // panel sizes, hi and lo (2-CTA form: extents of its TMA views)
   // one 2-D FP32 tensor map per group (CUtensorMap, 128 bytes each) over the row-strided
   // output of mode-0 groups, or null: the staged epilogue then stores 32 x 32 pieces by TMA
   const void *cmaps;
+  long long spin_limit;  // try_wait probes of every bounded wait before it gives up
+  int skip_copies;       // error-path self-test: the producer issues no copies (waits run out)
 };
 
-// byte offset of element (r, k) inside a panel of tiles with `rows` rows per tile
-// (tile index = (r / rows) * kb + k / kslice), K-major SWIZZLE_128B
+// byte offset of the hi element (r, k) inside a panel of tiles with `rows` rows per tile
+// (tile index = (r / rows) * kb + k / kslice), K-major SWIZZLE_128B; every tile is its hi
+// half (rows x 128 bytes) followed by its lo half, so the lo element is rows * 128 bytes
+// further (tc_lo_delta)
 __host__ __device__ inline int64_t tc_panel_offset(int64_t r, int64_t k, int rows, int kb, int kind) {
   const int ks = kind == TC_TF32 ? 32 : 64;
   const int eb = kind == TC_TF32 ? 4 : 2;
@@ -67,8 +74,10 @@ __host__ __device__ inline int64_t tc_panel_offset(int64_t r, int64_t k, int row
   const int rr = (int)(r % rows);
   const int byte = (int)(k % ks) * eb;
   const int chunk = (byte >> 4) ^ (rr & 7);
-  return tile * (int64_t)rows * TC_ROW_BYTES + (rr >> 3) * 1024 + (rr & 7) * 128 + chunk * 16 + (byte & 15);
+  return tile * 2 * (int64_t)rows * TC_ROW_BYTES + (rr >> 3) * 1024 + (rr & 7) * 128 + chunk * 16 + (byte & 15);
 }
+// distance from a hi element to its lo element in a panel with `rows` rows per tile
+__host__ __device__ inline int64_t tc_lo_delta(int rows) { return (int64_t)rows * TC_ROW_BYTES; }
 
 // Host plan object for one grouped GEMM (device tables uploaded on first use).
 struct TcGemm {
@@ -89,19 +98,26 @@ struct TcGemm {
   std::vector<TcGroup> groups;
   std::vector<TcTile> tiles;
   std::vector<int64_t> rowmap;
-  int64_t a_bytes = 0, b_bytes = 0;  // panel sizes (one of hi/lo)
+  int64_t a_bytes = 0, b_bytes = 0;  // panel sizes (hi and lo together)
   void *d_mem = nullptr;
   int d_dev = -1;
   double flops = 0.0;  // 2*M*N*K summed over groups (useful flops, one product)
+  long long spin_limit = TC_SPIN_LIMIT;  // probes of every bounded wait in the kernel
+  int skip_copies = 0;                   // error-path self-test only (ctn_selftest_wait_timeout)
 
   // append a group; returns its index.  Panels are laid out back to back.
   int add_group(int M, int N, int K, int mode, int64_t c_off, int ldc, int64_t rm_off);
   void finalize();  // builds the tile list (largest K first)
+  // out[0] useful flops (2*M*N*K, one product), out[1] executed MMA flops of the tiles (one
+  // product: 128 (256 for 2-CTA) rows x the tile's N rounded to 16 x its K slices), out[2] operand
+  // panel bytes the tiles copy into shared memory per launch (hi and lo, all products), out[3]
+  // the operands' own bytes (M*K + N*K elements, hi and lo, each once)
+  void stats(double *out) const;
   ctn_status upload(cudaStream_t st);
   // encode (once per output buffer) the TMA store maps of the mode-0 groups over c32; run()
   // with the same c32 then stores those groups' tiles by TMA
   ctn_status bind_c32(float *c32, cudaStream_t st);
-  ctn_status run(const uint8_t *a_hi, const uint8_t *a_lo, const uint8_t *b_hi, const uint8_t *b_lo, float *c32,
+  ctn_status run(const uint8_t *a, const uint8_t *b, float *c32,
                  double *c64, int *err, cudaStream_t st);
   void *d_cmaps = nullptr;
   const float *cmaps_for = nullptr;
@@ -148,8 +164,8 @@ struct Packer {
   int d_dev = -1;
   void finalize();
   ctn_status upload(cudaStream_t st);
-  // src is FP64 (src_is_f32 == 0) or FP32
-  ctn_status run(const void *src, int src_is_f32, uint8_t *hi, uint8_t *lo, cudaStream_t st);
+  // src is FP64 (src_is_f32 == 0) or FP32; panel receives hi and lo tiles interleaved
+  ctn_status run(const void *src, int src_is_f32, uint8_t *panel, cudaStream_t st);
   ~Packer();
 };
 
@@ -193,8 +209,9 @@ inline void chunk_items(const std::vector<int64_t> &begin, int64_t per_item, std
 
 // Launch helpers over device-resident tables (the caller owns every buffer).
 ctn_status tc_launch_tables(int kind, int bn, const TcGroup *d_groups, const TcTile *d_tiles, int64_t ntiles,
-                            const int64_t *d_rowmap, const uint8_t *a_hi, const uint8_t *a_lo, const uint8_t *b_hi,
-                            const uint8_t *b_lo, float *c32, double *c64, int *err, cudaStream_t st);
+                            const int64_t *d_rowmap, const uint8_t *a, const uint8_t *b, float *c32, double *c64,
+                            int *err, cudaStream_t st);
+// `panel` receives hi and lo tiles interleaved; `tile_rows` is its rows per tile (128 or BN)
 ctn_status pack_launch_tables(int kind, const PackSeg *d_segs, const int64_t *d_begin, int nseg, int64_t nchunks,
-                              const void *src, int src_is_f32, uint8_t *hi, uint8_t *lo, cudaStream_t st);
+                              const void *src, int src_is_f32, uint8_t *panel, int tile_rows, cudaStream_t st);
 }  // namespace ctn

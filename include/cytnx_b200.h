@@ -189,11 +189,20 @@ ctn_status ctn_split_gemm_f64(int64_t M, int64_t N, int64_t K, const double *A, 
  * the reference.  Scratch lives in a 32 MiB static device array held by every GPU
  * that loads the library until exit; problems needing more are rejected with
  * CTN_ERR_INVALID.  The first call on a device looks up the array's address
- * (cudaGetSymbolAddress) and should come before any stream capture.  All calls share
+ * (cudaGetSymbolAddress) and should come before any stream capture; the address is kept
+ * for the process, so a device reset afterwards is not supported.  All calls share
  * the array: calls that overlap on the GPU race, so serialise them.  Synchronises
  * the stream. */
 ctn_status ctn_split_gemm_f64_noalloc(int64_t M, int64_t N, int64_t K, const double *A, const double *B, double *C,
                                       int precision, void *stream);
+
+/* Self-test of the bounded-wait error path of the tcgen05 GEMM: one 128 x 128 x 128 split GEMM
+ * whose producer issues no copies, so the MMA warp's wait for its first operand stage runs out
+ * after `spin_limit` probes; the kernel records the error, stops its other roles, frees its
+ * TMEM and returns.  Returns CTN_ERR_TIMEOUT (with the code of the wait in ctn_last_error())
+ * when that path works; the context stays usable.  Allocates a small device buffer.
+ * Synchronises the stream.  No counterpart in the reference (its kernels do not wait). */
+ctn_status ctn_selftest_wait_timeout(int precision, long long spin_limit, void *stream);
 
 /* ---------------------------------------------------------------- BLAS-1 (FP64)
  * Results of reductions land in device memory (out points to device doubles). */
@@ -245,6 +254,11 @@ ctn_status ctn_heff2_profile(ctn_heff2_plan *plan, const double *psi, double *ou
 double ctn_heff2_gemm_flops(const ctn_heff2_plan *plan, int step);
 /* the same for the stacked tensor-core GEMMs of a split precision (one product counted) */
 double ctn_heff2_split_gemm_flops(ctn_heff2_plan *plan, int precision, int step);
+/* work accounting of the split-precision GEMMs (step 1 in out[0..3], step 4 in out[4..7]):
+ * useful flops (2*M*N*K, one product), executed MMA flops of the tiles including their padding
+ * (one product), the operand panel bytes the tiles copy into shared memory per matvec (hi and
+ * lo panels, with every re-read), and the operands' own bytes (hi and lo, each element once) */
+ctn_status ctn_heff2_split_stats(ctn_heff2_plan *plan, int precision, double *out);
 void ctn_heff2_plan_destroy(ctn_heff2_plan *plan);
 /* tile widths (N of the UMMA tiles: 32, 48, 64, 96, 128, 144, 160, 192 or 256; negative -128, -192,
  * -256 select 2-CTA cta_group::2 tiles of 256 rows) of the step-1 and
@@ -278,6 +292,8 @@ ctn_status ctn_heff2_batch_create(ctn_heff2_plan *const *plans, int nprob, const
 size_t ctn_heff2_batch_workspace_bytes(const ctn_heff2_batch *batch);
 /* useful flops of one batched matvec (2*M*N*K over the GEMM groups, one product) */
 double ctn_heff2_batch_gemm_flops(const ctn_heff2_batch *batch);
+/* the same accounting as ctn_heff2_split_stats for the batched GEMMs */
+ctn_status ctn_heff2_batch_stats(const ctn_heff2_batch *batch, double *out);
 ctn_status ctn_heff2_batch_set_env(ctn_heff2_batch *batch, const void *L_all, const void *R_all,
                                    void *workspace, void *stream);
 ctn_status ctn_heff2_batch_matvec(ctn_heff2_batch *batch, const void *psi_all, void *out_all,

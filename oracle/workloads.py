@@ -307,3 +307,37 @@ def mps_heff_times_site(bond_q, bond_d, site_flats, k: int, mpo_values=None, phy
     if not np.array_equal(Y.itoi, ref.itoi):
         raise RuntimeError("H_eff A_k blocks are not in A_k's order")
     return Y.flat()
+
+
+def env_left(L: BlockTensor, A: BlockTensor, M: BlockTensor) -> BlockTensor:
+    """L'[w, a, ap] = sum L[w,a,ap] A[a,s,b] M[w,wn,s,sp] A*[ap,sp,bp] (real data; legs by
+    position), the left update of example/DMRG/dmrg_two_sites_U1.py:115-126, as the three
+    pairwise contractions env . A, . M, . A^dagger.  Result legs (b -> a, wn -> w, bp -> ap) in the
+    order [w, a, ap]."""
+    Lr = L.relabel(["w", "a", "ap"])
+    Ar = A.relabel(["a", "s", "b"])
+    Ad = BlockTensor([b.redirect() for b in A.bonds], ["ap", "sp", "bp"], A.rowrank, A.itoi, A.blocks)
+    t = Lr.contract(Ar).contract(M.relabel(["w", "wn", "s", "sp"])).contract(Ad)
+    t = t.relabel([{"b": "a", "wn": "w", "bp": "ap"}[l] for l in t.labels])
+    return t.permute([t.labels.index(l) for l in ("w", "a", "ap")])
+
+
+def env_right(R: BlockTensor, A: BlockTensor, M: BlockTensor) -> BlockTensor:
+    """R'[w, a, ap] = sum A[a,s,b] R[wn,b,bp] M[w,wn,s,sp] A*[ap,sp,bp] (real data; legs by
+    position), the right update of example/DMRG/dmrg_two_sites_U1.py:151-161."""
+    Rr = R.relabel(["wn", "b", "bp"])
+    Ar = A.relabel(["a", "s", "b"])
+    Ad = BlockTensor([b.redirect() for b in A.bonds], ["ap", "sp", "bp"], A.rowrank, A.itoi, A.blocks)
+    t = Ar.contract(Rr).contract(M.relabel(["w", "wn", "s", "sp"])).contract(Ad)
+    return t.permute([t.labels.index(l) for l in ("w", "a", "ap")])
+
+
+def random_site(qv, dv, seed: int) -> BlockTensor:
+    """A U(1) site tensor A[a (ket), s (bra), b (bra)] on the bond qv/dv at both ends, ~N(0,1)."""
+    syms = [(-1, 1)]
+    V = Bond(KET, _col(qv), dv, syms)
+    phys = Bond(KET, _col(SPIN_PHYS_Q), [1, 1], syms)
+    bonds = [V, phys.redirect(), V.redirect()]
+    itoi = enumerate_blocks(bonds)
+    n = sum(int(np.prod([bonds[i].degs[q] for i, q in enumerate(t)])) for t in itoi)
+    return BlockTensor.from_flat(bonds, ["a", "s", "b"], 2, itoi, np.random.default_rng(seed).standard_normal(n))

@@ -48,3 +48,26 @@ def test_nan_in_environment_is_reported():
     y = torch.empty_like(x)
     H2.apply_flat(x, y, "fp64")
     assert torch.isfinite(y).all()
+
+
+@pytest.mark.parametrize("precision", [1, 2])
+def test_tcgen05_bounded_wait_expires_and_context_survives(precision):
+    """The tcgen05 GEMM's bounded waits (ctn_selftest_wait_timeout: a producer that issues no
+    copies, 2^16 probes per wait): the MMA warp's first wait runs out, the kernel records
+    the error, stops its other roles, frees TMEM and returns; the host sees CTN_ERR_TIMEOUT
+    and the next GEMM on the same context is correct."""
+    from cytnx_b200 import _lib
+
+    lib = _lib.lib()
+    rc = lib.ctn_selftest_wait_timeout(precision, 1 << 16, _lib.stream_ptr())
+    assert rc == 4, (rc, lib.ctn_last_error())
+    assert b"bounded wait expired" in lib.ctn_last_error()
+    g = torch.Generator(device="cuda").manual_seed(3)
+    A = torch.randn(300, 200, dtype=torch.float64, device="cuda", generator=g)
+    B = torch.randn(200, 150, dtype=torch.float64, device="cuda", generator=g)
+    ws = torch.empty(lib.ctn_split_gemm_workspace_bytes(300, 150, 200, precision), dtype=torch.uint8, device="cuda")
+    C = torch.empty(300, 150, dtype=torch.float64, device="cuda")
+    _lib.check(lib.ctn_split_gemm_f64(300, 150, 200, A.data_ptr(), B.data_ptr(), C.data_ptr(), precision,
+                                      ws.data_ptr(), _lib.stream_ptr()), "split_gemm")
+    ref = A @ B
+    assert (torch.linalg.matrix_norm(C - ref) / torch.linalg.matrix_norm(ref)).item() < 1e-4

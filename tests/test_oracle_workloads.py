@@ -109,3 +109,17 @@ def test_oracle_mps_heff_times_site_gives_the_energy():
     for k in range(Ls):
         y = OW.mps_heff_times_site(bond_q, bond_d, flats, k)
         assert abs(float(np.dot(flats[k], y)) - E) <= 1e-12 * max(1.0, abs(E))
+
+
+def test_oracle_env_updates_are_the_networks():
+    """env_left / env_right equal dense contractions of the example's networks (small D)."""
+    ops = OW.xxz_two_site(16, seed=6)
+    q, d = OW.u1_sector_sizes(16)
+    A = OW.random_site(q, d, seed=2)
+    Ld, Rd, Md, Ad = ops["L"].dense(), ops["R"].dense(), ops["M1"].dense(), A.dense()
+    ref_l = np.einsum("wap,asb,wnsS,pSq->nbq", Ld, Ad, Md, Ad)
+    got_l = OW.env_left(ops["L"], A, ops["M1"]).dense()
+    assert np.linalg.norm(got_l - ref_l) <= 1e-12 * np.linalg.norm(ref_l)
+    ref_r = np.einsum("asb,nbq,wnsS,pSq->wap", Ad, Rd, Md, Ad)
+    got_r = OW.env_right(ops["R"], A, ops["M1"]).dense()
+    assert np.linalg.norm(got_r - ref_r) <= 1e-12 * np.linalg.norm(ref_r)

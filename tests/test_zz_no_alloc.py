@@ -70,3 +70,52 @@ def test_noalloc_rejects_oversize():
         _lib.check(_lib.lib().ctn_split_gemm_f64_noalloc(8192, 8192, 8192, A.data_ptr(), A.data_ptr(),
                                                          A.data_ptr(), _lib.PRECISIONS["3xtf32"],
                                                          _lib.stream_ptr()), "split_gemm_noalloc")
+
+
+def test_noalloc_allocates_nothing():
+    """After a warm-up call (which loads the kernels), further calls leave the device's free
+    memory and torch's allocator untouched."""
+    from cytnx_b200 import _lib
+
+    p = _lib.PRECISIONS["bf16x3"]
+    g = torch.Generator(device="cuda").manual_seed(5)
+    A = torch.randn(256, 192, dtype=torch.float64, device="cuda", generator=g)
+    B = torch.randn(192, 160, dtype=torch.float64, device="cuda", generator=g)
+    C = torch.empty(256, 160, dtype=torch.float64, device="cuda")
+
+    def call():
+        _lib.check(_lib.lib().ctn_split_gemm_f64_noalloc(256, 160, 192, A.data_ptr(), B.data_ptr(), C.data_ptr(), p,
+                                                         _lib.stream_ptr()), "split_gemm_noalloc")
+
+    call()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    alloc0 = torch.cuda.memory_allocated()
+    for _ in range(3):
+        call()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert torch.cuda.memory_allocated() == alloc0
+
+
+def test_noalloc_size_limit_boundary():
+    """3xTF32 panels take 32 KiB per (128-row tile x 32-wide K slice) for A and B alike: at
+    M = N = 512, K = 4064 (127 slices) the problem fits the 32 MiB array with its tables;
+    K = 4096 (128 slices) fills the array with panels alone and is rejected."""
+    from cytnx_b200 import _lib
+    from cytnx_b200._lib import CytnxError
+
+    p = _lib.PRECISIONS["3xtf32"]
+    g = torch.Generator(device="cuda").manual_seed(9)
+    M = N = 512
+    K = 4064
+    A = torch.randn(M, K, dtype=torch.float64, device="cuda", generator=g)
+    B = torch.randn(K, N, dtype=torch.float64, device="cuda", generator=g)
+    ref = _with_workspace(A, B, p)
+    C = _noalloc(A, B, p)
+    assert torch.linalg.matrix_norm(C - ref).item() / torch.linalg.matrix_norm(ref).item() < tol("3xtf32", K)
+    A2 = torch.zeros(M, 4096, dtype=torch.float64, device="cuda")
+    with pytest.raises(CytnxError, match="static device array"):
+        _lib.check(_lib.lib().ctn_split_gemm_f64_noalloc(M, N, 4096, A2.data_ptr(), A2.data_ptr(), C.data_ptr(), p,
+                                                         _lib.stream_ptr()), "split_gemm_noalloc")
