@@ -616,13 +616,14 @@ def run_batched(args, world, rank, dev, st):
     import cytnx_b200 as c
     from cytnx_b200 import _lib
     from cytnx_b200 import workloads as W
-    from cytnx_b200.batch import BatchedTwoSiteHeff, shard_problems
+    from cytnx_b200.batch import BatchedTwoSiteHeff, problem_flops, shard_problems
 
     t_setup = time.perf_counter()
     dims = W.hubbard_batch_dims(args.batch_problems, seed=0)
-    # cost model for sharding: D^3 (the GEMM flops of a problem grow ~ D^3)
-    mine = shard_problems([float(d) ** 3 for d in dims], world)[rank]
-    probs = W.hubbard_batch([dims[i] for i in mine])
+    # cost model for sharding: each problem's algorithmic flops (host planner, every rank alike)
+    all_probs = W.hubbard_batch(dims)
+    mine = shard_problems([problem_flops(p) for p in all_probs], world)[rank]
+    probs = [all_probs[i] for i in mine]
     data = [W.problem_data(p, 1000 + i) for p, i in zip(probs, mine)]
     out = {"problems": args.batch_problems, "D_range": [128, 2048], "model": "Hubbard U=4 t=1, d=4, (N,2Sz) U(1)xU(1)",
            "sector_sigma": 4.0, "io_dtype": "f32", "shards": world, "forms": {}}
@@ -1091,6 +1092,21 @@ def run_mps_autograd(args, dev):
         errs.append(float(np.linalg.norm(gnum[k].cpu().numpy() - ref) / np.linalg.norm(ref)))
     out["grad_vs_oracle_2HeffA_rel_err_max"] = max(errs)
     out["grad_vs_oracle_2HeffA_sites"] = [0, L // 2, L - 1]
+    # CPU baseline: the same energy and gradient by the oracle's environment sweeps (pairwise
+    # contractions restating BlockUniTensor::contract, OpenBLAS), all host threads
+    t0 = time.perf_counter()
+    num_o, den_o, g_o = OW.mps_energy_grad(bq, bd, flats)
+    cpu_s = time.perf_counter() - t0
+    with torch.no_grad():
+        E_gpu = float(mps.energy(checkpoint_every=4))
+    gd = torch.autograd.grad(mps.energy(checkpoint_every=4), mps.params)
+    gerr = max(float(np.linalg.norm(gd[k].cpu().numpy() - g_o[k]) / max(np.linalg.norm(g_o[k]), 1e-300))
+               for k in (0, L // 2, L - 1))
+    out["cpu_baseline"] = {"eval_grad_s": cpu_s, "cores": os.cpu_count() or 1, "kind": "port",
+                           "sample": "one energy + gradient of the L=32, D=512 MPS by the oracle's left/right "
+                                     "environment sweeps (BlockUniTensor::contract restated, OpenBLAS)",
+                           "energy_rel_diff_vs_gpu": abs(num_o / den_o - E_gpu) / abs(E_gpu),
+                           "grad_rel_diff_vs_gpu_max": gerr}
     if args.mps_lbfgs_steps > 0:
         x = torch.cat([p.detach().reshape(-1) for p in mps.params]).clone().requires_grad_(True)
         opt = torch.optim.LBFGS([x], lr=1.0, max_iter=args.mps_lbfgs_steps, history_size=30,

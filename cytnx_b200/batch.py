@@ -258,6 +258,27 @@ class BatchedTwoSiteHeff:
         return {"step1": best1, "step4": best4, "ms_step1": t1, "ms_step4": t4}
 
 
+def problem_flops(problem) -> float:
+    """Algorithmic flops of one matvec of a structure-only two-site problem (L, M1, M2, R,
+    psi): 2*m*n*k over every block pair of the four contractions L -> M1 -> M2 -> R, counted
+    on the host (the cost model of the sharding)."""
+    from .heff import _struct_contract
+    from .unitensor import contract_plan_flops, structure_only
+
+    L, M1, M2, R, psi = problem
+    P = structure_only(psi.bonds(), ["a", "s1", "s2", "b"])
+    Ls = structure_only(L.bonds(), ["w", "a", "ap"])
+    M1s = structure_only(M1.bonds(), ["w", "w1", "s1", "s1p"])
+    M2s = structure_only(M2.bonds(), ["w1", "w2", "s2", "s2p"])
+    Rs = structure_only(R.bonds(), ["w2", "b", "bp"])
+    f = contract_plan_flops(Ls, P)
+    T = _struct_contract(Ls, P)
+    for X in (M1s, M2s, Rs):
+        f += contract_plan_flops(T, X)
+        T = _struct_contract(T, X)
+    return f
+
+
 def shard_problems(costs: Sequence[float], nshards: int) -> List[List[int]]:
     """Split problems over ``nshards`` ranks by longest-processing-time-first: problems in
     decreasing cost go to the currently lightest shard (ties: lowest rank).  Deterministic,

@@ -341,3 +341,74 @@ def random_site(qv, dv, seed: int) -> BlockTensor:
     itoi = enumerate_blocks(bonds)
     n = sum(int(np.prod([bonds[i].degs[q] for i, q in enumerate(t)])) for t in itoi)
     return BlockTensor.from_flat(bonds, ["a", "s", "b"], 2, itoi, np.random.default_rng(seed).standard_normal(n))
+
+
+def mps_energy_grad(bond_q, bond_d, site_flats, mpo_values=None, phys_q=SPIN_PHYS_Q, inner_q=XXZ_INNER_Q,
+                    left_channel: int = 0, right_channel: int = 4):
+    """<A|H|A>, <A|A> and the gradient of E = <A|H|A>/<A|A> for every site of a finite MPS
+    (real data), by left and right environment sweeps of pairwise contractions (the
+    example's networks): d<A|H|A>/dA_k = 2 H_eff,k A_k, d<A|A>/dA_k = 2 N_eff,k A_k, and
+    dE/dA_k = (2 H_eff,k A_k - 2 E N_eff,k A_k) / <A|A>.  Returns (num, den, [grad_k flat])."""
+    mpo_values = xxz_mpo_values() if mpo_values is None else mpo_values
+    Ls = len(site_flats)
+    syms = [(-1, 1)]
+    V = [Bond(KET, _col(q), d, syms) for q, d in zip(bond_q, bond_d)]
+    phys = Bond(KET, _col(phys_q), [1] * len(phys_q), syms)
+    inner = Bond(KET, _col(inner_q), [1] * len(inner_q), syms)
+    M = _mpo(inner, phys, mpo_values, ["w", "wn", "s", "sp"])
+
+    def site(j, labels, dagger=False):
+        bonds = [V[j], phys.redirect(), V[j + 1].redirect()]
+        itoi = enumerate_blocks(bonds)
+        if dagger:
+            bonds = [b.redirect() for b in bonds]
+        return BlockTensor.from_flat(bonds, labels, 2, itoi, np.asarray(site_flats[j], np.float64))
+
+    def unit(bonds, labels, tup):
+        itoi = enumerate_blocks(bonds)
+        sizes = [int(np.prod([bonds[i].degs[q] for i, q in enumerate(t)])) for t in itoi]
+        flat = np.zeros(sum(sizes))
+        b = [i for i, t in enumerate(itoi.tolist()) if tuple(t) == tuple(tup)][0]
+        flat[sum(sizes[:b])] = 1.0
+        return BlockTensor.from_flat(bonds, labels, 1, itoi, flat)
+
+    def relab(t, m):
+        return t.relabel([m[l] for l in t.labels])
+
+    HL = [unit([inner.redirect(), V[0].redirect(), V[0]], ["w", "a", "ap"], (left_channel, 0, 0))]
+    NL = [unit([V[0].redirect(), V[0]], ["a", "ap"], (0, 0))]
+    for j in range(Ls - 1):
+        A, Ad = site(j, ["a", "s", "b"]), site(j, ["ap", "s", "bp"], True)
+        t = HL[-1].contract(A).contract(M).contract(site(j, ["ap", "sp", "bp"], True))
+        HL.append(relab(t, {"b": "a", "wn": "w", "bp": "ap"}))
+        NL.append(relab(NL[-1].contract(A).contract(Ad), {"b": "a", "bp": "ap"}))
+    HR = [None] * Ls
+    NR = [None] * Ls
+    HR[Ls - 1] = unit([inner, V[Ls], V[Ls].redirect()], ["wn", "b", "bp"], (right_channel, 0, 0))
+    NR[Ls - 1] = unit([V[Ls], V[Ls].redirect()], ["b", "bp"], (0, 0))
+    for j in range(Ls - 1, 0, -1):
+        A, Ad = site(j, ["a", "s", "b"]), site(j, ["ap", "s", "bp"], True)
+        t = A.contract(HR[j]).contract(M).contract(site(j, ["ap", "sp", "bp"], True))
+        HR[j - 1] = relab(t, {"w": "wn", "a": "b", "ap": "bp"})
+        NR[j - 1] = relab(A.contract(NR[j]).contract(Ad), {"a": "b", "ap": "bp"})
+    hA, nA = [], []
+    for k in range(Ls):
+        Ak = site(k, ["a", "s", "b"])
+        Y = HL[k].contract(Ak).contract(M).contract(HR[k])
+        Y = Y.permute([Y.labels.index(l) for l in ("ap", "sp", "bp")])
+        Z = NL[k].contract(Ak).contract(NR[k])
+        Z = Z.permute([Z.labels.index(l) for l in ("ap", "s", "bp")])
+        hA.append(_in_order(Y, Ak))
+        nA.append(_in_order(Z, Ak))
+    a0 = np.asarray(site_flats[0], np.float64)
+    num = float(np.dot(a0, hA[0]))
+    den = float(np.dot(a0, nA[0]))
+    E = num / den
+    grads = [(2.0 * h - 2.0 * E * n) / den for h, n in zip(hA, nA)]
+    return num, den, grads
+
+
+def _in_order(Y: BlockTensor, ref: BlockTensor) -> np.ndarray:
+    """Y's blocks flattened in ref's block order (matched by qnum tuple)."""
+    idx = {tuple(t): i for i, t in enumerate(Y.itoi.tolist())}
+    return np.concatenate([Y.blocks[idx[tuple(t)]].ravel() for t in ref.itoi.tolist()])

@@ -123,3 +123,33 @@ def test_oracle_env_updates_are_the_networks():
     ref_r = np.einsum("asb,nbq,wnsS,pSq->wap", Ad, Rd, Md, Ad)
     got_r = OW.env_right(ops["R"], A, ops["M1"]).dense()
     assert np.linalg.norm(got_r - ref_r) <= 1e-12 * np.linalg.norm(ref_r)
+
+
+def test_oracle_mps_energy_grad_matches_finite_differences():
+    """The oracle's environment-sweep energy and gradient (config-5 CPU baseline) against
+    central finite differences, and its H_eff A against mps_heff_times_site."""
+    rng = np.random.default_rng(8)
+    bond_q = [[0], [-1, 1], [-2, 0, 2], [-1, 1], [0]]
+    bond_d = [[1], [2, 2], [1, 3, 1], [2, 2], [1]]
+    flats = []
+    for j in range(4):
+        V0 = O.Bond(-1, np.array(bond_q[j]).reshape(-1, 1), bond_d[j])
+        V1 = O.Bond(-1, np.array(bond_q[j + 1]).reshape(-1, 1), bond_d[j + 1])
+        ph = O.Bond(-1, np.array([1, -1]).reshape(-1, 1), [1, 1])
+        bonds = [V0, ph.redirect(), V1.redirect()]
+        n = sum(int(np.prod([bonds[i].degs[q] for i, q in enumerate(t)])) for t in O.enumerate_blocks(bonds))
+        flats.append(rng.standard_normal(n))
+    num, den, grads = OW.mps_energy_grad(bond_q, bond_d, flats)
+    for k in range(4):
+        y = OW.mps_heff_times_site(bond_q, bond_d, flats, k)
+        assert abs(float(np.dot(flats[k], y)) - num) <= 1e-12 * abs(num)
+    h = 1e-6
+    for k, i in ((0, 0), (2, 3), (3, 1)):
+        fp = [f.copy() for f in flats]
+        fm = [f.copy() for f in flats]
+        fp[k][i] += h
+        fm[k][i] -= h
+        ep = OW.mps_energy_grad(bond_q, bond_d, fp)
+        em = OW.mps_energy_grad(bond_q, bond_d, fm)
+        fd = (ep[0] / ep[1] - em[0] / em[1]) / (2 * h)
+        assert abs(fd - grads[k][i]) <= 1e-7 * max(1.0, abs(fd))

@@ -72,3 +72,57 @@ def test_two_gloo_ranks_agree_on_shards():
     assert not set(shards[0]) & set(shards[1])
     assert abs(sum(loads) - total) <= 1e-6 * total
     assert max(loads) - min(loads) <= biggest
+
+
+def _rank_matvecs(rank, world, port, result_q):
+    """Each rank takes its LPT shard (flop cost model) of a small Hubbard batch, computes its
+    problems' matvecs (the oracle stands in for the device path on CPU) and the results are
+    gathered by problem index."""
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    from datetime import timedelta
+
+    import numpy as np
+    from cytnx_b200.batch import problem_flops
+    from oracle import workloads as OW
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        dims = [40, 96, 17, 64, 128, 33]
+        costs = [problem_flops(p) for p in W.hubbard_batch(dims)]
+        mine = shard_problems(costs, world)[rank]
+        local = {i: OW.heff_matvec(OW.hubbard_two_site(dims[i], 100 + i)) for i in mine}
+        gathered = [None] * world
+        dist.all_gather_object(gathered, local)
+        if rank == 0:
+            merged = {}
+            for g in gathered:
+                merged.update(g)
+            result_q.put(({i: v.tolist() for i, v in merged.items()}, costs))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_matvecs_gather_to_the_single_rank_result():
+    import numpy as np
+    from oracle import workloads as OW
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_matvecs, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    try:
+        merged, costs = q.get(timeout=180)
+    finally:
+        for p in procs:
+            p.join(timeout=180)
+    assert all(p.exitcode == 0 for p in procs)
+    dims = [40, 96, 17, 64, 128, 33]
+    assert sorted(merged) == list(range(len(dims)))
+    for i, D in enumerate(dims):
+        ref = OW.heff_matvec(OW.hubbard_two_site(D, 100 + i))
+        assert np.array_equal(np.asarray(merged[i]), ref)
+    # the cost model is the algorithmic flop count: larger problems cost more
+    assert costs[4] > costs[1] > costs[0] > costs[2]
