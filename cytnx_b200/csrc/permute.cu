@@ -302,6 +302,25 @@ struct TmaGeom {
 
 __device__ __forceinline__ uint32_t smem32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
+// rotate a 128-bit value (little-endian words) left by `bits` (0..127)
+__device__ __forceinline__ uint4 rotl128(uint4 x, int bits) {
+  const int w = bits >> 5, s = bits & 31;
+  if (w & 2) {
+    uint32_t t = x.x; x.x = x.z; x.z = t;
+    t = x.y; x.y = x.w; x.w = t;
+  }
+  if (w & 1) {
+    const uint32_t t = x.w;
+    x.w = x.z; x.z = x.y; x.y = x.x; x.x = t;
+  }
+  uint4 y;
+  y.x = __funnelshift_l(x.w, x.x, s);
+  y.y = __funnelshift_l(x.x, x.y, s);
+  y.z = __funnelshift_l(x.y, x.z, s);
+  y.w = __funnelshift_l(x.z, x.w, s);
+  return y;
+}
+
 template <int ES>
 __global__ void __launch_bounds__(TMA_THREADS) k_transpose_tma(const __grid_constant__ CUtensorMap in_map,
                                                               uint8_t *__restrict__ dst, TmaGeom g) {
@@ -385,7 +404,18 @@ __global__ void __launch_bounds__(TMA_THREADS) k_transpose_tma(const __grid_cons
     if (g.nbatch > 1) out_base += (int64_t)c.x3 * g.bout[1];
     if (g.nbatch > 2) out_base += (int64_t)c.x4 * g.bout[2];
     const uint8_t *tile = buf[slot];
-    const int ch = threadIdx.x % CHUNKS, ar = threadIdx.x / CHUNKS;
+    // A warp covers CW output vectors (along b) of 32 / CW a rows.  Staged row bl sits at
+    // bl * 128 bytes with its 16-byte chunks XOR-swizzled by (bl & 7), so the rows that the
+    // CW lanes of one a row read at step e must differ in (bl & 7) to reach different
+    // banks: lane ch reads its VEC rows in an order rotated by `rot` and the assembled
+    // vector is rotated back in registers.  Every staged load of the warp is then one
+    // shared-memory wavefront (8 distinct chunks, or lanes sharing a 32-bit word).
+    constexpr int CW = CHUNKS < 8 ? CHUNKS : 8;   // output vectors per a row within a warp
+    constexpr int WG = CHUNKS / CW;               // warps per a row
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int ch_lo = lane % CW;
+    const int ch = (warp % WG) * CW + ch_lo, ar = (warp / WG) * (32 / CW) + lane / CW;
+    const int rot = VEC >= 8 ? (ch_lo * (8 / CW)) & (VEC - 1) : (ch_lo >> 1) & (VEC - 1);
 #pragma unroll
     for (int a_off = 0; a_off < TA; a_off += AROWS) {
       const int al = a_off + ar;  // local a
@@ -399,10 +429,11 @@ __global__ void __launch_bounds__(TMA_THREADS) k_transpose_tma(const __grid_cons
       const int byte = al * ES;
 #pragma unroll
       for (int e = 0; e < VEC; ++e) {
-        const int bl = ch * VEC + e;  // local b = staged row
+        const int bl = ch * VEC + ((e + rot) & (VEC - 1));  // local b = staged row
         const int sw = (((byte >> 4) ^ (bl & 7)) << 4) | (byte & 15);
         v.e[e] = *reinterpret_cast<const T *>(tile + bl * 128 + sw);
       }
+      v.q = rotl128(v.q, rot * ES * 8);  // element j of the vector is staged row ch * VEC + j
       T *o = reinterpret_cast<T *>(dst) + (out_base + ag * g.out_stride_a + bg0);
       const int nvalid = g.nb - bg0 < VEC ? (int)(g.nb - bg0) : VEC;
       if (nvalid == VEC && ((reinterpret_cast<uintptr_t>(o) & 15) == 0)) {
