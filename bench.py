@@ -437,6 +437,23 @@ def main():
         dist.all_reduce(t2, op=dist.ReduceOp.MAX)
     e2e_val = world * flops * args.steps / (float(t2.item()) * 1e-3) / 1e12
 
+    # the host link alone: the same two copies per step, on the same streams, with no matvec
+    torch.cuda.synchronize()
+    e4, e5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e4.record(s_cmp)
+    s_in.wait_stream(s_cmp)
+    s_out.wait_stream(s_cmp)
+    for i in range(args.steps):
+        with torch.cuda.stream(s_in):
+            d_in[i % 2].copy_(h_in, non_blocking=True)
+        with torch.cuda.stream(s_out):
+            h_out[i % 2].copy_(d_out[i % 2], non_blocking=True)
+    s_cmp.wait_stream(s_in)
+    s_cmp.wait_stream(s_out)
+    e5.record(s_cmp)
+    torch.cuda.synchronize()
+    link_ms = e4.elapsed_time(e5) / args.steps
+
     # ---- Lanczos (the reference's Gnd recurrence, fixed iteration count): seconds per step
     lanczos = {}
     for form in forms:
@@ -517,6 +534,7 @@ def main():
                  "kernel_flops_per_matvec": g_flops, "kernel_ms_per_matvec": g_ms})
     clocks = sampler.summary()
     permute = run_permute(args, dev, st, pk.get("hbm_gbs"))
+    prec_floor = run_precision_floor(dev) if rank == 0 else None
     fp64_d1024 = run_fp64_d1024(args, dev, st, dgemm_tflops, rank)
     config1 = run_config1(args, dev, st, dgemm_tflops) if rank == 0 else None
     batched = run_batched(args, world, rank, dev, st) if args.batch_problems > 0 else None
@@ -554,7 +572,10 @@ def main():
             "dE_rel_vs_fp64": refined[args.precision]["dE_rel_vs_fp64"],
             "residual_norm_over_x": refined[args.precision]["residual_abs"],
             "e2e": {"value": e2e_val, "unit": "TFLOP/s", "h2d_bytes_per_step": int(x.numel() * 8),
-                    "d2h_bytes_per_step": int(x.numel() * 8)},
+                    "d2h_bytes_per_step": int(x.numel() * 8), "ms_per_step": float(t2.item()) / args.steps,
+                    "copies_only_ms_per_step": link_ms,
+                    "note": "copies overlap the matvecs; copies_only is the same H2D + D2H pair per step "
+                            "with no compute (the host link's duplex time)"},
             "gpu_launches": head["launches_per_matvec"] * args.steps,
             "roofline": roof,
             "peaks": {"hbm_gbs": pk.get("hbm_gbs"), "bf16_tflops": pk.get("bf16_tflops"), "source": src,
@@ -562,6 +583,7 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cpu,
             "permute": permute,
+            "precision_floor": prec_floor,
             "dense_single_site_D64": config1,
             "fp64_D1024": fp64_d1024,
             "batched_hubbard": batched,
@@ -602,6 +624,64 @@ def oracle_checks(D, ys, ground, energies):
     for f in out["refined"]:
         out["refined"][f]["dE_rel_vs_oracle"] = abs(energies[f] - e_ref) / abs(e_ref) if e_ref else None
     out["host_seconds"] = time.perf_counter() - t0
+    return out
+
+
+def run_precision_floor(dev, M=512, N=512, K=1408, chunks=(1408, 256, 64, 32)):
+    """Where the error of one split-precision product comes from, measured on the device.
+
+    C = A B with A, B ~ N(0, 1) FP64 and K = 1408 (the contraction length of the D=4096 step-4
+    GEMM).  For each split form: the relative Frobenius error of the tensor-core GEMM against
+    FP64 when K is cut into chunks whose partial products are summed in FP64 (chunk = K: one
+    FP32 accumulation over the whole K, the product as the matvec runs it; chunk = one K slice
+    of the panel layout: the accumulator leaves FP32 after every slice), and the floor of the
+    split representation itself (hi*hi + hi*lo + lo*hi of the same rounded values, summed
+    exactly in FP64)."""
+    import torch
+
+    from cytnx_b200 import _lib
+
+    g = torch.Generator(device=dev).manual_seed(2024)
+    A = torch.randn(M, K, dtype=torch.float64, device=dev, generator=g)
+    B = torch.randn(K, N, dtype=torch.float64, device=dev, generator=g)
+    ref = A @ B
+    nref = torch.linalg.matrix_norm(ref)
+
+    def split_gemm(a, b, p):
+        m, k = a.shape
+        n = b.shape[1]
+        ws = torch.empty(_lib.lib().ctn_split_gemm_workspace_bytes(m, n, k, p), dtype=torch.uint8, device=dev)
+        c = torch.empty(m, n, dtype=torch.float64, device=dev)
+        _lib.check(_lib.lib().ctn_split_gemm_f64(m, n, k, a.data_ptr(), b.data_ptr(), c.data_ptr(), p, ws.data_ptr(),
+                                                 _lib.stream_ptr()), "precision_floor")
+        return c
+
+    def tf32(x32):  # round to nearest, ties away (cvt.rna.tf32.f32)
+        bits = x32.view(torch.int32)
+        return ((bits + 0x1000) & -0x2000).view(torch.float32)
+
+    def rnd(x, form):
+        return tf32(x.float()) if form == "3xtf32" else x.to(torch.bfloat16)
+
+    out = {"M": M, "N": N, "K": K}
+    for form in ("3xtf32", "bf16x3"):
+        p = _lib.PRECISIONS[form]
+        row = {}
+        for ch in chunks:
+            C = torch.zeros_like(ref)
+            for k0 in range(0, K, ch):
+                C += split_gemm(A[:, k0:k0 + ch].contiguous(), B[k0:k0 + ch].contiguous(), p)
+            row[str(ch)] = float((torch.linalg.matrix_norm(C - ref) / nref).item())
+        ah = rnd(A, form).double()
+        al = rnd(A - ah, form).double()
+        bh = rnd(B, form).double()
+        bl = rnd(B - bh, form).double()
+        rep = ah @ bh + ah @ bl + al @ bh
+        out[form] = {"rel_err_by_fp64_chunk": row,
+                     "representation_floor": float((torch.linalg.matrix_norm(rep - ref) / nref).item())}
+    out["note"] = ("the per-chunk errors fall with the chunk length down to one K slice (the tensor pipe "
+                   "accumulates in FP32, so the error of one product grows with K); the 3xTF32 error at one "
+                   "K slice is the smallest any FP32-accumulated split product reaches")
     return out
 
 

@@ -448,8 +448,8 @@ extern "C" ctn_status ctn_heff2_set_epilogue(ctn_heff2_plan *p, int precision, i
   CTN_REQUIRE(p, "ctn_heff2_set_epilogue: null plan");
   CTN_REQUIRE(precision == CTN_PREC_3XTF32 || precision == CTN_PREC_BF16X3,
               "ctn_heff2_set_epilogue: split precision only");
-  CTN_REQUIRE(epi_step1 >= -1 && epi_step1 <= 1 && epi_step4 >= -1 && epi_step4 <= 1,
-              "ctn_heff2_set_epilogue: -1 (automatic), 0 (direct) or 1 (staged)");
+  CTN_REQUIRE(epi_step1 >= -1 && epi_step1 <= 2 && epi_step4 >= -1 && epi_step4 <= 2,
+              "ctn_heff2_set_epilogue: -1 (automatic), 0 (direct), 1 (staged) or 2 (fragments)");
   const int k = split_kind(precision);
   p->split_epi[k][0] = epi_step1;
   p->split_epi[k][1] = epi_step4;

@@ -313,7 +313,8 @@ ctn_status heff_split_prepare(ctn_heff2_plan *p, int kind) {
     if (p_group[q] < 0) continue;
     const TcGroup &g = s->g1.groups[p_group[q]];
     const BlkInfo &b = p->Pb[q];  // [a][1][1][b]: element (row b, k a) at off + k*d3 + row
-    PackSeg sg{b.off, 1, b.d[3], (int32_t)b.d[3], (int32_t)b.d[0], (int32_t)p_col[q], 0, g.b_off, bn, g.kb};
+    PackSeg sg{b.off, 1, b.d[3], (int32_t)b.d[3], (int32_t)b.d[0], (int32_t)p_col[q], 0, g.b_off,
+               s->g1.b_tile_rows(), g.kb};
     s->pk_P.segs.push_back(sg);
   }
   s->pk_L.finalize();
@@ -351,7 +352,8 @@ ctn_status heff_split_prepare(ctn_heff2_plan *p, int kind) {
     if (r_group[r] < 0) continue;
     const TcGroup &g = s->g4.groups[r_group[r]];
     const BlkInfo &b = p->Rb[r];  // [w2][b][b']: element (row b', k b) at off + k*d2 + row
-    PackSeg sg{b.off, 1, b.d[2], (int32_t)b.d[2], (int32_t)b.d[1], 0, (int32_t)r_k[r], g.b_off, s->g4.bn, g.kb};
+    PackSeg sg{b.off, 1, b.d[2], (int32_t)b.d[2], (int32_t)b.d[1], 0, (int32_t)r_k[r], g.b_off,
+               s->g4.b_tile_rows(), g.kb};
     s->pk_R.segs.push_back(sg);
   }
   s->pk_R.finalize();
@@ -416,8 +418,8 @@ ctn_status heff_split_prepare(ctn_heff2_plan *p, int kind) {
 void heff_split_apply_epilogue(ctn_heff2_plan *p, int kind) {
   HeffSplit *s = p->split[kind];
   if (!s) return;
-  s->g1.epi_staged = p->split_epi[kind][0] < 0 ? s->g1.epi_auto : p->split_epi[kind][0] != 0;
-  s->g4.epi_staged = p->split_epi[kind][1] < 0 ? s->g4.epi_auto : p->split_epi[kind][1] != 0;
+  s->g1.epi_staged = p->split_epi[kind][0] < 0 ? s->g1.epi_auto : p->split_epi[kind][0];
+  s->g4.epi_staged = p->split_epi[kind][1] < 0 ? s->g4.epi_auto : p->split_epi[kind][1];
 }
 
 ctn_status heff_split_stats(const ctn_heff2_plan *p, int kind, double *out) {

@@ -112,6 +112,41 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
       : "r"(addr));
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// 16 TMEM lanes x 32 columns (four 256-bit groups): lane t of the warp receives, for group j,
+// r[4j], r[4j+1] = row (t / 4), columns 8j + 2 (t % 4) + {0, 1} and r[4j+2], r[4j+3] = the same
+// columns of row (t / 4) + 8 (rows relative to the lane in `addr`)
+__device__ __forceinline__ void tmem_ld_frag16(uint32_t addr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.16x256b.x4.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(addr));
+}
+// two adjacent output columns (col, col + 1) of one row from registers: FP32 row-strided or
+// row-mapped output (8-byte store when aligned) or FP64 row-mapped output (16-byte store)
+__device__ __forceinline__ void epi_store_pair(int mode, int64_t dst, int col, int ncols, uint32_t a, uint32_t b,
+                                               float *c32, double *c64) {
+  if (dst < 0 || col >= ncols) return;
+  const int64_t o = dst + col;
+  const bool two = col + 1 < ncols;
+  if (mode != 1) {
+    float *q = c32 + o;
+    if (two && (o & 1) == 0) {
+      *reinterpret_cast<float2 *>(q) = make_float2(__uint_as_float(a), __uint_as_float(b));
+    } else {
+      q[0] = __uint_as_float(a);
+      if (two) q[1] = __uint_as_float(b);
+    }
+  } else {
+    double *q = c64 + o;
+    if (two && (o & 1) == 0) {
+      *reinterpret_cast<double2 *>(q) = make_double2((double)__uint_as_float(a), (double)__uint_as_float(b));
+    } else {
+      q[0] = (double)__uint_as_float(a);
+      if (two) q[1] = (double)__uint_as_float(b);
+    }
+  }
+}
 
 // Epilogue store of one 32-column piece of a warp's 32 accumulator rows.  Each lane holds
 // its row's 32 FP32 values (TMEM lane = row); they are staged in the warp's padded
@@ -391,11 +426,43 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
       // 4 KB box (SWIZZLE_128B layout, conflict-free) and one lane stores it with a 2-D TMA
       // store; rows past M and columns past N are clipped by the tensor map.  The box is
       // reused once the previous store has read it (bulk-group wait on the read).
-      const bool tma_out = p.cmaps != nullptr && g.mode == 0 && p.epi_staged;
+      const bool tma_out = p.cmaps != nullptr && g.mode == 0 && p.epi_staged == 1;
       // row-mapped FP64 groups launched with only an FP32 output go out as FP32 (mode 2)
       const int mode = (g.mode == 1 && p.c64 == nullptr) ? 2 : g.mode;
+      // Fragment form (epi_staged == 2): no shared memory at all.  16-lane x 32-column TMEM
+      // fragments put 4 lanes on 8 consecutive columns of one row, so each store instruction
+      // writes 8 rows x 32 bytes (FP32) or 8 x 64 bytes (FP64) of whole sectors straight from
+      // registers; the main loop of the next tile keeps the shared-memory bandwidth, which the
+      // operand copies and the three products' operand reads already fill.
+      if (p.epi_staged == 2) {
 #pragma unroll 1
-      for (int c0 = 0; c0 < BN && any_row; c0 += 32) {
+        for (int h = 0; h < 2 && any_row; ++h) {
+          const int ra = tl.mt * TC_BM + q * 32 + 16 * h + (lane >> 2), rb = ra + 8;
+          int64_t da = -1, db = -1;
+          if (ra < g.M) da = g.mode == 0 ? g.c_off + (int64_t)ra * g.ldc : p.rowmap[g.rm_off + ra];
+          if (rb < g.M) db = g.mode == 0 ? g.c_off + (int64_t)rb * g.ldc : p.rowmap[g.rm_off + rb];
+          if (!__any_sync(0xffffffffu, da >= 0 || db >= 0)) continue;  // warp-uniform
+          const uint32_t hb = base + ((uint32_t)(16 * h) << 16);
+          // columns of this tile only: a 32-column fragment may reach past BN (into the other
+          // accumulator's columns), which belong to the next tile
+          const int cend = min(g.N, (tl.nt + 1) * BN);
+#pragma unroll 1
+          for (int c0 = 0; c0 < BN; c0 += 32) {
+            if (tl.nt * BN + c0 >= g.N) break;  // warp-uniform: past the group's last column
+            uint32_t v[16];
+            tmem_ld_frag16(hb + c0, v);
+            tmem_wait_ld();
+            const int cb = tl.nt * BN + c0 + 2 * (lane & 3);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              epi_store_pair(mode, da, cb + 8 * j, cend, v[4 * j], v[4 * j + 1], p.c32, p.c64);
+              epi_store_pair(mode, db, cb + 8 * j, cend, v[4 * j + 2], v[4 * j + 3], p.c32, p.c64);
+            }
+          }
+        }
+      }
+#pragma unroll 1
+      for (int c0 = 0; c0 < BN && any_row && p.epi_staged != 2; c0 += 32) {
         uint32_t v[32];
         tmem_ld16(base + c0, *reinterpret_cast<uint32_t(*)[16]>(&v[0]));
         tmem_ld16(base + c0 + 16, *reinterpret_cast<uint32_t(*)[16]>(&v[16]));
@@ -403,7 +470,11 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
         const int cg0 = tl.nt * BN + c0;
         if (cg0 >= g.N) continue;  // warp-uniform: the whole piece is past the tile edge
         const int ncol = min(min(32, BN - c0), g.N - cg0);  // a 32-column piece may pass the tile edge
-        if (tma_out) {
+        // a 32 x 32 TMA box is clipped at the group's last column only: a piece that passes the
+        // tile edge while the group goes on (BN not a multiple of 32) is stored directly
+        if (tma_out && c0 + 32 > BN && (tl.nt + 1) * BN < g.N) {
+          if (dst >= 0) epi_store_direct(v, dst, cg0, ncol, mode, p.c32, p.c64);
+        } else if (tma_out) {
           uint8_t *box = reinterpret_cast<uint8_t *>(smem + SM::EPI_OFF) +
                          (SM::EPI_DB ? (warp - 2) * 8192 + (pieces & 1) * 4096 : (warp - 2) * 4096);
           if (lane == 0) {
@@ -431,7 +502,7 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
                 : "memory");
             asm volatile("cp.async.bulk.commit_group;" ::: "memory");
           }
-        } else if (p.epi_staged) {
+        } else if (p.epi_staged == 1) {
           epi_store_piece(v, slab, lane, dst, cg0, ncol, mode, p.c32, p.c64);
         } else if (dst >= 0) {
           epi_store_direct(v, dst, cg0, ncol, mode, p.c32, p.c64);
@@ -599,14 +670,13 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p, con
         if (rank == 0) mbar_expect_tx(&full[stage], 2 * SM::STAGE_BYTES);
         const uint32_t fb = peer_addr(&full[stage], 0);
         // panel rows of 128 bytes: A tile (mt128, kb) hi + lo (256 rows, one box) and this
-        // CTA's half of the hi and of the lo B tile (nt, kb); a full B tile is BN rows hi then
-        // BN rows lo (SM::B_BYTES is half a tile)
+        // CTA's half of the B tile (nt, kb): the B panels of the 2-CTA form hold BN/2-row tiles
+        // (hi then lo), half 2 nt + rank, so it is one box of BN rows as well
         const int ya = (int)((g.a_off + ((int64_t)mt128 * g.kb + kb) * (2 * SM::A_BYTES)) / TC_ROW_BYTES);
-        const int yb = (int)((g.b_off + ((int64_t)tl.nt * g.kb + kb) * (4 * SM::B_BYTES) + (int64_t)rank * SM::B_BYTES) /
-                             TC_ROW_BYTES);
+        const int yb =
+            (int)((g.b_off + ((int64_t)(2 * tl.nt + (int)rank) * g.kb + kb) * (2 * SM::B_BYTES)) / TC_ROW_BYTES);
         tma_rows_pair(st, &ta, ya, fb);
         tma_rows_pair(st + 2 * SM::A_BYTES, &tb, yb, fb);
-        tma_rows_pair(st + 2 * SM::A_BYTES + SM::B_BYTES, &tb, yb + 2 * SM::B_BYTES / TC_ROW_BYTES, fb);
         filled[stage]++;
         if (++stage == STAGES) {
           stage = 0;
@@ -688,7 +758,7 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p, con
       if (r < g.M) dst = g.mode == 0 ? g.c_off + (int64_t)r * g.ldc : p.rowmap[g.rm_off + r];
       const bool any_row = __any_sync(0xffffffffu, dst >= 0);  // warp-uniform: rows of this quarter inside M
       // row-strided FP32 output with a tensor map: TMA stores of 32 x 32 pieces (as in k_tc_gemm)
-      const bool tma_out = p.cmaps != nullptr && g.mode == 0 && p.epi_staged;
+      const bool tma_out = p.cmaps != nullptr && g.mode == 0 && p.epi_staged != 0;
       // row-mapped FP64 groups launched with only an FP32 output go out as FP32 (mode 2)
       const int mode = (g.mode == 1 && p.c64 == nullptr) ? 2 : g.mode;
       uint8_t *box = reinterpret_cast<uint8_t *>(smem + SM::EPI_OFF) + (warp - 2) * 4096;
@@ -701,7 +771,11 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p, con
         const int cg0 = tl.nt * BN + c0;
         if (cg0 >= g.N) continue;  // warp-uniform: the whole piece is past the tile edge
         const int ncol = min(min(32, BN - c0), g.N - cg0);  // a 32-column piece may pass the tile edge
-        if (tma_out) {
+        // a 32 x 32 TMA box is clipped at the group's last column only: a piece that passes the
+        // tile edge while the group goes on (BN not a multiple of 32) is stored directly
+        if (tma_out && c0 + 32 > BN && (tl.nt + 1) * BN < g.N) {
+          if (dst >= 0) epi_store_direct(v, dst, cg0, ncol, mode, p.c32, p.c64);
+        } else if (tma_out) {
           if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
           __syncwarp();
 #pragma unroll
@@ -721,7 +795,7 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p, con
                 : "memory");
             asm volatile("cp.async.bulk.commit_group;" ::: "memory");
           }
-        } else if (p.epi_staged) {
+        } else if (p.epi_staged) {  // the 2-CTA form has no fragment form: staged for 1 and 2
           epi_store_piece(v, slab, lane, dst, cg0, ncol, mode, p.c32, p.c64);
         } else if (dst >= 0) {
           epi_store_direct(v, dst, cg0, ncol, mode, p.c32, p.c64);
@@ -1049,7 +1123,7 @@ ctn_status launch_tc_pair(const TcParams &prm, int64_t ntiles, cudaStream_t st) 
   CTN_REQUIRE(prm.a_bytes > 0 && prm.b_bytes > 0 && prm.a_bytes % 128 == 0 && prm.b_bytes % 128 == 0,
               "tcgen05 2-CTA GEMM: panel sizes unknown");
   CTN_TRY(encode_rows_map(&ma, prm.a, prm.a_bytes, 2 * TC_BM));  // hi + lo of one A tile per box
-  CTN_TRY(encode_rows_map(&mb, prm.b, prm.b_bytes, BN / 2));
+  CTN_TRY(encode_rows_map(&mb, prm.b, prm.b_bytes, BN));  // hi + lo of one BN/2-row half tile per box
   CTN_CUDA(cudaLaunchKernelEx(&cfg, k_tc_gemm_pair<KIND, BN, STAGES>, prm, ma, mb));
   return CTN_OK;
 }
@@ -1150,7 +1224,7 @@ void TcGemm::finalize() {
     used += (double)g.M * g.N;
     cover += (double)(pair ? (g.mt + 1) / 2 * 2 : g.mt) * TC_BM * (double)g.nt * bn;
   }
-  epi_staged = epi_auto = cover > 0.0 && used >= 0.5 * cover;
+  epi_staged = epi_auto = (cover > 0.0 && used >= 0.5 * cover) ? 1 : 0;
   std::vector<std::pair<int, TcTile>> tmp;
   for (size_t i = 0; i < groups.size(); ++i) {
     const TcGroup &g = groups[i];
@@ -1274,7 +1348,7 @@ ctn_status TcGemm::run(const uint8_t *a, const uint8_t *b, float *c32, double *c
   prm.tiles = (const TcTile *)(q + groups.size() * sizeof(TcGroup));
   prm.rowmap = (const int64_t *)(q + groups.size() * sizeof(TcGroup) + tiles.size() * sizeof(TcTile));
   prm.ntiles = (int64_t)tiles.size();
-  prm.epi_staged = epi_staged ? 1 : 0;
+  prm.epi_staged = epi_staged;
   prm.a_bytes = a_bytes;
   prm.b_bytes = b_bytes;
   prm.a = a;

@@ -54,7 +54,8 @@ struct TcParams {
   double *c64;
   const int64_t *rowmap;
   int *err;  // device error word: 0 ok, else the code of the wait that gave up
-  int epi_staged;  // 1: epilogue through the shared-memory slab (whole row segments), 0: direct
+  int epi_staged;  // epilogue form: 1 through shared memory (whole row segments / TMA stores),
+                   // 2 from 16-lane TMEM fragments straight to global memory, 0 one row per lane
   int64_t a_bytes, b_bytes;  // panel sizes, hi and lo (2-CTA form: extents of its TMA views)
   // one 2-D FP32 tensor map per group (CUtensorMap, 128 bytes each) over the row-strided
   // output of mode-0 groups, or null: the staged epilogue then stores 32 x 32 pieces by TMA
@@ -93,8 +94,11 @@ struct TcGemm {
     bn = w < 0 ? -w : w;
   }
   int width() const { return pair ? -bn : bn; }
-  bool epi_staged = false;  // chosen in finalize from the output mode and the tile fill
-  bool epi_auto = false;    // finalize's choice (restored by an automatic setting)
+  // rows per B panel tile: the 2-CTA form stores each BN-wide tile as two BN/2-row tiles, so
+  // that the half a CTA of the pair loads (hi and lo) is one contiguous copy
+  int b_tile_rows() const { return pair ? bn / 2 : bn; }
+  int epi_staged = 0;  // epilogue form (TcParams::epi_staged), chosen in finalize from the tile fill
+  int epi_auto = 0;    // finalize's choice (restored by an automatic setting)
   std::vector<TcGroup> groups;
   std::vector<TcTile> tiles;
   std::vector<int64_t> rowmap;

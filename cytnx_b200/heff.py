@@ -23,6 +23,8 @@ from .core import Device, Tensor, Type, require_cuda
 from .network import LinOp
 from .unitensor import UniTensor, UTenType, _desc, contract_plan_flops, layout_for, structure_only
 
+_EPI = {0: "direct", 1: "staged", 2: "fragments"}  # tensor-core GEMM epilogue forms
+
 
 def _plain_desc(u: UniTensor, keep):
     if u.uten_type() != UTenType.Block:
@@ -121,12 +123,13 @@ class TwoSiteHeff(LinOp):
         self._bound.discard(prec)
 
     def autotune(self, precision: Optional[str] = None, step1=(128, 160, 192, 256, -192),
-                 step4=(96, 128, 144, 160, 256, -128), reps: int = 5, epilogues=(0, 1)) -> dict:
+                 step4=(96, 128, 144, 160, 256, -128), reps: int = 5, epilogues=(0, 1, 2)) -> dict:
         """Pick the tensor-core tile width and epilogue form of steps 1 and 4 by timing them.
 
         The two GEMMs are independent kernels, so each is tuned with the other fixed:
         every width re-packs the operand panels (they depend on the width); for each
-        width both epilogue forms (0 direct, 1 staged through shared memory) are timed
+        width the epilogue forms (0 direct, 1 staged through shared memory, 2 TMEM fragments
+        stored from registers) are timed
         with the per-phase CUDA-event profile (ctn_heff2_profile).  Negative widths are the
         2-CTA tiles (256 rows, cluster of two SMs); one of each step is a default candidate."""
         import ctypes as ct
@@ -161,8 +164,8 @@ class TwoSiteHeff(LinOp):
         self.bind(precision)
         _lib.check(_lib.lib().ctn_heff2_set_epilogue(self._h, prec, best1[1], best4[1]), "autotune")
         return {"step1": best1[0], "step4": best4[0], "epilogue": [best1[1], best4[1]],
-                "ms_step1": {f"{k[0]}/{'staged' if k[1] else 'direct'}": v for k, v in table["step1"].items()},
-                "ms_step4": {f"{k[0]}/{'staged' if k[1] else 'direct'}": v for k, v in table["step4"].items()}}
+                "ms_step1": {f"{k[0]}/{_EPI[k[1]]}": v for k, v in table["step1"].items()},
+                "ms_step4": {f"{k[0]}/{_EPI[k[1]]}": v for k, v in table["step4"].items()}}
 
     # ---------------------------------------------------------------- Lanczos without Python callbacks
     def lanczos(self, psi0: UniTensor, maxiter: int = 40, cvgcrit: float = 1e-14,

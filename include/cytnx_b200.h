@@ -268,8 +268,9 @@ void ctn_heff2_plan_destroy(ctn_heff2_plan *plan);
 ctn_status ctn_heff2_set_tiles(ctn_heff2_plan *plan, int precision, int bn_step1, int bn_step4);
 /* epilogue form of the step-1 / step-4 tensor-core GEMMs: -1 automatic (staged through
  * shared memory when the tiles are at least half filled), 0 direct
- * (each lane stores its own accumulator row), 1 staged (whole row segments per store).
- * Takes effect on the next matvec; used by the autotuner. */
+ * (each lane stores its own accumulator row), 1 staged (whole row segments per store),
+ * 2 fragments (16-lane TMEM fragments stored from registers, no shared memory; the 2-CTA
+ * tiles run 2 as 1).  Takes effect on the next matvec; used by the autotuner. */
 ctn_status ctn_heff2_set_epilogue(ctn_heff2_plan *plan, int precision, int epi_step1, int epi_step4);
 
 /* ---------------------------------------------------------------- batched H_eff

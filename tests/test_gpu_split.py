@@ -95,7 +95,9 @@ def test_heff_split_tile_widths_agree(prec):
         err = (torch.linalg.vector_norm(y - y64) / torch.linalg.vector_norm(y64)).item()
         assert err < (1e-5 if prec == "3xtf32" else 2e-3), (b1, b4, err)
     tuned = H.autotune(prec, reps=2)
-    assert tuned["step1"] in (128, 160, 192, 256) and tuned["step4"] in (96, 128, 144, 160, 256)
+    # any of the default candidates (1-CTA widths and one 2-CTA width per step)
+    assert tuned["step1"] in (128, 160, 192, 256, -192) and tuned["step4"] in (96, 128, 144, 160, 256, -128)
+    assert tuned["epilogue"][0] in (0, 1, 2) and tuned["epilogue"][1] in (0, 1, 2)
 
 
 @pytest.mark.parametrize("prec", ["3xtf32", "bf16x3"])
@@ -120,17 +122,28 @@ def test_heff_split_pair_tiles_match_single_cta(prec):
 
 @pytest.mark.parametrize("prec", ["3xtf32", "bf16x3"])
 def test_epilogue_forms_are_bitwise_equal(prec):
-    """The direct and the shared-memory-staged epilogues store the same accumulators."""
+    """The direct, the shared-memory-staged and the TMEM-fragment epilogues store the same
+    accumulators (tile widths that are not multiples of 32 included: a fragment reaching past
+    the tile edge must not write the next tile's columns)."""
     from cytnx_b200 import _lib
 
     psi, H = _heff(384, seed=10)
     x = psi.flat_view()
     H.set_tiles(160, 144, prec)
     out = []
-    for e1, e4 in [(0, 0), (1, 1), (0, 1), (-1, -1)]:
+    for e1, e4 in [(0, 0), (1, 1), (0, 1), (-1, -1), (2, 2), (2, 0), (1, 2)]:
         _lib.check(_lib.lib().ctn_heff2_set_epilogue(H._h, _lib.PRECISIONS[prec], e1, e4))
         y = torch.zeros_like(x)
         H.apply_flat(x, y, prec)
         out.append(y)
     for y in out[1:]:
         assert torch.equal(y, out[0])
+    for b1, b4 in [(48, 96), (256, 128), (-128, 128)]:  # and other widths (2-CTA: 2 runs as staged)
+        H.set_tiles(b1, b4, prec)
+        ys = []
+        for e in (1, 2):
+            _lib.check(_lib.lib().ctn_heff2_set_epilogue(H._h, _lib.PRECISIONS[prec], e, e))
+            y = torch.zeros_like(x)
+            H.apply_flat(x, y, prec)
+            ys.append(y)
+        assert torch.equal(ys[0], ys[1]), (b1, b4)
