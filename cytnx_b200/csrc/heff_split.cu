@@ -135,10 +135,10 @@ __device__ __forceinline__ void mpo_store(const float (&x)[8], const MpoSegS &s,
   // panel offset (32-bit index math except the final byte offset)
   const int row = s.row0 + r, kabs = s.k0 + kloc;
   const int rr = row & (TC_BM - 1);
-  const int kslice = TF ? (kabs >> 5) : (kabs >> 6);
-  const int byte = TF ? ((kabs & 31) << 2) : ((kabs & 63) << 1);
-  const int64_t off = s.panel_off + ((int64_t)(row >> 7) * s.kb + kslice) * (2 * TC_A_TILE) + (rr >> 3) * 1024 +
-                      (rr & 7) * 128 + (((byte >> 4) ^ (rr & 7)) << 4);  // hi tile; lo = hi + TC_A_TILE
+  const int kslice = TF ? (kabs >> 4) : (kabs >> 5);  // 64-byte K slices: 16 TF32 / 32 BF16
+  const int byte = TF ? ((kabs & 15) << 2) : ((kabs & 31) << 1);
+  const int64_t off = s.panel_off + ((int64_t)(row >> 7) * s.kb + kslice) * (2 * TC_A_TILE) +
+                      tc_tile_byte(rr, byte);  // hi tile; lo = hi + TC_A_TILE
   if (TF) {
     float h[4], l[4];
 #pragma unroll

@@ -78,9 +78,13 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
 }
 
 
+// UMMA shared-memory descriptor of a K-major SWIZZLE_64B operand tile: start address, stride
+// byte offset = one 8-row atom (512 B), descriptor version 1, layout type 4 (64-byte swizzle);
+// the leading byte offset is unused for K-major swizzled operands
 __device__ __forceinline__ uint64_t smem_desc(const void *p) {
   const uint64_t a = smem_u32(p);
-  return ((a & 0x3FFFFull) >> 4) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+  return ((a & 0x3FFFFull) >> 4) | (1ull << 16) | ((uint64_t)(TC_ATOM_BYTES >> 4) << 32) | (1ull << 46) |
+         (4ull << 61);
 }
 
 __device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -237,11 +241,16 @@ __device__ __forceinline__ void epi_store_direct(const uint32_t (&v)[32], int64_
   }
 }
 
-template <int KIND, int BN, int STAGES>
+// A stage holds SPS consecutive K slices: [SPS A tile pairs (hi, lo)][SPS B tile pairs].  The
+// K slices of one row tile are consecutive tiles in the panels, so each operand of a stage is
+// one bulk copy of SPS tile pairs; two slices per stage (long-K groups) keep the copies large,
+// one slice per stage (short-K groups) keeps the ring deep.
+template <int KIND, int BN, int STAGES, int SPS>
 struct TcSmem {
   static constexpr int A_BYTES = TC_A_TILE;
   static constexpr int B_BYTES = BN * TC_ROW_BYTES;
-  static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+  static constexpr int B_OFF = SPS * 2 * A_BYTES;  // the B tile pairs of a stage
+  static constexpr int STAGE_BYTES = SPS * (2 * A_BYTES + 2 * B_BYTES);
   static constexpr int RING = STAGES * STAGE_BYTES;
   static constexpr int BAR_OFF = RING;                 // full[S], empty[S], tfull[2], tempty[2], drain
   static constexpr int EPI_OFF = RING + 1024;  // four warps' epilogue slabs (1024-aligned: TMA store boxes)
@@ -252,9 +261,9 @@ struct TcSmem {
   static constexpr int TOTAL = EPI_OFF + (EPI_DB ? EPI_DB_BYTES : EPI_BYTES);
 };
 
-template <int KIND, int BN, int STAGES>
+template <int KIND, int BN, int STAGES, int SPS>
 __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
-  using SM = TcSmem<KIND, BN, STAGES>;
+  using SM = TcSmem<KIND, BN, STAGES, SPS>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t *full = (uint64_t *)(smem + SM::BAR_OFF);
@@ -298,7 +307,7 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
     const int rem = g.N - tl.nt * BN;
     return rem >= BN ? BN : ((rem + 15) & ~15);
   };
-  constexpr int KSTEPS = 4;  // MMA K per instruction = 32 bytes of the 128-byte slice
+  constexpr int KSTEPS = TC_ROW_BYTES / 32;  // MMA K per instruction = 32 bytes of the 64-byte slice
 
   if (warp == 0 && lane == 0) {
     // ---------------------------------------------------------------- producer
@@ -311,7 +320,8 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
       const TcTile tl = p.tiles[t];
       const TcGroup g = p.groups[tl.group];
       const uint32_t b_bytes = (uint32_t)tile_n(g, tl) * TC_ROW_BYTES;  // the tile's B rows only
-      for (int kb = 0; kb < g.kb; ++kb) {
+      for (int kb = 0; kb < g.kb; kb += SPS) {
+        const int n = min(SPS, g.kb - kb);  // K slices in this stage
         if (!mbar_wait(&empty[stage], phase ^ 1, p.err, 1, p.spin_limit)) {
           ok = false;
           break;
@@ -324,16 +334,21 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
           continue;
         }
         uint8_t *st = smem + stage * SM::STAGE_BYTES;
-        mbar_expect_tx(&full[stage], 2 * SM::A_BYTES + 2 * b_bytes);
-        // tiles are stored hi then lo: A's pair is one copy, B's too when the tile is full width
+        mbar_expect_tx(&full[stage], (uint32_t)n * (2 * SM::A_BYTES + 2 * b_bytes));
+        // tiles are stored hi then lo and the K slices of a row tile back to back: A's n pairs are
+        // one copy, B's too when the tile is full width
         const int64_t ao = g.a_off + ((int64_t)tl.mt * g.kb + kb) * (2 * SM::A_BYTES);
         const int64_t bo = g.b_off + ((int64_t)tl.nt * g.kb + kb) * (2 * SM::B_BYTES);
-        bulk_g2s(st, p.a + ao, 2 * SM::A_BYTES, &full[stage]);
+        bulk_g2s(st, p.a + ao, (uint32_t)n * 2 * SM::A_BYTES, &full[stage]);
         if (b_bytes == (uint32_t)SM::B_BYTES) {
-          bulk_g2s(st + 2 * SM::A_BYTES, p.b + bo, 2 * SM::B_BYTES, &full[stage]);
+          bulk_g2s(st + SM::B_OFF, p.b + bo, (uint32_t)n * 2 * SM::B_BYTES, &full[stage]);
         } else {
-          bulk_g2s(st + 2 * SM::A_BYTES, p.b + bo, b_bytes, &full[stage]);
-          bulk_g2s(st + 2 * SM::A_BYTES + SM::B_BYTES, p.b + bo + SM::B_BYTES, b_bytes, &full[stage]);
+          for (int q = 0; q < n; ++q) {
+            uint8_t *sb = st + SM::B_OFF + q * 2 * SM::B_BYTES;
+            const int64_t bq = bo + (int64_t)q * 2 * SM::B_BYTES;
+            bulk_g2s(sb, p.b + bq, b_bytes, &full[stage]);
+            bulk_g2s(sb + SM::B_BYTES, p.b + bq + SM::B_BYTES, b_bytes, &full[stage]);
+          }
         }
         filled[stage]++;
         if (++stage == STAGES) {
@@ -360,21 +375,27 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
       if (!mbar_wait(&tempty[acc], acc_phase ^ 1, p.err, 2, p.spin_limit)) break;
       tc_fence_after();
       const uint32_t d = tmem_base + (uint32_t)(acc * BN);
-      for (int kb = 0; kb < g.kb; ++kb) {
+      for (int kb = 0; kb < g.kb; kb += SPS) {
+        const int n = min(SPS, g.kb - kb);
         if (!mbar_wait(&full[stage], phase, p.err, 3, p.spin_limit)) {
           ok = false;
           break;
         }
         tc_fence_after();
         uint8_t *st = smem + stage * SM::STAGE_BYTES;
-        const uint64_t ahi = smem_desc(st), alo = smem_desc(st + SM::A_BYTES);
-        const uint64_t bhi = smem_desc(st + 2 * SM::A_BYTES), blo = smem_desc(st + 2 * SM::A_BYTES + SM::B_BYTES);
 #pragma unroll
-        for (int j = 0; j < KSTEPS; ++j) {
-          const uint64_t adv = (uint64_t)(j * 32) >> 4;  // +32 bytes along K inside the swizzle row
-          tc_mma(d, alo + adv, bhi + adv, idesc, (kb | j) != 0, KIND);
-          tc_mma(d, ahi + adv, blo + adv, idesc, 1u, KIND);
-          tc_mma(d, ahi + adv, bhi + adv, idesc, 1u, KIND);
+        for (int q = 0; q < SPS; ++q) {
+          if (q >= n) break;
+          const uint64_t ahi = smem_desc(st + q * 2 * SM::A_BYTES), alo = smem_desc(st + q * 2 * SM::A_BYTES + SM::A_BYTES);
+          const uint64_t bhi = smem_desc(st + SM::B_OFF + q * 2 * SM::B_BYTES);
+          const uint64_t blo = smem_desc(st + SM::B_OFF + q * 2 * SM::B_BYTES + SM::B_BYTES);
+#pragma unroll
+          for (int j = 0; j < KSTEPS; ++j) {
+            const uint64_t adv = (uint64_t)(j * 32) >> 4;  // +32 bytes along K inside the swizzle row
+            tc_mma(d, alo + adv, bhi + adv, idesc, ((kb + q) | j) != 0, KIND);
+            tc_mma(d, ahi + adv, blo + adv, idesc, 1u, KIND);
+            tc_mma(d, ahi + adv, bhi + adv, idesc, 1u, KIND);
+          }
         }
         issued = true;
         tc_commit(&empty[stage]);
@@ -551,7 +572,7 @@ __device__ __forceinline__ uint32_t peer_addr(const void *p, uint32_t rank) {
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
   return r;
 }
-// 2-D TMA load of `rows` rows x 128 bytes at row y of a panel viewed as [rows][128 B]
+// 2-D TMA load of `rows` rows x 64 bytes at row y of a panel viewed as [rows][64 B]
 // (no swizzle: the panel bytes are copied as they are); completes on the leader's
 // barrier `bar_cluster` (cta_group::2)
 __device__ __forceinline__ void tma_rows_pair(void *dst, const CUtensorMap *map, int y, uint32_t bar_cluster) {
@@ -648,7 +669,7 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p, con
   constexpr uint32_t FMT = KIND == TC_TF32 ? 2u : 1u;
   constexpr uint32_t IDESC =
       (1u << 4) | (FMT << 7) | (FMT << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(256 >> 4) << 24);
-  constexpr int KSTEPS = 4;
+  constexpr int KSTEPS = TC_ROW_BYTES / 32;
 
   if (warp == 0 && lane == 0) {
     // ---------------------------------------------------------------- producer (both CTAs)
@@ -669,7 +690,7 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm_pair(TcParams p, con
         uint8_t *st = smem + stage * SM::STAGE_BYTES;
         if (rank == 0) mbar_expect_tx(&full[stage], 2 * SM::STAGE_BYTES);
         const uint32_t fb = peer_addr(&full[stage], 0);
-        // panel rows of 128 bytes: A tile (mt128, kb) hi + lo (256 rows, one box) and this
+        // panel rows of 64 bytes: A tile (mt128, kb) hi + lo (256 rows, one box) and this
         // CTA's half of the B tile (nt, kb): the B panels of the 2-CTA form hold BN/2-row tiles
         // (hi then lo), half 2 nt + rank, so it is one box of BN rows as well
         const int ya = (int)((g.a_off + ((int64_t)mt128 * g.kb + kb) * (2 * SM::A_BYTES)) / TC_ROW_BYTES);
@@ -974,7 +995,7 @@ __global__ void __launch_bounds__(PACK_THREADS) k_pack_items(PackItemParams p) {
 // a CTA loads a 32-row x 32-k (TF32) or 32 x 64 (BF16) tile with coalesced reads along
 // the rows (all of a thread's loads issued together), stages it in shared memory, then
 // each thread writes one 16-byte chunk with the 8 chunks of a panel row on 8 consecutive
-// threads (whole 128-byte rows per 8 threads).
+// threads (a panel row of two 64-byte K slices per 8 threads).
 using PackTileItem = PackTileItemH;  // rows r0..r0+31, local k chunks kc0..kc0+7
 struct PackTileParams {
   const PackSeg *segs;
@@ -1056,28 +1077,28 @@ __global__ void __launch_bounds__(256, 4) k_pack_tile(PackTileParams p) {
 
 
 
-template <int KIND, int BN, int STAGES>
+template <int KIND, int BN, int STAGES, int SPS>
 ctn_status launch_tc(const TcParams &prm, int64_t ntiles, cudaStream_t st) {
-  using SM = TcSmem<KIND, BN, STAGES>;
+  using SM = TcSmem<KIND, BN, STAGES, SPS>;
   const int smem = SM::TOTAL + 1024;
   static bool attr_set[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr_set[dev & 63]) {
-    CTN_CUDA(cudaFuncSetAttribute(k_tc_gemm<KIND, BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CTN_CUDA(cudaFuncSetAttribute(k_tc_gemm<KIND, BN, STAGES, SPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     attr_set[dev & 63] = true;
   }
   const int grid = (int)std::min<int64_t>(ntiles, nsm_count());
-  k_tc_gemm<KIND, BN, STAGES><<<grid, NTHREADS_TC, smem, st>>>(prm);
+  k_tc_gemm<KIND, BN, STAGES, SPS><<<grid, NTHREADS_TC, smem, st>>>(prm);
   CTN_CHECK_LAUNCH();
   return CTN_OK;
 }
 
-// 2-D view [bytes / 128][128] (uint8, no swizzle) of a panel buffer, boxes of `box_rows` rows
+// 2-D view [bytes / 64][64] (uint8, no swizzle) of a panel buffer, boxes of `box_rows` rows
 static ctn_status encode_rows_map(CUtensorMap *m, const void *base, int64_t bytes, int box_rows) {
-  const cuuint64_t dims[2] = {128, (cuuint64_t)(bytes / 128)};
-  const cuuint64_t strides[1] = {128};
-  const cuuint32_t box[2] = {128, (cuuint32_t)box_rows};
+  const cuuint64_t dims[2] = {(cuuint64_t)TC_ROW_BYTES, (cuuint64_t)(bytes / TC_ROW_BYTES)};
+  const cuuint64_t strides[1] = {(cuuint64_t)TC_ROW_BYTES};
+  const cuuint32_t box[2] = {(cuuint32_t)TC_ROW_BYTES, (cuuint32_t)box_rows};
   const cuuint32_t estr[2] = {1, 1};
   const EncodeTiledFn enc = encode_tiled();
   if (!enc) {
@@ -1120,7 +1141,8 @@ ctn_status launch_tc_pair(const TcParams &prm, int64_t ntiles, cudaStream_t st) 
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   CUtensorMap ma, mb;
-  CTN_REQUIRE(prm.a_bytes > 0 && prm.b_bytes > 0 && prm.a_bytes % 128 == 0 && prm.b_bytes % 128 == 0,
+  CTN_REQUIRE(prm.a_bytes > 0 && prm.b_bytes > 0 && prm.a_bytes % TC_ROW_BYTES == 0 &&
+                  prm.b_bytes % TC_ROW_BYTES == 0,
               "tcgen05 2-CTA GEMM: panel sizes unknown");
   CTN_TRY(encode_rows_map(&ma, prm.a, prm.a_bytes, 2 * TC_BM));  // hi + lo of one A tile per box
   CTN_TRY(encode_rows_map(&mb, prm.b, prm.b_bytes, BN));  // hi + lo of one BN/2-row half tile per box
@@ -1128,39 +1150,58 @@ ctn_status launch_tc_pair(const TcParams &prm, int64_t ntiles, cudaStream_t st) 
   return CTN_OK;
 }
 
+// ring depth: the most stages (at most 8) that fit in 227 KiB next to the barriers, the
+// alignment slack and the epilogue buffers (double TMA boxes for the 1-CTA form)
+constexpr int TC_SMEM_MAX = 227 * 1024;
+constexpr int tc_stages_1cta(int bn, int sps) {
+  return (TC_SMEM_MAX - 2048 - 4 * 2 * 4096) / (sps * (2 * TC_A_TILE + 2 * bn * TC_ROW_BYTES)) < 8
+             ? (TC_SMEM_MAX - 2048 - 4 * 2 * 4096) / (sps * (2 * TC_A_TILE + 2 * bn * TC_ROW_BYTES))
+             : 8;
+}
+constexpr int tc_stages_pair(int bn) {
+  return (TC_SMEM_MAX - 2048 - EPI_BYTES) / (2 * TC_A_TILE + bn * TC_ROW_BYTES) < 8
+             ? (TC_SMEM_MAX - 2048 - EPI_BYTES) / (2 * TC_A_TILE + bn * TC_ROW_BYTES)
+             : 8;
+}
+
 template <int KIND>
 ctn_status launch_tc_pair_kind(int bn, const TcParams &prm, cudaStream_t st) {
   switch (bn) {
-    case 128: return launch_tc_pair<KIND, 128, 4>(prm, prm.ntiles, st);
-    case 192: return launch_tc_pair<KIND, 192, 3>(prm, prm.ntiles, st);
-    case 256: return launch_tc_pair<KIND, 256, 3>(prm, prm.ntiles, st);
+    case 128: return launch_tc_pair<KIND, 128, tc_stages_pair(128)>(prm, prm.ntiles, st);
+    case 192: return launch_tc_pair<KIND, 192, tc_stages_pair(192)>(prm, prm.ntiles, st);
+    case 256: return launch_tc_pair<KIND, 256, tc_stages_pair(256)>(prm, prm.ntiles, st);
   }
   set_error("tcgen05 2-CTA GEMM: unsupported tile width %d (128, 192, 256)", bn);
   return CTN_ERR_UNSUPPORTED;
 }
 
 // tile widths compiled (UMMA M=128 allows N = 16..256 in steps of 16); the ring depth is
-// the largest that fits next to 2 x 16 KiB A tiles and 2 x BN x 128 B B tiles per stage
+// the largest that fits next to the epilogue boxes (SPS x (2 x 8 KiB A + 2 x BN x 64 B B) per stage)
+template <int KIND, int BN>
+ctn_status launch_tc_sps(int sps, const TcParams &prm, cudaStream_t st) {
+  if (sps == 2) return launch_tc<KIND, BN, tc_stages_1cta(BN, 2), 2>(prm, prm.ntiles, st);
+  return launch_tc<KIND, BN, tc_stages_1cta(BN, 1), 1>(prm, prm.ntiles, st);
+}
 template <int KIND>
-ctn_status launch_tc_kind(int bn, const TcParams &prm, cudaStream_t st) {
+ctn_status launch_tc_kind(int bn, int sps, const TcParams &prm, cudaStream_t st) {
   switch (bn) {
-    case 32: return launch_tc<KIND, 32, 5>(prm, prm.ntiles, st);
-    case 48: return launch_tc<KIND, 48, 4>(prm, prm.ntiles, st);
-    case 64: return launch_tc<KIND, 64, 4>(prm, prm.ntiles, st);
-    case 96: return launch_tc<KIND, 96, 3>(prm, prm.ntiles, st);
-    case 128: return launch_tc<KIND, 128, 3>(prm, prm.ntiles, st);
-    case 144: return launch_tc<KIND, 144, 3>(prm, prm.ntiles, st);
-    case 160: return launch_tc<KIND, 160, 2>(prm, prm.ntiles, st);
-    case 192: return launch_tc<KIND, 192, 2>(prm, prm.ntiles, st);
-    case 256: return launch_tc<KIND, 256, 2>(prm, prm.ntiles, st);
+    case 32: return launch_tc_sps<KIND, 32>(sps, prm, st);
+    case 48: return launch_tc_sps<KIND, 48>(sps, prm, st);
+    case 64: return launch_tc_sps<KIND, 64>(sps, prm, st);
+    case 96: return launch_tc_sps<KIND, 96>(sps, prm, st);
+    case 128: return launch_tc_sps<KIND, 128>(sps, prm, st);
+    case 144: return launch_tc_sps<KIND, 144>(sps, prm, st);
+    case 160: return launch_tc_sps<KIND, 160>(sps, prm, st);
+    case 192: return launch_tc_sps<KIND, 192>(sps, prm, st);
+    case 256: return launch_tc_sps<KIND, 256>(sps, prm, st);
   }
   set_error("tcgen05 GEMM: unsupported tile width %d (32, 48, 64, 96, 128, 144, 160, 192, 256)", bn);
   return CTN_ERR_UNSUPPORTED;
 }
-ctn_status launch_tc_any(int kind, int bn, bool pair, const TcParams &prm, cudaStream_t st) {
+ctn_status launch_tc_any(int kind, int bn, bool pair, int sps, const TcParams &prm, cudaStream_t st) {
   if (pair)
     return kind == TC_TF32 ? launch_tc_pair_kind<TC_TF32>(bn, prm, st) : launch_tc_pair_kind<TC_BF16>(bn, prm, st);
-  return kind == TC_TF32 ? launch_tc_kind<TC_TF32>(bn, prm, st) : launch_tc_kind<TC_BF16>(bn, prm, st);
+  return kind == TC_TF32 ? launch_tc_kind<TC_TF32>(bn, sps, prm, st) : launch_tc_kind<TC_BF16>(bn, sps, prm, st);
 }
 
 }  // namespace
@@ -1235,7 +1276,14 @@ void TcGemm::finalize() {
   }
   std::stable_sort(tmp.begin(), tmp.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
   tiles.clear();
-  for (auto &x : tmp) tiles.push_back(x.second);
+  double ksum = 0.0;
+  for (auto &x : tmp) {
+    tiles.push_back(x.second);
+    ksum += x.first;
+  }
+  // two K slices per stage when the tiles' K is long (fewer, larger copies per stage), one when
+  // it is short (a deeper ring over the few slices a tile has)
+  sps = (!tiles.empty() && ksum >= TC_SPS2_MEAN_SLICES * (double)tiles.size()) ? 2 : 1;
 }
 
 // Order of the uploaded tile table.  The kernels hand tiles to their W persistent workers
@@ -1358,7 +1406,7 @@ ctn_status TcGemm::run(const uint8_t *a, const uint8_t *b, float *c32, double *c
   prm.c32 = c32;
   prm.c64 = c64;
   prm.err = err;
-  return launch_tc_any(kind, bn, pair, prm, st);
+  return launch_tc_any(kind, bn, pair, sps, prm, st);
 }
 
 ctn_status tc_launch_tables(int kind, int bn, const TcGroup *d_groups, const TcTile *d_tiles, int64_t ntiles,
@@ -1381,7 +1429,7 @@ ctn_status tc_launch_tables(int kind, int bn, const TcGroup *d_groups, const TcT
   prm.c32 = c32;
   prm.c64 = c64;
   prm.err = err;
-  return launch_tc_any(kind, bn, false, prm, st);
+  return launch_tc_any(kind, bn, false, 1, prm, st);
 }
 
 ctn_status pack_launch_tables(int kind, const PackSeg *d_segs, const int64_t *d_begin, int nseg, int64_t nchunks,
@@ -1557,8 +1605,8 @@ extern "C" size_t ctn_split_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K
   const int kind = precision == CTN_PREC_BF16X3 ? ctn::TC_BF16 : ctn::TC_TF32;
   const int ks = ctn::tc_k_per_slice(kind);
   const int64_t kb = (K + ks - 1) / ks;
-  const int64_t a = round_up(M, 128) * kb * 128;
-  const int64_t b = round_up(N, 128) * kb * 128;
+  const int64_t a = round_up(M, 128) * kb * ctn::TC_ROW_BYTES;
+  const int64_t b = round_up(N, 128) * kb * ctn::TC_ROW_BYTES;
   return (size_t)(2 * a + 2 * b + 256 + 64);
 }
 

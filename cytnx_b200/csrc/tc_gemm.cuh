@@ -1,16 +1,18 @@
 // Split-precision grouped GEMM on the 5th-generation tensor cores (tcgen05 + TMEM).
 //
 // Operands are stored "pre-tiled": every group's A (M x K) and B^T (N x K) matrices are
-// cut into tiles of 128 (A) or BN (B) rows by one 128-byte K slice (32 TF32 or 64 BF16
-// values), each tile laid out exactly as the UMMA K-major SWIZZLE_128B canonical layout
-// expects in shared memory (8-row x 128-byte atoms, 16-byte chunk index XOR row % 8).
+// cut into tiles of 128 (A) or BN (B) rows by one 64-byte K slice (16 TF32 or 32 BF16
+// values), each tile laid out exactly as the UMMA K-major SWIZZLE_64B canonical layout
+// expects in shared memory (8-row x 64-byte atoms, 16-byte chunk index XOR (row / 2) % 4).
 // Each operand is split as x = hi + lo (both exactly representable in TF32 or BF16), and a
 // tile is stored as its hi half followed by its lo half: the hi and lo tiles of one K slice
 // move global -> shared with ONE contiguous bulk copy (TMA engine, cp.async.bulk +
-// mbarrier complete_tx), no tensor map needed, for any block shape.  (Bulk copies of 32 KB
-// and more stream from L2 at ~1.4x the rate of 16 KB ones on B200.)  Padding rows/columns
-// are zeros written once.  Every K slice issues three MMAs lo*hi + hi*lo + hi*hi into one
-// FP32 TMEM accumulator.
+// mbarrier complete_tx), no tensor map needed, for any block shape.  64-byte slices keep a
+// pipeline stage small (48 KiB for a 128 x 256 tile), so four to eight stages fit in shared
+// memory: the ring depth sets the operand stream rate of these GEMMs, whose blocks have
+// short K (a few hundred) and whose three products read every stage three times.  Padding
+// rows/columns are zeros written once.  Every 32-byte K step issues three MMAs
+// lo*hi + hi*lo + hi*hi into one FP32 TMEM accumulator.
 #pragma once
 #include <cstdint>
 #include <algorithm>
@@ -21,13 +23,16 @@
 namespace ctn {
 
 constexpr int TC_BM = 128;            // UMMA M (rows of an A tile, TMEM lanes)
-constexpr int TC_ROW_BYTES = 128;     // one swizzle row = one K slice
-constexpr int TC_A_TILE = TC_BM * TC_ROW_BYTES;  // 16 KiB
+constexpr int TC_ROW_BYTES = 64;      // one swizzle row = one K slice
+constexpr int TC_ATOM_BYTES = 8 * TC_ROW_BYTES;  // 8-row swizzle atom (the UMMA stride byte offset)
+constexpr int TC_A_TILE = TC_BM * TC_ROW_BYTES;  // 8 KiB
 constexpr long long TC_SPIN_LIMIT = 1ll << 24;   // try_wait probes of a bounded wait (~seconds)
+// mean K slices per tile from which a plan stages two slices per pipeline stage
+constexpr double TC_SPS2_MEAN_SLICES = 16.0;
 
 enum TcKind { TC_TF32 = 0, TC_BF16 = 1 };
 
-inline int tc_k_per_slice(int kind) { return kind == TC_TF32 ? 32 : 64; }
+inline int tc_k_per_slice(int kind) { return kind == TC_TF32 ? 16 : 32; }
 inline int tc_elem_bytes(int kind) { return kind == TC_TF32 ? 4 : 2; }
 
 // One stacked GEMM: C[M][N] = A[M][K] * B[K][N] over pre-tiled panels.
@@ -64,18 +69,19 @@ struct TcParams {
   int skip_copies;       // error-path self-test: the producer issues no copies (waits run out)
 };
 
+// byte offset of (row rr, byte b) of a tile, K-major SWIZZLE_64B: 8-row x 64-byte atoms, the
+// 16-byte chunk index XORed with address bits 7-8, i.e. (row / 2) % 4
+__host__ __device__ inline int tc_tile_byte(int rr, int byte) {
+  return (rr >> 3) * TC_ATOM_BYTES + (rr & 7) * TC_ROW_BYTES + ((((byte >> 4) ^ (rr >> 1)) & 3) << 4) + (byte & 15);
+}
 // byte offset of the hi element (r, k) inside a panel of tiles with `rows` rows per tile
-// (tile index = (r / rows) * kb + k / kslice), K-major SWIZZLE_128B; every tile is its hi
-// half (rows x 128 bytes) followed by its lo half, so the lo element is rows * 128 bytes
-// further (tc_lo_delta)
+// (tile index = (r / rows) * kb + k / kslice); every tile is its hi half (rows x 64 bytes)
+// followed by its lo half, so the lo element is rows * 64 bytes further (tc_lo_delta)
 __host__ __device__ inline int64_t tc_panel_offset(int64_t r, int64_t k, int rows, int kb, int kind) {
-  const int ks = kind == TC_TF32 ? 32 : 64;
+  const int ks = kind == TC_TF32 ? 16 : 32;
   const int eb = kind == TC_TF32 ? 4 : 2;
   const int64_t tile = (r / rows) * kb + k / ks;
-  const int rr = (int)(r % rows);
-  const int byte = (int)(k % ks) * eb;
-  const int chunk = (byte >> 4) ^ (rr & 7);
-  return tile * 2 * (int64_t)rows * TC_ROW_BYTES + (rr >> 3) * 1024 + (rr & 7) * 128 + chunk * 16 + (byte & 15);
+  return tile * 2 * (int64_t)rows * TC_ROW_BYTES + tc_tile_byte((int)(r % rows), (int)(k % ks) * eb);
 }
 // distance from a hi element to its lo element in a panel with `rows` rows per tile
 __host__ __device__ inline int64_t tc_lo_delta(int rows) { return (int64_t)rows * TC_ROW_BYTES; }
@@ -94,6 +100,7 @@ struct TcGemm {
     bn = w < 0 ? -w : w;
   }
   int width() const { return pair ? -bn : bn; }
+  int sps = 1;  // K slices per pipeline stage of the 1-CTA kernel (chosen in finalize)
   // rows per B panel tile: the 2-CTA form stores each BN-wide tile as two BN/2-row tiles, so
   // that the half a CTA of the pair loads (hi and lo) is one contiguous copy
   int b_tile_rows() const { return pair ? bn / 2 : bn; }

@@ -100,9 +100,9 @@ def test_noalloc_allocates_nothing():
 
 
 def test_noalloc_size_limit_boundary():
-    """3xTF32 panels take 32 KiB per (128-row tile x 32-wide K slice) for A and B alike: at
-    M = N = 512, K = 4064 (127 slices) the problem fits the 32 MiB array with its tables;
-    K = 4096 (128 slices) fills the array with panels alone and is rejected."""
+    """3xTF32 panels take 16 KiB per (128-row tile x 16-wide K slice) for A and B alike: at
+    M = N = 512, K = 4064 (254 slices) the problem fits the 32 MiB array with its tables;
+    K = 4096 (256 slices) fills the array with panels alone and is rejected."""
     from cytnx_b200 import _lib
     from cytnx_b200._lib import CytnxError
 
