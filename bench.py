@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--matvec-only", action="store_true",
                     help="profiling driver: bind the headline form with --tiles, run warmup + steps matvecs, exit")
     ap.add_argument("--tiles", default="", help="step-1,step-4 tile widths for --matvec-only (e.g. 192,128)")
+    ap.add_argument("--epi", default="", help="step-1,step-4 GEMM epilogue forms for --matvec-only / --lanczos-only "
+                                             "(0 direct, 1 staged, 2 TMEM fragments; default automatic)")
     ap.add_argument("--lanczos-only", type=int, default=0,
                     help="profiling driver: N restart cycles of the refined Lanczos (headline form, --tiles, "
                          "Krylov dimension 32), the cycles inside a profiler start/stop range, then exit")
@@ -159,6 +161,15 @@ class ClockSampler:
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def quiet_host():
+    """One BLAS thread for the oracle from here on: the worker threads a multi-threaded CPU
+    baseline leaves behind keep spinning for a while after each call and take host cores from
+    the thread that launches the next GPU measurement (host-latency-bound sections such as the
+    small dense configuration and the per-phase event profiles are sensitive to it)."""
+    if "oracle" in sys.modules:
+        sys.modules["oracle"].set_threads(1)
 
 
 def cpu_baseline_matvec(D, seed, sample_s, threads):
@@ -293,10 +304,18 @@ def main():
     st = torch.cuda.current_stream()
     psi, L, M1, M2, R = W.build_two_site(spec, mpo_vals, seed=0, device=local)
     H = c.TwoSiteHeff(L, M1, M2, R, psi, precision=args.precision)
-    if args.matvec_only:  # small fixed launch sequence for ncu: no autotuning, no other sections
-        if args.tiles and args.precision != "fp64":
+    def fixed_tiles():  # --tiles / --epi of the profiling drivers
+        if args.precision == "fp64":
+            return
+        if args.tiles:
             b1, b4 = (int(t) for t in args.tiles.split(","))
             H.set_tiles(b1, b4, args.precision)
+        if args.epi:
+            e1, e4 = (int(t) for t in args.epi.split(","))
+            _lib.check(_lib.lib().ctn_heff2_set_epilogue(H._h, _lib.PRECISIONS[args.precision], e1, e4), "epi")
+
+    if args.matvec_only:  # small fixed launch sequence for ncu: no autotuning, no other sections
+        fixed_tiles()
         x = psi.flat_view()
         y = torch.empty_like(x)
         for _ in range(args.warmup + args.steps):
@@ -309,9 +328,7 @@ def main():
             dist.destroy_process_group()
         return
     if args.lanczos_only > 0:  # restart cycles of the refined driver inside a profiler range (ncu)
-        if args.tiles and args.precision != "fp64":
-            b1, b4 = (int(t) for t in args.tiles.split(","))
-            H.set_tiles(b1, b4, args.precision)
+        fixed_tiles()
         H.lanczos_refined(psi, precision=args.precision, krylov_dim=32, max_restarts=2, tol=0.0)  # warm
         torch.cuda.synchronize()
         torch.cuda.profiler.start()
@@ -533,11 +550,16 @@ def main():
                  "traffic_unit": "bytes per matvec (steps 1 and 4, ncu capture)",
                  "kernel_flops_per_matvec": g_flops, "kernel_ms_per_matvec": g_ms})
     clocks = sampler.summary()
+    quiet_host()
     permute = run_permute(args, dev, st, pk.get("hbm_gbs"))
+    quiet_host()
     prec_floor = run_precision_floor(dev) if rank == 0 else None
     fp64_d1024 = run_fp64_d1024(args, dev, st, dgemm_tflops, rank)
+    quiet_host()
     config1 = run_config1(args, dev, st, dgemm_tflops) if rank == 0 else None
+    quiet_host()
     batched = run_batched(args, world, rank, dev, st) if args.batch_problems > 0 else None
+    quiet_host()
     mps_ad = run_mps_autograd(args, dev) if args.mps_lbfgs_steps > 0 else None
     if rank == 0:
         ora = None

@@ -509,6 +509,15 @@ extern "C" ctn_status ctn_heff2_lanczos_refined(ctn_heff2_plan *plan, int precis
                               ctn::as_stream(stream), /*w_f32=*/split);
 }
 
+// median of per-repetition phase times: a repetition that the host was slow to launch (the
+// first phase of each repetition holds the launch latency) does not move it
+static double median_of(std::vector<double> v) {
+  if (v.empty()) return 0.0;
+  std::sort(v.begin(), v.end());
+  const size_t n = v.size();
+  return n % 2 ? v[n / 2] : 0.5 * (v[n / 2 - 1] + v[n / 2]);
+}
+
 extern "C" ctn_status ctn_heff2_profile(ctn_heff2_plan *p, const double *psi, double *out, int precision, int reps,
                                         double *ms_out, int *launches_out, void *stream) {
   CTN_REQUIRE(p && reps > 0 && ms_out, "ctn_heff2_profile: bad argument");
@@ -516,10 +525,14 @@ extern "C" ctn_status ctn_heff2_profile(ctn_heff2_plan *p, const double *psi, do
   if (precision == CTN_PREC_3XTF32 || precision == CTN_PREC_BF16X3) {
     const int k = split_kind(precision);
     CTN_REQUIRE(p->split_bound[k], "ctn_heff2_profile: environments not bound for this precision");
-    double acc[4] = {0, 0, 0, 0};
+    std::vector<double> t[4];
     CTN_TRY(ctn::heff_split_matvec(p, k, psi, out, st, nullptr));  // warm
-    for (int r = 0; r < reps; ++r) CTN_TRY(ctn::heff_split_matvec(p, k, psi, out, st, acc));
-    for (int i = 0; i < 4; ++i) ms_out[i] = acc[i] / reps;
+    for (int r = 0; r < reps; ++r) {
+      double one[4] = {0, 0, 0, 0};
+      CTN_TRY(ctn::heff_split_matvec(p, k, psi, out, st, one));
+      for (int i = 0; i < 4; ++i) t[i].push_back(one[i]);
+    }
+    for (int i = 0; i < 4; ++i) ms_out[i] = median_of(t[i]);
     if (launches_out) *launches_out = 4;
     return CTN_OK;
   }
@@ -533,7 +546,7 @@ extern "C" ctn_status ctn_heff2_profile(ctn_heff2_plan *p, const double *psi, do
   CTN_TRY(p->g4.upload(st));
   cudaEvent_t ev[4];
   for (auto &e : ev) CTN_CUDA(cudaEventCreate(&e));
-  double acc[3] = {0, 0, 0};
+  std::vector<double> acc[3];
   for (int r = 0; r < reps; ++r) {
     CTN_CUDA(cudaEventRecord(ev[0], st));
     CTN_TRY(p->g1.run(Lt, psi, X1, st));
@@ -546,12 +559,12 @@ extern "C" ctn_status ctn_heff2_profile(ctn_heff2_plan *p, const double *psi, do
     for (int k = 0; k < 3; ++k) {
       float ms = 0.f;
       CTN_CUDA(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
-      acc[k] += ms;
+      acc[k].push_back(ms);
     }
   }
   for (auto &e : ev) cudaEventDestroy(e);
   ms_out[0] = 0.0;
-  for (int k = 0; k < 3; ++k) ms_out[k + 1] = acc[k] / reps;
+  for (int k = 0; k < 3; ++k) ms_out[k + 1] = median_of(acc[k]);
   if (launches_out) *launches_out = 3;
   return CTN_OK;
 }

@@ -245,7 +245,7 @@ ctn_status ctn_heff2_set_env(ctn_heff2_plan *plan, const double *L, const double
 ctn_status ctn_heff2_matvec(ctn_heff2_plan *plan, const double *psi, double *out, int precision,
                             void *stream);
 /* measurement aid: run `reps` matvecs with CUDA events between the phases on
- * `stream`; ms_out[0..3] receive the mean device time of operand packing (split
+ * `stream`; ms_out[0..3] receive the median over the repetitions of the device time of operand packing (split
  * forms only, 0 for FP64), step 1 (grouped GEMM), steps 2+3 (MPO combination) and
  * step 4 (grouped GEMM); launches_out the number of kernel launches one matvec issues. */
 ctn_status ctn_heff2_profile(ctn_heff2_plan *plan, const double *psi, double *out, int precision, int reps,
