@@ -269,9 +269,6 @@ ctn_status heff_split_prepare(ctn_heff2_plan *p, int kind) {
   s->g1.set_width(p->split_bn[kind][0]);
   s->g4.set_width(p->split_bn[kind][1]);
   s->pk_L.kind = s->pk_P.kind = s->pk_R.kind = kind;
-  // psi rows are its contiguous axis: the step-1 B operand (psi^T) is packed N-major, without
-  // a transpose, wherever the tile width allows
-  s->g1.b_mn = s->pk_P.mn = tc_b_mn_ok(kind, s->g1.width());
   const int bn = s->g1.bn;
   // ---------------- step 1 groups: one per left sector a
   std::map<int64_t, std::vector<int64_t>> Lg, Pg;
@@ -290,9 +287,9 @@ ctn_status heff_split_prepare(ctn_heff2_plan *p, int kind) {
       l_row[l] = M;
       M += p->Lb[l].d[0] * p->Lb[l].d[2];
     }
-    for (int64_t q : jt->second) {  // each psi block's X1 columns (B rows) start at a multiple of 8:
-      p_col[q] = N;                  // 32-byte FP32 rows, whole 16-byte chunks of the N-major B panel
-      N = up(N + p->Pb[q].d[1] * p->Pb[q].d[2] * p->Pb[q].d[3], 8);
+    for (int64_t q : jt->second) {  // each psi block's X1 columns start on a 16-byte boundary
+      p_col[q] = N;
+      N = up(N + p->Pb[q].d[1] * p->Pb[q].d[2] * p->Pb[q].d[3], 4);
     }
     if (M == 0 || N == 0 || K == 0) continue;
     const int64_t ldc = up(N, 4);  // FP32 rows start on 16-byte boundaries (TMA bulk stores)
@@ -559,7 +556,6 @@ HeffSplit *split_batch(std::vector<ctn_heff2_plan *> &plans, const int64_t *psi_
   B->g1.kind = B->g4.kind = kind;
   B->g1.set_width(bn1);
   B->g4.set_width(bn4);
-  B->g1.b_mn = B->pk_P.mn = tc_b_mn_ok(kind, B->g1.width());
   B->g1.balance = B->g4.balance = false;
   B->pk_L.kind = B->pk_P.kind = B->pk_R.kind = kind;
   B->in_f32 = fp32_io;

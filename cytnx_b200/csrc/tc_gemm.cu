@@ -87,14 +87,6 @@ __device__ __forceinline__ uint64_t smem_desc(const void *p) {
          (4ull << 61);
 }
 
-// descriptor of an N-major (MN-major) SWIZZLE_64B B tile (tc_panel_offset_mn): leading byte
-// offset = the stride between 64-byte N groups, stride byte offset = one 8-K-row atom
-__device__ __forceinline__ uint64_t smem_desc_mn(const void *p, int kind) {
-  const uint64_t a = smem_u32(p);
-  return ((a & 0x3FFFFull) >> 4) | ((uint64_t)(tc_mn_group_bytes(kind) >> 4) << 16) |
-         ((uint64_t)(TC_ATOM_BYTES >> 4) << 32) | (1ull << 46) | (4ull << 61);
-}
-
 __device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                        uint32_t accum, int kind) {
   if (kind == TC_TF32) {
@@ -327,10 +319,7 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
     for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
       const TcTile tl = p.tiles[t];
       const TcGroup g = p.groups[tl.group];
-      // the tile's B rows only (N-major: whole 64-byte N groups, each its K slice's atoms)
-      constexpr int MN_NA = TC_ROW_BYTES / (KIND == TC_TF32 ? 4 : 2);
-      const uint32_t b_bytes = p.b_mn ? (uint32_t)((tile_n(g, tl) + MN_NA - 1) / MN_NA) * tc_mn_group_bytes(KIND)
-                                      : (uint32_t)tile_n(g, tl) * TC_ROW_BYTES;
+      const uint32_t b_bytes = (uint32_t)tile_n(g, tl) * TC_ROW_BYTES;  // the tile's B rows only
       for (int kb = 0; kb < g.kb; kb += SPS) {
         const int n = min(SPS, g.kb - kb);  // K slices in this stage
         if (!mbar_wait(&empty[stage], phase ^ 1, p.err, 1, p.spin_limit)) {
@@ -382,7 +371,7 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
     for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
       const TcTile tl = p.tiles[t];
       const TcGroup g = p.groups[tl.group];
-      const uint32_t idesc = IDESC0 | ((uint32_t)(tile_n(g, tl) >> 3) << 17) | ((uint32_t)(p.b_mn != 0) << 16);
+      const uint32_t idesc = IDESC0 | ((uint32_t)(tile_n(g, tl) >> 3) << 17);
       if (!mbar_wait(&tempty[acc], acc_phase ^ 1, p.err, 2, p.spin_limit)) break;
       tc_fence_after();
       const uint32_t d = tmem_base + (uint32_t)(acc * BN);
@@ -398,19 +387,14 @@ __global__ void __launch_bounds__(NTHREADS_TC, 1) k_tc_gemm(TcParams p) {
         for (int q = 0; q < SPS; ++q) {
           if (q >= n) break;
           const uint64_t ahi = smem_desc(st + q * 2 * SM::A_BYTES), alo = smem_desc(st + q * 2 * SM::A_BYTES + SM::A_BYTES);
-          uint8_t *sb = st + SM::B_OFF + q * 2 * SM::B_BYTES;
-          const uint64_t bhi = p.b_mn ? smem_desc_mn(sb, KIND) : smem_desc(sb);
-          const uint64_t blo = p.b_mn ? smem_desc_mn(sb + SM::B_BYTES, KIND) : smem_desc(sb + SM::B_BYTES);
-          // one MMA's K (32 bytes) is 32 bytes along a K-major row, or 32 / elem K rows = that
-          // many 64-byte rows of N-major atoms
-          const uint64_t badv = p.b_mn ? (uint64_t)((32 / (KIND == TC_TF32 ? 4 : 2)) * TC_ROW_BYTES) >> 4 : 2;
+          const uint64_t bhi = smem_desc(st + SM::B_OFF + q * 2 * SM::B_BYTES);
+          const uint64_t blo = smem_desc(st + SM::B_OFF + q * 2 * SM::B_BYTES + SM::B_BYTES);
 #pragma unroll
           for (int j = 0; j < KSTEPS; ++j) {
             const uint64_t adv = (uint64_t)(j * 32) >> 4;  // +32 bytes along K inside the swizzle row
-            const uint64_t bj = badv * (uint64_t)j;
-            tc_mma(d, alo + adv, bhi + bj, idesc, ((kb + q) | j) != 0, KIND);
-            tc_mma(d, ahi + adv, blo + bj, idesc, 1u, KIND);
-            tc_mma(d, ahi + adv, bhi + bj, idesc, 1u, KIND);
+            tc_mma(d, alo + adv, bhi + adv, idesc, ((kb + q) | j) != 0, KIND);
+            tc_mma(d, ahi + adv, blo + adv, idesc, 1u, KIND);
+            tc_mma(d, ahi + adv, bhi + adv, idesc, 1u, KIND);
           }
         }
         issued = true;
@@ -1007,55 +991,6 @@ __global__ void __launch_bounds__(PACK_THREADS) k_pack_items(PackItemParams p) {
   }
 }
 
-// N-major pack (Packer::mn): chunk g of a segment is (row chunk g % nrc, k = g / nrc), i.e.
-// E consecutive rows at one k, read from E consecutive source rows (contiguous when sr == 1,
-// so a warp reads 32 x E consecutive elements) and stored as one 16-byte hi and one lo chunk
-// of the N-major panel.  Segment row offsets (row0) are multiples of E.
-template <int KIND, bool F32>
-__global__ void __launch_bounds__(PACK_THREADS) k_pack_mn(PackItemParams p) {
-  constexpr int E = KIND == TC_TF32 ? 4 : 8;
-  for (int64_t it = blockIdx.x; it < p.nitems; it += gridDim.x) {
-    const PackItem wi = p.items[it];
-#pragma unroll
-    for (int j = 0; j < PACK_UNROLL; ++j) {
-      const int64_t g = wi.chunk0 + threadIdx.x + j * PACK_THREADS;
-      if (g >= p.nchunks) break;
-      int lo_s = wi.seg0, hi_s = wi.seg1;  // last segment with begin <= g
-      while (lo_s < hi_s) {
-        const int mid = (lo_s + hi_s + 1) >> 1;
-        if (__ldg(p.begin + mid) <= g) lo_s = mid;
-        else hi_s = mid - 1;
-      }
-      const PackSeg s = p.segs[lo_s];
-      const int64_t cl = g - __ldg(p.begin + lo_s);
-      const int nrc = (s.rows + E - 1) / E;
-      const int k = (int)(cl / nrc);
-      const int r = (int)(cl - (int64_t)k * nrc) * E;
-      double x[8];
-      const int64_t i0 = s.src_off + (int64_t)r * s.sr + (int64_t)k * s.sk;
-      if (!F32 && s.sr == 1 && r + E <= s.rows && (i0 & 1) == 0) {  // whole chunk, 16-byte loads
-        const double2 *q = reinterpret_cast<const double2 *>((const double *)p.src + i0);
-#pragma unroll
-        for (int e = 0; e < E / 2; ++e) {
-          const double2 v = __ldg(q + e);
-          x[2 * e] = v.x;
-          x[2 * e + 1] = v.y;
-        }
-#pragma unroll
-        for (int e = E; e < 8; ++e) x[e] = 0.0;
-      } else {
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          x[e] = 0.0;
-          if (e < E && r + e < s.rows) x[e] = load_src<F32>(p.src, i0 + (int64_t)e * s.sr);
-        }
-      }
-      const int64_t off = s.panel_off + tc_panel_offset_mn(s.row0 + r, s.k0 + k, s.tile_rows, s.kb, KIND);
-      store_split<KIND>(x, p.hi, p.lo, off);
-    }
-  }
-}
-
 // Transposing pack for segments whose rows are the contiguous source axis (sr == 1):
 // a CTA loads a 32-row x 32-k (TF32) or 32 x 64 (BF16) tile with coalesced reads along
 // the rows (all of a thread's loads issued together), stages it in shared memory, then
@@ -1468,7 +1403,6 @@ ctn_status TcGemm::run(const uint8_t *a, const uint8_t *b, float *c32, double *c
   prm.b = b;
   prm.spin_limit = spin_limit;
   prm.skip_copies = skip_copies;
-  prm.b_mn = (b_mn && !pair) ? 1 : 0;  // the 2-CTA form reads K-major B only
   prm.c32 = c32;
   prm.c64 = c64;
   prm.err = err;
@@ -1492,7 +1426,6 @@ ctn_status tc_launch_tables(int kind, int bn, const TcGroup *d_groups, const TcT
   prm.b = b;
   prm.spin_limit = TC_SPIN_LIMIT;
   prm.skip_copies = 0;
-  prm.b_mn = 0;
   prm.c32 = c32;
   prm.c64 = c64;
   prm.err = err;
@@ -1528,18 +1461,12 @@ void Packer::finalize() {
   seg_chunk_begin.assign(segs.size() + 1, 0);
   const int E = kind == TC_TF32 ? 4 : 8;
   for (size_t i = 0; i < segs.size(); ++i) {
-    // K-major: chunks of E k values per row; N-major: chunks of E rows per k
-    const int64_t c = mn ? (int64_t)((segs[i].rows + E - 1) / E) * segs[i].cols
-                         : (int64_t)((segs[i].cols + E - 1) / E) * segs[i].rows;
-    seg_chunk_begin[i + 1] = seg_chunk_begin[i] + c;
+    const int64_t kc = (segs[i].cols + E - 1) / E;
+    seg_chunk_begin[i + 1] = seg_chunk_begin[i] + kc * segs[i].rows;
   }
   nchunks = seg_chunk_begin.back();
   chunk_items(seg_chunk_begin, PACK_ITEM, items);
   tile_items.clear();
-  if (mn) {  // no transpose needed: the flat chunk items
-    transposing = false;
-    return;
-  }
   bool all_rows = !segs.empty();
   for (const auto &sg : segs) all_rows &= (sg.sr == 1);
   if (all_rows) {
@@ -1645,15 +1572,7 @@ ctn_status Packer::run(const void *src, int src_is_f32, uint8_t *panel, cudaStre
     const int64_t grid = std::min<int64_t>(prm.nitems, (int64_t)nsm_count() * resident_ctas(kern, PACK_THREADS) * 4);
     kern<<<(unsigned)grid, PACK_THREADS, 0, st>>>(prm);
   };
-  if (mn) {
-    if (kind == TC_TF32) {
-      if (src_is_f32) launch(k_pack_mn<TC_TF32, true>);
-      else launch(k_pack_mn<TC_TF32, false>);
-    } else {
-      if (src_is_f32) launch(k_pack_mn<TC_BF16, true>);
-      else launch(k_pack_mn<TC_BF16, false>);
-    }
-  } else if (kind == TC_TF32) {
+  if (kind == TC_TF32) {
     if (src_is_f32) launch(k_pack_items<TC_TF32, true>);
     else launch(k_pack_items<TC_TF32, false>);
   } else {

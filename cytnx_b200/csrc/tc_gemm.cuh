@@ -67,7 +67,6 @@ struct TcParams {
   const void *cmaps;
   long long spin_limit;  // try_wait probes of every bounded wait before it gives up
   int skip_copies;       // error-path self-test: the producer issues no copies (waits run out)
-  int b_mn;              // 1: B panels are N-major (tc_panel_offset_mn), 0: K-major
 };
 
 // byte offset of (row rr, byte b) of a tile, K-major SWIZZLE_64B: 8-row x 64-byte atoms, the
@@ -84,25 +83,6 @@ __host__ __device__ inline int64_t tc_panel_offset(int64_t r, int64_t k, int row
   const int64_t tile = (r / rows) * kb + k / ks;
   return tile * 2 * (int64_t)rows * TC_ROW_BYTES + tc_tile_byte((int)(r % rows), (int)(k % ks) * eb);
 }
-// N-major (MN-major) panel tiles of B, used where the operand's rows (N) are its contiguous
-// axis so that packing needs no transpose: a tile of `rows` N values x one K slice is made of
-// 8 K-row x 64-byte atoms (64 bytes = 32 BF16 / 16 TF32 consecutive N values, the same
-// SWIZZLE_64B chunk pattern with the K row in place of the row), the K slice's atoms of one N
-// group back to back (tc_mn_group_bytes apart from the next N group), hi half then lo half
-__host__ __device__ inline int tc_mn_group_bytes(int kind) { return (kind == TC_TF32 ? 2 : 4) * TC_ATOM_BYTES; }
-__host__ __device__ inline int64_t tc_panel_offset_mn(int64_t n, int64_t k, int rows, int kb, int kind) {
-  const int ks = kind == TC_TF32 ? 16 : 32;
-  const int eb = kind == TC_TF32 ? 4 : 2;
-  const int na = TC_ROW_BYTES / eb;  // N values per atom row
-  const int64_t tile = (n / rows) * kb + k / ks;
-  const int nn = (int)(n % rows), kk = (int)(k % ks);
-  return tile * 2 * (int64_t)rows * TC_ROW_BYTES + (int64_t)(nn / na) * tc_mn_group_bytes(kind) +
-         (kk >> 3) * TC_ATOM_BYTES + tc_tile_byte(kk & 7, (nn % na) * eb);
-}
-// the N-major B form is used for BF16 (kind::f16) operands, with whole atom groups per tile
-// width (a multiple of 32 columns) and the 1-CTA kernel; with kind::tf32 operands an N-major
-// B tile in this layout gave zero products on B200, so TF32 keeps K-major B panels
-inline bool tc_b_mn_ok(int kind, int width) { return kind == TC_BF16 && width > 0 && width % 32 == 0; }
 // distance from a hi element to its lo element in a panel with `rows` rows per tile
 __host__ __device__ inline int64_t tc_lo_delta(int rows) { return (int64_t)rows * TC_ROW_BYTES; }
 
@@ -121,7 +101,6 @@ struct TcGemm {
   }
   int width() const { return pair ? -bn : bn; }
   int sps = 1;  // K slices per pipeline stage of the 1-CTA kernel (chosen in finalize)
-  bool b_mn = false;  // B panels N-major (tc_panel_offset_mn; 1-CTA widths with tc_b_mn_ok)
   // rows per B panel tile: the 2-CTA form stores each BN-wide tile as two BN/2-row tiles, so
   // that the half a CTA of the pair loads (hi and lo) is one contiguous copy
   int b_tile_rows() const { return pair ? bn / 2 : bn; }
@@ -186,9 +165,6 @@ struct PackTileItemH {
 
 struct Packer {
   int kind = TC_TF32;
-  // N-major panel (tc_panel_offset_mn): each 16-byte chunk holds consecutive rows at one k,
-  // read from consecutive source rows (no transpose when the rows are the contiguous axis)
-  bool mn = false;
   std::vector<struct PackTileItemH> tile_items;  // transposing work items (all segments row-contiguous)
   bool transposing = false;
   std::vector<PackSeg> segs;
