@@ -876,6 +876,25 @@ def run_fp64_d1024(args, dev, st, dgemm_tflops, rank):
     e1.record(st)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / reps
+    # the same matvecs replayed from a CUDA graph (the three kernels of a D=1024 matvec are short
+    # enough that host-issued back-to-back calls can be limited by the host's launch rate)
+    ms_graph = None
+    try:
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, capture_error_mode="thread_local"):
+            for _ in range(20):
+                H.apply_flat(x, y, "fp64")
+        g.replay()
+        torch.cuda.synchronize()
+        e0.record(st)
+        for _ in range(reps // 20):
+            g.replay()
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms_graph = e0.elapsed_time(e1) / (reps // 20 * 20)
+        del g
+    except Exception as ex:  # report the host-issued figure alone
+        print(f"[bench] fp64_D1024 graph replay unavailable: {ex}", file=sys.stderr)
     ph = (ctypes.c_double * 4)()
     nl = ctypes.c_int()
     _lib.check(_lib.lib().ctn_heff2_profile(H._h, x.data_ptr(), y.data_ptr(), 0, 20, ph, ctypes.byref(nl),
@@ -898,7 +917,10 @@ def run_fp64_d1024(args, dev, st, dgemm_tflops, rank):
     s = S.flat_view()
     kept = int(S.shape()[0])
     out = {"workload": "u1_xxz_two_site_heff_D1024_fp64", "algorithmic_flops_per_matvec": flops,
-           "matvec_ms": ms, "matvec_tflops": flops / (ms * 1e-3) / 1e12, "phase_ms": [ph[i] for i in range(4)],
+           "matvec_ms": ms, "matvec_tflops": flops / (ms * 1e-3) / 1e12,
+           "matvec_ms_graph": ms_graph,
+           "matvec_tflops_graph": flops / (ms_graph * 1e-3) / 1e12 if ms_graph else None,
+           "phase_ms": [ph[i] for i in range(4)],
            "lanczos_iters": it, "lanczos_s_per_step": t_lan / max(it, 1), "energy_40": E,
            "svd_truncate_s": t_svd, "svd_kept": kept, "svd_norm2_kept": float((s * s).sum().item()),
            "roofline": {"bound": "fp64 tensor (DMMA)", "kernel": "k_gemm_grouped_f64 (steps 1 and 4)",
