@@ -77,6 +77,7 @@ _SIGS = {
     "ctn_split_gemm_f64": (c_int, [c_i64, c_i64, c_i64, c_vp, c_vp, c_vp, c_int, c_vp, c_vp]),
     "ctn_split_gemm_f64_noalloc": (c_int, [c_i64, c_i64, c_i64, c_vp, c_vp, c_vp, c_int, c_vp]),
     "ctn_selftest_wait_timeout": (c_int, [c_int, ctypes.c_longlong, c_vp]),
+    "ctn_selftest_barrier_timeout": (c_int, [ctypes.c_longlong, c_vp]),
     "ctn_dot_f64": (c_int, [c_vp, c_vp, c_i64, c_vp, c_vp]),
     "ctn_nrm2_f64": (c_int, [c_vp, c_i64, c_vp, c_vp]),
     "ctn_axpy_f64": (c_int, [c_vp, c_vp, c_i64, c_vp, c_dbl, c_vp]),

@@ -334,6 +334,163 @@ __global__ void __launch_bounds__(RT) k_lanczos_step(const WT *__restrict__ w, c
   finish(acc, partials, ticket, nrm, 1);
 }
 
+// The two kernels above in one cooperative launch: pass 1 (alpha and gamma as in k_dot2s,
+// the partials summed by every CTA in the order k_dot2s's last CTA uses), a grid-wide barrier, pass 2 (the update and the norm as in k_lanczos_step)
+// over the same elements, whose w, u and q are then read again from L2.  One launch and one
+// ramp instead of two.  The barrier is a counter and a generation word in the two-sum
+// workspace; every wait on it is bounded (about a second), after which the CTA raises *err,
+// writes NaN to alpha and leaves.  A cooperative launch makes all CTAs resident at once, so
+// the barrier completes unless the launch itself went wrong.
+constexpr long long BARRIER_SPINS = 1ll << 24;  // x ~64 ns of sleep: about a second
+
+// `extra` > 0 (the self-test only) waits for arrivals that never come
+__device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned *gen, unsigned extra, long long spins) {
+  __shared__ int passed;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned g0 = *(volatile unsigned *)gen;
+    __threadfence();
+    const unsigned a = atomicAdd(count, 1u);
+    if (a == gridDim.x - 1 + extra) {
+      *(volatile unsigned *)count = 0u;  // re-arm for the next launch
+      __threadfence();
+      atomicAdd(gen, 1u);
+      passed = 1;
+    } else {
+      passed = 0;
+      for (long long it = 0; it < spins; ++it) {
+        if (*(volatile unsigned *)gen != g0) {
+          passed = 1;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return passed != 0;
+}
+
+template <bool VEC, typename WT>
+__global__ void __launch_bounds__(RT, 4) k_krylov_step(const WT *__restrict__ w, const double *__restrict__ u,
+                                                   const double *__restrict__ up, const double *__restrict__ q,
+                                                   double *__restrict__ dst, int64_t n, const double *s_ptr,
+                                                   const double *sp_ptr, double *out_alpha, double *out_gamma,
+                                                   double *nrm, double *ws, double *ws2, unsigned *err,
+                                                   unsigned extra, long long spins) {
+  const int64_t tid = (int64_t)blockIdx.x * RT + threadIdx.x;
+  const int64_t step = (int64_t)gridDim.x * RT;
+  // ---- pass 1: <w, u> and <w, q>
+  double sa = 0.0, sb = 0.0;
+  if (VEC) {
+    const int64_t n2 = n / 2;
+    const double2 *a2 = reinterpret_cast<const double2 *>(u), *b2 = reinterpret_cast<const double2 *>(q);
+    for (int64_t i = tid; i < n2; i += 2 * step) {
+      const bool two = i + step < n2;
+      const double2 x0 = ld_pair(w, i), y0 = a2[i], z0 = b2[i];
+      double2 x1 = make_double2(0.0, 0.0), y1 = x1, z1 = x1;
+      if (two) {
+        x1 = ld_pair(w, i + step);
+        y1 = a2[i + step];
+        z1 = b2[i + step];
+      }
+      sa = fma(x0.x, y0.x, sa);
+      sa = fma(x0.y, y0.y, sa);
+      sb = fma(x0.x, z0.x, sb);
+      sb = fma(x0.y, z0.y, sb);
+      sa = fma(x1.x, y1.x, sa);
+      sa = fma(x1.y, y1.y, sa);
+      sb = fma(x1.x, z1.x, sb);
+      sb = fma(x1.y, z1.y, sb);
+    }
+    if (tid == 0 && (n & 1)) {
+      sa = fma((double)w[n - 1], u[n - 1], sa);
+      sb = fma((double)w[n - 1], q[n - 1], sb);
+    }
+  } else {
+    for (int64_t i = tid; i < n; i += step) {
+      const double x = (double)w[i];
+      sa = fma(x, u[i], sa);
+      sb = fma(x, q[i], sb);
+    }
+  }
+  sa = block_sum(sa);
+  sb = block_sum(sb);
+  if (threadIdx.x == 0) {
+    ws2[2 * blockIdx.x] = sa;
+    ws2[2 * blockIdx.x + 1] = sb;
+  }
+  unsigned *bar = reinterpret_cast<unsigned *>(ws2 + 2 * MAXCTA + 2);  // [count, generation]
+  if (!grid_barrier(bar, bar + 1, extra, spins)) {
+    if (threadIdx.x == 0) {
+      atomicExch(err, 1u);
+      *out_alpha = __longlong_as_double(0x7ff8000000000000ll);
+    }
+    return;
+  }
+  // ---- every CTA: alpha, gamma from all partials (k_dot2s's order)
+  double va = 0.0, vb = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += RT) {
+    va += ((volatile double *)ws2)[2 * i];
+    vb += ((volatile double *)ws2)[2 * i + 1];
+  }
+  va = block_sum(va);
+  vb = block_sum(vb);
+  __shared__ double coef[2];
+  const double s = *s_ptr;
+  const double inv = safe_inv(s);
+  if (threadIdx.x == 0) {
+    coef[0] = va * inv * inv;  // alpha
+    coef[1] = vb * inv;        // gamma
+    if (blockIdx.x == 0) {
+      *out_alpha = coef[0];
+      *out_gamma = coef[1];
+    }
+  }
+  __syncthreads();
+  // ---- pass 2: the update of k_lanczos_step
+  const double ca = coef[0] * inv;
+  const double cp = up ? s * safe_inv(*sp_ptr) : 0.0;
+  const double cg = coef[1];
+  double acc = 0.0;
+  auto one = [&](double wv, double uv, double pv, double qv) -> double {
+    double v = fma(-ca, uv, wv * inv);
+    v = fma(-cp, pv, v);
+    v = fma(-cg, qv, v);
+    acc = fma(v, v, acc);
+    return v;
+  };
+  if (VEC) {
+    const int64_t n2 = n / 2;
+    const double2 *u2 = reinterpret_cast<const double2 *>(u), *p2 = reinterpret_cast<const double2 *>(up),
+                  *q2 = reinterpret_cast<const double2 *>(q);
+    double2 *d2 = reinterpret_cast<double2 *>(dst);
+    const double2 z = make_double2(0.0, 0.0);
+    for (int64_t i = tid; i < n2; i += 2 * step) {
+      const bool two = i + step < n2;
+      const double2 w0 = ld_pair(w, i), u0 = u2[i], p0 = up ? p2[i] : z, q0 = q2[i];
+      double2 w1 = z, u1 = z, p1 = z, q1 = z;
+      if (two) {
+        w1 = ld_pair(w, i + step);
+        u1 = u2[i + step];
+        if (up) p1 = p2[i + step];
+        q1 = q2[i + step];
+      }
+      d2[i] = make_double2(one(w0.x, u0.x, p0.x, q0.x), one(w0.y, u0.y, p0.y, q0.y));
+      if (two) d2[i + step] = make_double2(one(w1.x, u1.x, p1.x, q1.x), one(w1.y, u1.y, p1.y, q1.y));
+    }
+    if (tid == 0 && (n & 1)) {
+      const int64_t k = n - 1;
+      dst[k] = one((double)w[k], u[k], up ? up[k] : 0.0, q[k]);
+    }
+  } else {
+    for (int64_t i = tid; i < n; i += step) dst[i] = one((double)w[i], u[i], up ? up[i] : 0.0, q[i]);
+  }
+  acc = block_sum(acc);
+  finish(acc, ws, reinterpret_cast<unsigned *>(ws + MAXCTA), nrm, 1);
+}
+
 // out = sum_j c[j] * K[j]  (Krylov combination), c on device
 // (16-byte loads of four Krylov vectors at a time when every row is 16-byte aligned)
 template <bool VEC>
@@ -457,7 +614,7 @@ int grid_for(int64_t n) {
 size_t reduce_ws_bytes() { return (MAXCTA + 8) * sizeof(double); }
 size_t reduce2_ws_bytes() { return (2 * MAXCTA + 8) * sizeof(double); }
 
-// ws2 layout (dot2s_f64): [2 * MAXCTA partials][ticket]
+// ws2 layout (dot2s_f64, krylov_step_f64): [2 * MAXCTA partials][ticket][spare][barrier count][barrier generation]
 // ws layout: [partials MAXCTA doubles][ticket (8 bytes)]
 ctn_status dot_f64(const float *x, const double *y, int64_t n, double *out, double *ws, cudaStream_t st) {
   int g = grid_for(n);
@@ -550,6 +707,43 @@ ctn_status lanczos_step_f64(const float *w, const double *u, const double *up, c
   return lanczos_step_any(w, u, up, q, dst, n, alpha, gamma, s, sp, nrm, ws, st);
 }
 
+// the fused step: one cooperative launch of k_krylov_step with k_dot2s's grid (capped at the
+// CTAs that fit on the device at once); CTN_ERR_UNSUPPORTED when the device has no
+// cooperative launch (the caller then runs the two kernels)
+template <typename WT>
+static ctn_status krylov_step_any(const WT *w, const double *u, const double *up, const double *q, double *dst,
+                                  int64_t n, const double *s, const double *sp, double *out_alpha,
+                                  double *out_gamma, double *nrm, double *ws, double *ws2, unsigned *err,
+                                  cudaStream_t st, unsigned extra = 0, long long spins = BARRIER_SPINS) {
+  const bool vec = aligned16(w) && aligned16(u) && aligned16(dst) && (!up || aligned16(up)) && aligned16(q);
+  void (*kern)(const WT *, const double *, const double *, const double *, double *, int64_t, const double *,
+               const double *, double *, double *, double *, double *, double *, unsigned *, unsigned, long long) =
+      vec ? k_krylov_step<true, WT> : k_krylov_step<false, WT>;
+  int dev = 0, coop = 0, nsm = 0, occ = 0;
+  CTN_CUDA(cudaGetDevice(&dev));
+  CTN_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  if (!coop) return CTN_ERR_UNSUPPORTED;
+  CTN_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  CTN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, RT, 0));
+  const int g = std::min(grid_stream(n), std::max(1, nsm * occ));
+  void *args[] = {(void *)&w,   (void *)&u,         (void *)&up,        (void *)&q,   (void *)&dst,
+                  (void *)&n,   (void *)&s,         (void *)&sp,        (void *)&out_alpha,
+                  (void *)&out_gamma, (void *)&nrm, (void *)&ws,        (void *)&ws2, (void *)&err,
+                  (void *)&extra, (void *)&spins};
+  CTN_CUDA(cudaLaunchCooperativeKernel((const void *)kern, dim3(g), dim3(RT), args, 0, st));
+  return CTN_OK;
+}
+ctn_status krylov_step_f64(const double *w, const double *u, const double *up, const double *q, double *dst,
+                           int64_t n, const double *s, const double *sp, double *out_alpha, double *out_gamma,
+                           double *nrm, double *ws, double *ws2, unsigned *err, cudaStream_t st) {
+  return krylov_step_any(w, u, up, q, dst, n, s, sp, out_alpha, out_gamma, nrm, ws, ws2, err, st);
+}
+ctn_status krylov_step_f64(const float *w, const double *u, const double *up, const double *q, double *dst,
+                           int64_t n, const double *s, const double *sp, double *out_alpha, double *out_gamma,
+                           double *nrm, double *ws, double *ws2, unsigned *err, cudaStream_t st) {
+  return krylov_step_any(w, u, up, q, dst, n, s, sp, out_alpha, out_gamma, nrm, ws, ws2, err, st);
+}
+
 ctn_status div_copy_f64(const double *x, double *y, int64_t n, const double *a, cudaStream_t st) {
   k_div_copy<<<grid_for(n), RT, 0, st>>>(x, y, n, a);
   CTN_CHECK_LAUNCH();
@@ -587,3 +781,43 @@ ctn_status basis_combine_f64(const double *V, int64_t n, int m, const double *Y,
 }
 
 }  // namespace ctn
+
+// Self-test of the fused Krylov step's bounded grid barrier: one launch on a small vector whose
+// barrier waits for one arrival more than the grid has, so every CTA's wait runs out after
+// `spin_limit` probes, raises the error word and leaves.
+namespace ctn {
+ctn_status selftest_barrier_timeout(long long spin_limit, cudaStream_t st) {
+  const int64_t n = 1 << 14;
+  const size_t wsb = reduce_ws_bytes(), ws2b = reduce2_ws_bytes();
+  const size_t bytes = 4 * n * sizeof(double) + wsb + ws2b + 8 * sizeof(double);
+  double *buf = nullptr;
+  CTN_CUDA(cudaMalloc(&buf, bytes));
+  ctn_status rc = cudaMemsetAsync(buf, 0, bytes, st) == cudaSuccess ? CTN_OK : CTN_ERR_CUDA;
+  double *w = buf, *u = buf + n, *q = buf + 2 * n, *dst = buf + 3 * n;
+  double *ws = buf + 4 * n, *ws2 = ws + wsb / sizeof(double), *scal = ws2 + ws2b / sizeof(double);
+  unsigned *err = reinterpret_cast<unsigned *>(scal + 7);
+  const double one = 1.0;
+  if (rc == CTN_OK && cudaMemcpyAsync(scal, &one, sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess)
+    rc = CTN_ERR_CUDA;
+  if (rc == CTN_OK)
+    rc = krylov_step_any<double>(w, u, nullptr, q, dst, n, scal, nullptr, scal + 1, scal + 2, scal + 3, ws, ws2, err,
+                                 st, 1u, spin_limit);
+  unsigned herr = 0;
+  if (rc == CTN_OK && (cudaMemcpyAsync(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                       cudaStreamSynchronize(st) != cudaSuccess))
+    rc = CTN_ERR_CUDA;
+  cudaFree(buf);
+  if (rc != CTN_OK) return rc;
+  if (herr) {
+    set_error("fused Krylov step: the grid barrier's bounded wait expired");
+    return CTN_ERR_TIMEOUT;
+  }
+  set_error("ctn_selftest_barrier_timeout: the kernel passed its barrier");
+  return CTN_ERR_INVALID;
+}
+}  // namespace ctn
+
+extern "C" ctn_status ctn_selftest_barrier_timeout(long long spin_limit, void *stream) {
+  CTN_REQUIRE(spin_limit > 0, "ctn_selftest_barrier_timeout: spin_limit must be positive");
+  return ctn::selftest_barrier_timeout(spin_limit, ctn::as_stream(stream));
+}

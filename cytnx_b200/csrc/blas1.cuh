@@ -32,6 +32,16 @@ ctn_status lanczos_step_f64(const double *w, const double *u, const double *up, 
 ctn_status lanczos_step_f64(const float *w, const double *u, const double *up, const double *q, double *dst,
                             int64_t n, const double *alpha, const double *gamma, const double *s, const double *sp,
                             double *nrm, double *ws, cudaStream_t st);
+// dot2s_f64 then lanczos_step_f64 (out_a -> alpha, out_b -> gamma, q required) in one
+// cooperative launch with a bounded grid barrier; ws and ws2 as for the two; a barrier wait
+// that runs out sets *err (device word, zeroed by the caller) and alpha to NaN.  Returns
+// CTN_ERR_UNSUPPORTED without launching when the device has no cooperative launch.
+ctn_status krylov_step_f64(const double *w, const double *u, const double *up, const double *q, double *dst,
+                           int64_t n, const double *s, const double *sp, double *out_alpha, double *out_gamma,
+                           double *nrm, double *ws, double *ws2, unsigned *err, cudaStream_t st);
+ctn_status krylov_step_f64(const float *w, const double *u, const double *up, const double *q, double *dst,
+                           int64_t n, const double *s, const double *sp, double *out_alpha, double *out_gamma,
+                           double *nrm, double *ws, double *ws2, unsigned *err, cudaStream_t st);
 ctn_status div_copy_f64(const double *x, double *y, int64_t n, const double *a, cudaStream_t st);
 ctn_status combine_f64(const double *K, int64_t n, int m, const double *c, double *out, cudaStream_t st);
 // block Krylov helpers (basis V: m vectors of n doubles back to back)

@@ -305,13 +305,16 @@ ctn_status lanczos_refined(int (*mv_lo)(void *, const double *, double *, void *
   CTN_REQUIRE(krydim >= 2 && max_restarts >= 1 && n > 0 && tol >= 0, "[Lanczos refined] bad argument");
   // work: [w n][scalars 8][reduction ws][two-sum ws][Ritz coefficients m][alpha m][beta m]
   double *w = work;
-  double *scal = work + n;  // [0] norm [1] theta [3] rho [4] gamma (overlap with q0)
+  double *scal = work + n;  // [0] norm [1] theta [3] rho [4] gamma (overlap with q0) [6] error word
   double *ws = work + n + 8;
   double *ws2 = ws + reduce_ws_bytes() / sizeof(double);
   double *cdev = ws2 + reduce2_ws_bytes() / sizeof(double);
   double *alpha = cdev + krydim;
   double *beta = alpha + krydim;
   CTN_CUDA(cudaMemsetAsync(ws, 0, reduce_ws_bytes() + reduce2_ws_bytes(), st));
+  unsigned *err = reinterpret_cast<unsigned *>(scal + 6);
+  CTN_CUDA(cudaMemsetAsync(err, 0, sizeof(double), st));
+  bool fused = true;  // one cooperative launch per Krylov step while the device supports it
   double host = 0.0;
   int64_t n_lo = 0, n_hi = 0;
   CTN_TRY(nrm2_f64(psi0, n, scal + 0, ws, st));
@@ -352,6 +355,13 @@ ctn_status lanczos_refined(int (*mv_lo)(void *, const double *, double *, void *
       if (mv_lo(u_lo, uj, w, st) != 0) return CTN_ERR_CUDA;
       ++n_lo;
       auto step = [&](const auto *wv) -> ctn_status {
+        if (fused && j + 1 < krydim) {
+          const ctn_status r = krylov_step_f64(wv, uj, up, q0, krylov + (int64_t)(j + 1) * n, n, beta + j - 1,
+                                               j >= 2 ? beta + j - 2 : nullptr, alpha + j, scal + 4, beta + j, ws,
+                                               ws2, err, st);
+          if (r != CTN_ERR_UNSUPPORTED) return r;
+          fused = false;
+        }
         CTN_TRY(dot2s_f64(wv, uj, q0, n, beta + j - 1, alpha + j, scal + 4, ws2, st));
         if (j + 1 < krydim)
           CTN_TRY(lanczos_step_f64(wv, uj, up, q0, krylov + (int64_t)(j + 1) * n, n, alpha + j, scal + 4,
@@ -364,7 +374,13 @@ ctn_status lanczos_refined(int (*mv_lo)(void *, const double *, double *, void *
     }
     CTN_CUDA(cudaMemcpyAsync(As.data(), alpha, sizeof(double) * krydim, cudaMemcpyDeviceToHost, st));
     CTN_CUDA(cudaMemcpyAsync(Bs.data(), beta, sizeof(double) * krydim, cudaMemcpyDeviceToHost, st));
+    unsigned err_host = 0;
+    CTN_CUDA(cudaMemcpyAsync(&err_host, err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     CTN_CUDA(cudaStreamSynchronize(st));
+    if (err_host) {
+      set_error("[Lanczos refined] the grid barrier of a fused Krylov step gave up waiting");
+      return CTN_ERR_TIMEOUT;
+    }
     // a zero beta (breakdown) ends the Krylov space there
     int m = krydim;
     for (int j = 0; j + 1 < krydim; ++j)

@@ -204,6 +204,14 @@ ctn_status ctn_split_gemm_f64_noalloc(int64_t M, int64_t N, int64_t K, const dou
  * Synchronises the stream.  No counterpart in the reference (its kernels do not wait). */
 ctn_status ctn_selftest_wait_timeout(int precision, long long spin_limit, void *stream);
 
+/* Self-test of the bounded grid barrier of the fused Krylov step of ctn_lanczos_refined:
+ * one cooperative launch on a 16384-element vector whose barrier waits for an arrival that
+ * never comes, so every CTA's wait runs out after `spin_limit` probes (about 64 ns each) and
+ * raises the error word.  Returns CTN_ERR_TIMEOUT when that path works (CTN_ERR_UNSUPPORTED
+ * without cooperative launch); the context stays usable.  Allocates a small device buffer and
+ * synchronises the stream.  No counterpart in the reference. */
+ctn_status ctn_selftest_barrier_timeout(long long spin_limit, void *stream);
+
 /* ---------------------------------------------------------------- BLAS-1 (FP64)
  * Results of reductions land in device memory (out points to device doubles). */
 ctn_status ctn_dot_f64(const double *x, const double *y, int64_t n, double *out, void *stream);
@@ -323,8 +331,10 @@ ctn_status ctn_lanczos_gnd(ctn_matvec_fn matvec, void *user, const double *psi0,
  * an FP64 re-orthogonalisation against q0, FP64 tridiagonal solve, v <- Ritz vector.  Stops
  * when |r| <= tol * |E| or after max_restarts FP64 matvecs.  krylov: krydim * n doubles;
  * work >= n + 3200 + 3 * krydim doubles.  The Krylov steps keep alpha / beta on the device
- * (one host synchronisation per restart).  *energy / *residual: FP64 Rayleigh quotient
- * and |r| of the returned unit vector; matvecs[0..1] = low / FP64 products used.
+ * (one host synchronisation per restart); each step's two reductions and its update run as
+ * one cooperative launch whose grid barrier is a bounded wait (CTN_ERR_TIMEOUT if it gives
+ * up).  *energy / *residual: FP64 Rayleigh quotient and |r| of the returned unit vector;
+ * matvecs[0..1] = low / FP64 products used.
  * No direct counterpart in the reference (its Lanczos_ER restarts in one precision,
  * src/linalg/Lanczos_ER.cpp); the recurrence is that of Lanczos_Gnd_Ut. */
 ctn_status ctn_lanczos_refined(ctn_matvec_fn matvec_lo, void *user_lo, ctn_matvec_fn matvec_hi,

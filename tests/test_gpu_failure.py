@@ -50,6 +50,24 @@ def test_nan_in_environment_is_reported():
     assert torch.isfinite(y).all()
 
 
+def test_krylov_grid_barrier_expires_and_context_survives():
+    """The fused Krylov step's grid barrier (ctn_selftest_barrier_timeout: a barrier that waits
+    for one arrival more than the grid has, 2^12 probes per CTA): every CTA's wait runs out,
+    the host sees CTN_ERR_TIMEOUT, and a refined Lanczos run on the same context, whose Krylov
+    steps use the same kernel, still converges."""
+    import cytnx_b200 as c
+    from cytnx_b200 import _lib
+
+    lib = _lib.lib()
+    rc = lib.ctn_selftest_barrier_timeout(1 << 12, _lib.stream_ptr())
+    assert rc == 4, (rc, lib.ctn_last_error())
+    assert b"bounded wait expired" in lib.ctn_last_error()
+    psi, L, M1, M2, R = _build(seed=5)
+    H = c.TwoSiteHeff(L, M1, M2, R, psi)
+    r = H.lanczos_refined(psi, precision="bf16x3", krylov_dim=8, max_restarts=40, tol=1e-10)
+    assert math.isfinite(r["energy"]) and r["residual"] <= 1e-10 * abs(r["energy"])
+
+
 @pytest.mark.parametrize("precision", [1, 2])
 def test_tcgen05_bounded_wait_expires_and_context_survives(precision):
     """The tcgen05 GEMM's bounded waits (ctn_selftest_wait_timeout: a producer that issues no
