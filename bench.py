@@ -348,10 +348,14 @@ def main():
     forms = [args.precision] + [f for f in ("3xtf32", "bf16x3", "fp64") if f != args.precision]
 
     def timed_matvecs(form, steps, sampler=None):
+        """K matvecs replayed from one CUDA graph (TwoSiteHeff.capture: the same kernels as the
+        eager calls without their per-launch host work), W warm-up matvecs from another; also
+        the same K matvecs issued eagerly one call at a time, for comparison."""
         y = torch.empty_like(x)
         H.bind(form)
-        for _ in range(args.warmup):
-            H.apply_flat(x, y, form)
+        warm = H.capture(x, y, form, count=max(1, args.warmup))
+        run = H.capture(x, y, form, count=steps)
+        warm.replay()
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
@@ -360,16 +364,25 @@ def main():
         if sampler is not None:
             sampler.__enter__()
         e0.record(st)
-        for _ in range(steps):
-            H.apply_flat(x, y, form)
+        run.replay()
         e1.record(st)
         torch.cuda.synchronize()
         if sampler is not None:
             sampler.__exit__(None, None, None)
-        t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+        y_graph = y.clone()
+        e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e2.record(st)
+        for _ in range(steps):
+            H.apply_flat(x, y, form)
+        e3.record(st)
+        torch.cuda.synchronize()
+        if not torch.equal(y, y_graph):
+            raise RuntimeError(f"{form}: graph-replayed matvec differs from the eager one")
+        t = torch.tensor([e0.elapsed_time(e1), e2.elapsed_time(e3)], dtype=torch.float64, device=dev)
         if world > 1:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item()), y
+        del warm, run
+        return float(t[0].item()), y, float(t[1].item())
 
     def phases(form):
         ms = (ctypes.c_double * 4)()
@@ -382,9 +395,9 @@ def main():
     results = {}
     sampler = ClockSampler(local)
     for i, form in enumerate(forms):
-        ms, y = timed_matvecs(form, args.steps, sampler if i == 0 else None)
+        ms, y, ms_eager = timed_matvecs(form, args.steps, sampler if i == 0 else None)
         ph, nl = phases(form)
-        results[form] = {"ms_total": ms, "ms_per_matvec": ms / args.steps,
+        results[form] = {"ms_total": ms, "ms_per_matvec": ms / args.steps, "ms_per_matvec_eager": ms_eager / args.steps,
                          "tflops": world * flops * args.steps / (ms * 1e-3) / 1e12, "phase_ms": ph,
                          "launches_per_matvec": nl, "y": y}
     head = results[args.precision]
@@ -580,6 +593,10 @@ def main():
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": head["ms_per_matvec"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": args.precision, "data": "synthetic (seeded numpy PCG64)",
+            "matvec_launch": "the K timed matvecs replayed from one CUDA graph (TwoSiteHeff.capture), "
+                             "checked equal to the eager calls; ms_per_step_eager: the same K issued one call "
+                             "at a time through TwoSiteHeff.apply_flat",
+            "ms_per_step_eager": head["ms_per_matvec_eager"],
             "config": config_base,
             "algorithmic_flops_per_matvec": flops,
             "autotuned_tiles": tiles,

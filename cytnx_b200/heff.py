@@ -58,6 +58,20 @@ def plan_two_site(L: UniTensor, M1: UniTensor, M2: UniTensor, R: UniTensor, psi:
     return h.value, (Lc, M1c, M2c, Rc, Pc), out_bonds, out_layout
 
 
+class MatvecGraph:
+    """Replayable CUDA graph of TwoSiteHeff matvecs (TwoSiteHeff.capture)."""
+
+    def __init__(self, op: "TwoSiteHeff", precision: str, graph, buffers):
+        self._op, self._graph, self._buffers = op, graph, buffers
+        self._prec = _lib.PRECISIONS[precision]
+        self._replans = op._replans.get(self._prec, 0)
+
+    def replay(self) -> None:
+        if self._op._replans.get(self._prec, 0) != self._replans:
+            raise CytnxError("[TwoSiteHeff] the captured matvec graph is stale: set_tiles re-planned its precision")
+        self._graph.replay()
+
+
 class TwoSiteHeff(LinOp):
     def __init__(self, L: UniTensor, M1: UniTensor, M2: UniTensor, R: UniTensor, psi: UniTensor,
                  precision: str = "fp64"):
@@ -77,6 +91,7 @@ class TwoSiteHeff(LinOp):
         self._bound = set()  # precisions whose environments are bound (each has its own workspace)
         self.precision = precision
         self._algo_flops = None
+        self._replans = {}  # per precision: how often set_tiles re-planned it
 
     def __del__(self):
         try:
@@ -105,6 +120,22 @@ class TwoSiteHeff(LinOp):
         _lib.check(_lib.lib().ctn_heff2_matvec(self._h, x.data_ptr(), y.data_ptr(), prec, _lib.stream_ptr()),
                    "TwoSiteHeff.matvec")
 
+    def capture(self, x: torch.Tensor, y: torch.Tensor, precision: Optional[str] = None,
+                count: int = 1) -> "MatvecGraph":
+        """A CUDA graph of `count` matvecs y = H x on these buffers; ``replay()`` runs them again
+        on the current stream without the per-launch host work (the matvec entry point only
+        enqueues kernels and memsets on its stream, so it is capturable).  The graph reads the
+        bound environments and the plan's device tables: it stays valid until set_tiles (or
+        autotune) re-plans this precision, after which replay() raises."""
+        prec = (precision or self.precision).lower()
+        self.apply_flat(x, y, prec)  # binds, uploads the tables, sets kernel attributes
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, capture_error_mode="thread_local"):
+            for _ in range(int(count)):
+                self.apply_flat(x, y, prec)
+        return MatvecGraph(self, prec, g, (x, y))
+
     def matvec(self, v: UniTensor) -> UniTensor:
         lbl = v.labels()
         x = v.contiguous().flat_view()
@@ -119,6 +150,7 @@ class TwoSiteHeff(LinOp):
     def set_tiles(self, bn_step1: int, bn_step4: int, precision: Optional[str] = None) -> None:
         prec = _lib.PRECISIONS[(precision or self.precision).lower()]
         _lib.check(_lib.lib().ctn_heff2_set_tiles(self._h, prec, int(bn_step1), int(bn_step4)), "set_tiles")
+        self._replans[prec] = self._replans.get(prec, 0) + 1  # invalidates captured graphs
         self._ws.pop(prec, None)
         self._bound.discard(prec)
 

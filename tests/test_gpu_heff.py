@@ -297,3 +297,31 @@ def test_refined_lanczos_c_abi_dense_operator(n, krydim):
     hv = Hm.cpu().numpy() @ v
     assert np.linalg.norm(hv - E.value * v) <= 2e-12 * abs(E.value)
     assert cnt[1] == rs.value + 1
+
+
+@pytest.mark.parametrize("form", ["bf16x3", "fp64"])
+def test_captured_matvec_graph_replays_eager_bits(form):
+    """TwoSiteHeff.capture: a CUDA graph of three matvecs replays the eager result bit for bit
+    (also on a new input written into the captured buffer), and re-planning the precision
+    (set_tiles) makes the graph refuse to replay."""
+    import cytnx_b200 as c
+    from cytnx_b200._lib import CytnxError
+
+    psi, L, M1, M2, R = build(256, seed=4)
+    H = c.TwoSiteHeff(L, M1, M2, R, psi)
+    x = psi.flat_view().clone()
+    y = torch.empty_like(x)
+    g = H.capture(x, y, form, count=3)
+    ref = torch.empty_like(x)
+    for seed in (0, 1):
+        x.copy_(torch.randn(x.numel(), dtype=torch.float64, device=x.device,
+                            generator=torch.Generator(device=x.device).manual_seed(seed)))
+        y.zero_()
+        g.replay()
+        H.apply_flat(x, ref, form)
+        torch.cuda.synchronize()
+        assert torch.equal(y, ref)
+    if form != "fp64":
+        H.set_tiles(128, 96, form)
+        with pytest.raises(CytnxError, match="stale"):
+            g.replay()
