@@ -93,12 +93,6 @@ void split_layout(HeffSplit *s) {
   s->total = o;
 }
 
-__device__ __forceinline__ float to_tf32f(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
-}
-
 struct MpoSParams {
   const MpoSegS *segs;
   const MpoTermS *terms;
