@@ -22,7 +22,7 @@
 namespace ctn {
 
 namespace {
-constexpr int BM = 64, BK = 16;  // tile rows and k depth; the tile width BN is 64 or 32
+constexpr int BK = 16;  // k depth of a stage; tiles are BM x BN = 64 x 64, 64 x 32 or 32 x 32
 constexpr int PAD = 4;
 constexpr int NTHREADS = 128;
 
@@ -52,14 +52,14 @@ __device__ __forceinline__ void dmma_16x8x16(double (&c)[4], const double (&a)[8
 // Shared-memory tiles keep the operand's contiguous global axis contiguous, so the
 // cp.async writes are conflict-free; the +4 double padding makes every fragment read
 // pattern below conflict-free as well (bank = 8*x + 2*y for the 4x4 lanes of a phase).
-template <bool TA, bool TB, int BN>
+template <bool TA, bool TB, int BM, int BN>
 struct SmemT {
   double A[2][TA ? BK : BM][(TA ? BM : BK) + PAD];
   double B[2][TB ? BN : BK][(TB ? BK : BN) + PAD];
 };
 
-template <bool TA, bool TB, int BN>
-__device__ __forceinline__ void load_stage(SmemT<TA, TB, BN> &sm, int buf, const double *__restrict__ A,
+template <bool TA, bool TB, int BM, int BN>
+__device__ __forceinline__ void load_stage(SmemT<TA, TB, BM, BN> &sm, int buf, const double *__restrict__ A,
                                            const double *__restrict__ B, const GemmPairD &p, int m, int n,
                                            int m0, int n0, int k0) {
   const int tid = threadIdx.x;
@@ -97,25 +97,27 @@ __device__ __forceinline__ void load_stage(SmemT<TA, TB, BN> &sm, int buf, const
   }
 }
 
-// BN = 64: each of the 4 warps computes a 32 x 32 piece (2 x 4 m16n8 products per k step);
-// BN = 32: a 32 x 16 piece (2 x 2), for plans with too few 64 x 64 tiles to fill the SMs.
-template <bool TA, bool TB, int BN>
+// Each of the 4 warps computes a (BM / 2) x (BN / 2) quarter of the tile: 64 x 64 tiles 2 x 4
+// m16n8 products per k step, 64 x 32 tiles 2 x 2 (plans with too few 64 x 64 tiles to fill the
+// SMs), 32 x 32 tiles 1 x 2 (plans of small blocks, where 64-row tiles are mostly padding).
+template <bool TA, bool TB, int BM, int BN>
 __global__ void __launch_bounds__(NTHREADS) k_gemm_grouped_f64(
     const double *__restrict__ A, const double *__restrict__ B, double *__restrict__ C,
     const GemmTaskD *__restrict__ tasks, const GemmPairD *__restrict__ pairs,
     const GemmTileD *__restrict__ tiles, int64_t ntiles) {
+  constexpr int MI = BM / 32;  // m16 products per warp
   constexpr int NJ = BN / 16;  // n8 products per warp
-  __shared__ __align__(16) SmemT<TA, TB, BN> sm;
+  __shared__ __align__(16) SmemT<TA, TB, BM, BN> sm;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int wm = (warp >> 1) * 32, wn = (warp & 1) * (BN / 2);
+  const int wm = (warp >> 1) * (BM / 2), wn = (warp & 1) * (BN / 2);
   const int g = lane >> 2, t4 = lane & 3;
   for (int64_t ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
     const GemmTileD tile = tiles[ti];
     const GemmTaskD task = tasks[tile.task];
     const int m0 = tile.m0, n0 = tile.n0;
-    double acc[2][NJ][4];
+    double acc[MI][NJ][4];
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < MI; ++i)
 #pragma unroll
       for (int j = 0; j < NJ; ++j)
 #pragma unroll
@@ -130,7 +132,7 @@ __global__ void __launch_bounds__(NTHREADS) k_gemm_grouped_f64(
     GemmPairD cur;
     if (have) {
       cur = pairs[task.pair_begin + pi];
-      load_stage<TA, TB, BN>(sm, 0, A, B, cur, task.m, task.n, m0, n0, 0);
+      load_stage<TA, TB, BM, BN>(sm, 0, A, B, cur, task.m, task.n, m0, n0, 0);
     }
     cp_async_commit();
     while (have) {
@@ -143,13 +145,13 @@ __global__ void __launch_bounds__(NTHREADS) k_gemm_grouped_f64(
         if (npi < npairs) nxt = pairs[task.pair_begin + npi];
       }
       const bool have_next = npi < npairs;
-      if (have_next) load_stage<TA, TB, BN>(sm, buf ^ 1, A, B, nxt, task.m, task.n, m0, n0, nkt * BK);
+      if (have_next) load_stage<TA, TB, BM, BN>(sm, buf ^ 1, A, B, nxt, task.m, task.n, m0, n0, nkt * BK);
       cp_async_commit();
       cp_async_wait<1>();
       __syncthreads();
-      double a[2][8], b[NJ][4];
+      double a[MI][8], b[NJ][4];
 #pragma unroll
-      for (int i = 0; i < 2; ++i)
+      for (int i = 0; i < MI; ++i)
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
           const int r = wm + i * 16 + g + 8 * (e & 1), k = t4 + 4 * (e >> 1);
@@ -163,7 +165,7 @@ __global__ void __launch_bounds__(NTHREADS) k_gemm_grouped_f64(
           b[j][e] = TB ? sm.B[buf][cidx][k] : sm.B[buf][k][cidx];
         }
 #pragma unroll
-      for (int i = 0; i < 2; ++i)
+      for (int i = 0; i < MI; ++i)
 #pragma unroll
         for (int j = 0; j < NJ; ++j) dmma_16x8x16(acc[i][j], a[i], b[j]);
       __syncthreads();
@@ -176,7 +178,7 @@ __global__ void __launch_bounds__(NTHREADS) k_gemm_grouped_f64(
     cp_async_wait<0>();
     double *Cp = C + task.c_off;
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < MI; ++i)
 #pragma unroll
       for (int j = 0; j < NJ; ++j) {
         const int r0 = m0 + wm + i * 16 + g;
@@ -196,14 +198,14 @@ __global__ void __launch_bounds__(NTHREADS) k_gemm_grouped_f64(
 }  // namespace
 
 void build_tiles_f64(const std::vector<GemmTaskD> &tasks, const std::vector<GemmPairD> &pairs,
-                     std::vector<GemmTileD> &tiles, int bn) {
+                     std::vector<GemmTileD> &tiles, int bm, int bn) {
   tiles.clear();
   std::vector<std::pair<double, GemmTileD>> tmp;
   for (size_t t = 0; t < tasks.size(); ++t) {
     const GemmTaskD &tk = tasks[t];
     double kt = 0;
     for (int p = 0; p < tk.pair_count; ++p) kt += std::max(0, pairs[tk.pair_begin + p].k);
-    for (int m0 = 0; m0 < tk.m; m0 += BM)
+    for (int m0 = 0; m0 < tk.m; m0 += bm)
       for (int n0 = 0; n0 < tk.n; n0 += bn) {
         GemmTileD g;
         g.task = (int32_t)t;
@@ -220,7 +222,7 @@ void build_tiles_f64(const std::vector<GemmTaskD> &tasks, const std::vector<Gemm
 
 ctn_status launch_gemm_f64(const double *A, const double *B, double *C, const GemmTaskD *d_tasks,
                            const GemmPairD *d_pairs, const GemmTileD *d_tiles, int64_t ntiles, int flags,
-                           int bn, cudaStream_t st) {
+                           int bm, int bn, cudaStream_t st) {
   if (ntiles == 0) return CTN_OK;
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
@@ -228,19 +230,26 @@ ctn_status launch_gemm_f64(const double *A, const double *B, double *C, const Ge
   // 128 threads, ~17 KB smem: up to 8+ CTAs per SM resident
   const int64_t grid = std::min<int64_t>(ntiles, (int64_t)nsm * 12);
   auto go = [&](auto kern) { kern<<<(unsigned)grid, NTHREADS, 0, st>>>(A, B, C, d_tasks, d_pairs, d_tiles, ntiles); };
-  if (bn == 32) {
+  if (bm == 32) {
     switch (flags & 3) {
-      case 0: go(k_gemm_grouped_f64<false, false, 32>); break;
-      case 1: go(k_gemm_grouped_f64<true, false, 32>); break;
-      case 2: go(k_gemm_grouped_f64<false, true, 32>); break;
-      default: go(k_gemm_grouped_f64<true, true, 32>); break;
+      case 0: go(k_gemm_grouped_f64<false, false, 32, 32>); break;
+      case 1: go(k_gemm_grouped_f64<true, false, 32, 32>); break;
+      case 2: go(k_gemm_grouped_f64<false, true, 32, 32>); break;
+      default: go(k_gemm_grouped_f64<true, true, 32, 32>); break;
+    }
+  } else if (bn == 32) {
+    switch (flags & 3) {
+      case 0: go(k_gemm_grouped_f64<false, false, 64, 32>); break;
+      case 1: go(k_gemm_grouped_f64<true, false, 64, 32>); break;
+      case 2: go(k_gemm_grouped_f64<false, true, 64, 32>); break;
+      default: go(k_gemm_grouped_f64<true, true, 64, 32>); break;
     }
   } else {
     switch (flags & 3) {
-      case 0: go(k_gemm_grouped_f64<false, false, 64>); break;
-      case 1: go(k_gemm_grouped_f64<true, false, 64>); break;
-      case 2: go(k_gemm_grouped_f64<false, true, 64>); break;
-      default: go(k_gemm_grouped_f64<true, true, 64>); break;
+      case 0: go(k_gemm_grouped_f64<false, false, 64, 64>); break;
+      case 1: go(k_gemm_grouped_f64<true, false, 64, 64>); break;
+      case 2: go(k_gemm_grouped_f64<false, true, 64, 64>); break;
+      default: go(k_gemm_grouped_f64<true, true, 64, 64>); break;
     }
   }
   CTN_CHECK_LAUNCH();

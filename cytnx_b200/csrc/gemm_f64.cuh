@@ -1,5 +1,6 @@
 // Device-side task tables of the grouped FP64 GEMM and the owning host object.
 #pragma once
+#include <algorithm>
 #include <cstdint>
 #include <vector>
 
@@ -9,6 +10,9 @@ namespace ctn {
 
 #ifndef F64_NARROW_BELOW
 #define F64_NARROW_BELOW 6  // 64 x 32 tiles when a plan has fewer 64 x 64 tiles than this many per SM
+#endif
+#ifndef F64_SMALL_PADDING
+#define F64_SMALL_PADDING 1.25  // 32 x 32 tiles when the wider tiles execute this many times the products of 32 x 32 tiles
 #endif
 
 struct GemmTaskD {
@@ -27,10 +31,10 @@ struct GemmTileD {
 };
 
 void build_tiles_f64(const std::vector<GemmTaskD> &tasks, const std::vector<GemmPairD> &pairs,
-                     std::vector<GemmTileD> &tiles, int bn);
+                     std::vector<GemmTileD> &tiles, int bm, int bn);
 ctn_status launch_gemm_f64(const double *A, const double *B, double *C, const GemmTaskD *d_tasks,
                            const GemmPairD *d_pairs, const GemmTileD *d_tiles, int64_t ntiles, int flags,
-                           int bn, cudaStream_t st);
+                           int bm, int bn, cudaStream_t st);
 
 // Host tables + their device copy (uploaded once, on the first launch on a device).
 struct GroupedGemmF64 {
@@ -41,18 +45,30 @@ struct GroupedGemmF64 {
   int d_dev = -1;
   double flops = 0.0;
   int flags = 0;          // operand orientation shared by every pair of the plan
-  int bn = 64;            // tile width: 64, or 32 when 64-wide tiles would not fill the SMs
+  int bm = 64, bn = 64;   // tile: 64 x 64; 64 x 32 when 64 x 64 would not fill the SMs; 32 x 32 for small blocks
   bool mixed = false;     // pairs disagree on the orientation (rejected at run time)
 
+  // products the tiles execute, with K padded to the 16-deep stages
+  double executed(int tm, int tn) const {
+    double w = 0.0;
+    for (const auto &t : tasks) {
+      double kp = 0.0;
+      for (int p = 0; p < t.pair_count; ++p) kp += (double)((std::max(0, pairs[t.pair_begin + p].k) + 15) / 16 * 16);
+      w += (double)((t.m + tm - 1) / tm) * tm * (double)((t.n + tn - 1) / tn) * tn * kp;
+    }
+    return w;
+  }
   void finalize() {
     // fewer than six 64 x 64 tiles per SM (148 SMs; about 1.5 waves of four resident CTAs):
-    // 64 x 32 tiles, twice as many CTAs, less padding on narrow groups and a fuller last wave
+    // 64 x 32 tiles, twice as many CTAs, less padding on narrow groups and a fuller last wave;
+    // blocks so small that these tiles execute F64_SMALL_PADDING times the products of 32 x 32
+    // tiles (D ~ 1000 two-site problems: sectors of 2-68 states): 32 x 32 tiles
+    bm = 64;
     bn = 64;
-    build_tiles_f64(tasks, pairs, tiles, bn);
-    if (tiles.size() < F64_NARROW_BELOW * 148) {
-      bn = 32;
-      build_tiles_f64(tasks, pairs, tiles, bn);
-    }
+    build_tiles_f64(tasks, pairs, tiles, bm, bn);
+    if (tiles.size() < F64_NARROW_BELOW * 148) bn = 32;
+    if (executed(bm, bn) > F64_SMALL_PADDING * executed(32, 32)) bm = bn = 32;
+    if (bm != 64 || bn != 64) build_tiles_f64(tasks, pairs, tiles, bm, bn);
     flags = pairs.empty() ? 0 : (pairs[0].flags & 3);
     mixed = false;
     for (const auto &p : pairs) mixed |= ((p.flags & 3) != flags);
@@ -95,7 +111,7 @@ struct GroupedGemmF64 {
     const GemmTaskD *dt = (const GemmTaskD *)p;
     const GemmPairD *dp = (const GemmPairD *)(p + tasks.size() * sizeof(GemmTaskD));
     const GemmTileD *dl = (const GemmTileD *)(p + tasks.size() * sizeof(GemmTaskD) + pairs.size() * sizeof(GemmPairD));
-    return launch_gemm_f64(A, B, C, dt, dp, dl, (int64_t)tiles.size(), flags, bn, st);
+    return launch_gemm_f64(A, B, C, dt, dp, dl, (int64_t)tiles.size(), flags, bm, bn, st);
   }
   ~GroupedGemmF64() {
     if (d_mem) cudaFree(d_mem);
