@@ -65,11 +65,12 @@ struct VecT<16> { using T = U128; };
 // col = u % row_units; the row's input offset comes from decomposing `row` over
 // the new axes 0..rank-2.
 // IT: index type of the decomposition (32-bit when every index fits: integer division
-// is several times cheaper than in 64 bits, and it runs once per copied unit).
+// is several times cheaper than in 64 bits, and it runs once per copied unit).  The input
+// strides in g are in units (the host divides them exactly: every stride of an outer axis is
+// a multiple of the row, which is a whole number of units).
 template <typename U, typename IT>
 __global__ void __launch_bounds__(256) k_row_gather(const U *__restrict__ src, U *__restrict__ dst,
-                                                    PermGeom g, int64_t row_units,
-                                                    int64_t total_units, int64_t in_row_stride_units_scale) {
+                                                    PermGeom g, int64_t row_units, int64_t total_units) {
   int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t step = (int64_t)gridDim.x * blockDim.x;
   const IT ru = (IT)row_units;
@@ -77,14 +78,14 @@ __global__ void __launch_bounds__(256) k_row_gather(const U *__restrict__ src, U
     const IT uu = (IT)u;
     IT row = uu / ru;
     const IT col = uu - row * ru;
-    int64_t off = 0;  // input element offset of the row start
+    int64_t off = 0;  // input unit offset of the row start
     for (int i = g.rank - 2; i >= 0; --i) {
       const IT d = (IT)g.out_shape[i];
       const IT q = row / d;
       off += (int64_t)(row - q * d) * g.in_stride_of_out[i];
       row = q;
     }
-    dst[u] = src[off / in_row_stride_units_scale + col];
+    dst[u] = src[off + col];
   }
 }
 
@@ -103,28 +104,32 @@ struct TransGeom {
   int64_t bout[kMaxRank];   // their output strides
 };
 
-template <typename T>
+// IT: the integer type of the tile and batch index arithmetic (32-bit when the tile count
+// and every batch axis fit, which turns the per-tile divisions from 64-bit software routines
+// into 32-bit ones); element offsets stay 64-bit.
+template <typename T, typename IT>
 __global__ void __launch_bounds__(256) k_transpose(const T *__restrict__ src, T *__restrict__ dst,
                                                    TransGeom g) {
   __shared__ T tile[32][33];
-  const int64_t ntile = g.tiles_a * g.tiles_b;
-  const int64_t total = ntile * g.batch;
-  for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
-    int64_t bidx = t / ntile;
-    int64_t tt = t - bidx * ntile;
-    int64_t tb = tt / g.tiles_a;
-    int64_t ta = tt - tb * g.tiles_a;
+  const IT tiles_a = (IT)g.tiles_a;
+  const IT ntile = (IT)(g.tiles_a * g.tiles_b);
+  const IT total = (IT)(g.tiles_a * g.tiles_b * g.batch);
+  for (IT t = blockIdx.x; t < total; t += gridDim.x) {
+    const IT bidx = t / ntile;
+    const IT tt = t - bidx * ntile;
+    const IT tb = tt / tiles_a;
+    const IT ta = tt - tb * tiles_a;
     int64_t in_off = 0, out_off = 0;
-    int64_t r = bidx;
+    IT r = bidx;
     for (int i = g.nbatch_dims - 1; i >= 0; --i) {
-      int64_t d = g.bshape[i];
-      int64_t q = r / d;
-      int64_t c = r - q * d;
-      in_off += c * g.bin[i];
-      out_off += c * g.bout[i];
+      const IT d = (IT)g.bshape[i];
+      const IT q = r / d;
+      const IT c = r - q * d;
+      in_off += (int64_t)c * g.bin[i];
+      out_off += (int64_t)c * g.bout[i];
       r = q;
     }
-    const int64_t a0 = ta * 32, b0 = tb * 32;
+    const int64_t a0 = (int64_t)ta * 32, b0 = (int64_t)tb * 32;
     // read: rows of b, contiguous along a
     const int64_t ia = a0 + threadIdx.x;
 #pragma unroll
@@ -183,7 +188,7 @@ __global__ void __launch_bounds__(256) k_transpose_short(const T *__restrict__ s
 // compile time so the staging registers stay few (occupancy carries the bytes in flight).
 constexpr int STAGED_THREADS = 256;
 
-template <typename T, int NB, int APT>
+template <typename T, int NB, int APT, typename IT>
 __global__ void __launch_bounds__(STAGED_THREADS) k_transpose_staged(const T *__restrict__ src, T *__restrict__ dst,
                                                                      TransGeom g) {
   extern __shared__ __align__(16) unsigned char staged_smem[];
@@ -191,18 +196,18 @@ __global__ void __launch_bounds__(STAGED_THREADS) k_transpose_staged(const T *__
   constexpr int TA = STAGED_THREADS * APT;
   const int nb = (int)g.nb;
   const int tid = threadIdx.x;
-  const int64_t tiles_a = (g.na + TA - 1) / TA;
-  const int64_t total = tiles_a * g.batch;
-  for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
-    int64_t bidx = t / tiles_a;
-    const int64_t a0 = (t - bidx * tiles_a) * TA;
+  const IT tiles_a = (IT)((g.na + TA - 1) / TA);
+  const IT total = (IT)((g.na + TA - 1) / TA * g.batch);
+  for (IT t = blockIdx.x; t < total; t += gridDim.x) {
+    IT bidx = t / tiles_a;
+    const int64_t a0 = (int64_t)(t - bidx * tiles_a) * TA;
     int64_t in_off = 0, out_off = 0;
     for (int i = g.nbatch_dims - 1; i >= 0; --i) {
-      const int64_t d = g.bshape[i];
-      const int64_t q = bidx / d;
-      const int64_t c = bidx - q * d;
-      in_off += c * g.bin[i];
-      out_off += c * g.bout[i];
+      const IT d = (IT)g.bshape[i];
+      const IT q = bidx / d;
+      const IT c = bidx - q * d;
+      in_off += (int64_t)c * g.bin[i];
+      out_off += (int64_t)c * g.bout[i];
       bidx = q;
     }
     const int cnt_a = (int)(g.na - a0 < TA ? g.na - a0 : TA);
@@ -253,10 +258,15 @@ static bool launch_staged_nb(const void *src, void *dst, const TransGeom &g, int
   const int64_t ta = (int64_t)STAGED_THREADS * apt;
   const int64_t total = (g.na + ta - 1) / ta * g.batch;
   const int64_t blocks = std::min<int64_t>(total, (int64_t)nsm * 64);
-  if (apt == 2)
-    k_transpose_staged<T, NB, 2><<<(unsigned)blocks, STAGED_THREADS, smem, st>>>((const T *)src, (T *)dst, g);
+  const bool narrow = total + blocks < ((int64_t)1 << 32);  // 32-bit tile arithmetic
+  if (apt == 2 && narrow)
+    k_transpose_staged<T, NB, 2, uint32_t><<<(unsigned)blocks, STAGED_THREADS, smem, st>>>((const T *)src, (T *)dst, g);
+  else if (apt == 2)
+    k_transpose_staged<T, NB, 2, int64_t><<<(unsigned)blocks, STAGED_THREADS, smem, st>>>((const T *)src, (T *)dst, g);
+  else if (narrow)
+    k_transpose_staged<T, NB, 1, uint32_t><<<(unsigned)blocks, STAGED_THREADS, smem, st>>>((const T *)src, (T *)dst, g);
   else
-    k_transpose_staged<T, NB, 1><<<(unsigned)blocks, STAGED_THREADS, smem, st>>>((const T *)src, (T *)dst, g);
+    k_transpose_staged<T, NB, 1, int64_t><<<(unsigned)blocks, STAGED_THREADS, smem, st>>>((const T *)src, (T *)dst, g);
   return true;
 }
 
@@ -321,7 +331,8 @@ __device__ __forceinline__ uint4 rotl128(uint4 x, int bits) {
   return y;
 }
 
-template <int ES>
+// IT: integer type of the tile and batch index arithmetic (32-bit when it fits)
+template <int ES, typename IT>
 __global__ void __launch_bounds__(TMA_THREADS) k_transpose_tma(const __grid_constant__ CUtensorMap in_map,
                                                               uint8_t *__restrict__ dst, TmaGeom g) {
   constexpr int TA = 128 / ES;
@@ -332,8 +343,9 @@ __global__ void __launch_bounds__(TMA_THREADS) k_transpose_tma(const __grid_cons
   __shared__ __align__(1024) uint8_t buf[2][TILE];
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ int stop;
-  const int64_t ntile = g.tiles_a * g.tiles_b;
-  const int64_t total = ntile * g.batch;
+  const IT tiles_a = (IT)g.tiles_a;
+  const IT ntile = (IT)(g.tiles_a * g.tiles_b);
+  const IT total = (IT)(g.tiles_a * g.tiles_b * g.batch);
   if (threadIdx.x == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem32(&bar[0])));
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem32(&bar[1])));
@@ -344,24 +356,27 @@ __global__ void __launch_bounds__(TMA_THREADS) k_transpose_tma(const __grid_cons
   struct C5 {
     int x0, x1, x2, x3, x4;
   };
-  auto coords = [&](int64_t t) -> C5 {
-    int64_t bidx = t / ntile, tt = t - bidx * ntile;
-    const int64_t tb = tt / g.tiles_a, ta = tt - tb * g.tiles_a;
+  auto coords = [&](IT t) -> C5 {
+    IT bidx = t / ntile;
+    const IT tt = t - bidx * ntile;
+    const IT tb = tt / tiles_a, ta = tt - tb * tiles_a;
     C5 c{(int)(ta * TA), (int)(tb * TMA_TB), 0, 0, 0};
     if (g.nbatch > 0) {
-      const int64_t q = bidx / g.bshape[0];
-      c.x2 = (int)(bidx - q * g.bshape[0]);
+      const IT d = (IT)g.bshape[0];
+      const IT q = bidx / d;
+      c.x2 = (int)(bidx - q * d);
       bidx = q;
     }
     if (g.nbatch > 1) {
-      const int64_t q = bidx / g.bshape[1];
-      c.x3 = (int)(bidx - q * g.bshape[1]);
+      const IT d = (IT)g.bshape[1];
+      const IT q = bidx / d;
+      c.x3 = (int)(bidx - q * d);
       bidx = q;
     }
     if (g.nbatch > 2) c.x4 = (int)bidx;
     return c;
   };
-  auto issue = [&](int64_t t, int slot) {
+  auto issue = [&](IT t, int slot) {
     const C5 c = coords(t);
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem32(&bar[slot])), "r"(TILE)
                  : "memory");
@@ -372,12 +387,12 @@ __global__ void __launch_bounds__(TMA_THREADS) k_transpose_tma(const __grid_cons
         "r"(smem32(&bar[slot]))
         : "memory");
   };
-  int64_t t = blockIdx.x;
+  IT t = blockIdx.x;
   if (threadIdx.x == 0 && t < total) issue(t, 0);
   uint32_t phase[2] = {0, 0};
   for (int i = 0; t < total; ++i, t += gridDim.x) {
     const int slot = i & 1;
-    const int64_t tn = t + gridDim.x;
+    const IT tn = t + gridDim.x;
     if (threadIdx.x == 0) {
       if (tn < total) issue(tn, slot ^ 1);  // that buffer was released by the last __syncthreads
       bool ok = false;
@@ -532,7 +547,10 @@ static bool try_transpose_tma(const void *src, void *dst, int r, const int64_t *
     return false;
   const int64_t total = g.tiles_a * g.tiles_b * g.batch;
   const int64_t blocks = std::min<int64_t>(total, (int64_t)sm_count() * 8);
-  k_transpose_tma<ES><<<(unsigned)blocks, TMA_THREADS, 0, st>>>(map, (uint8_t *)dst, g);
+  if (total + 2 * blocks < ((int64_t)1 << 32))  // t and t + grid stay below 2^32
+    k_transpose_tma<ES, uint32_t><<<(unsigned)blocks, TMA_THREADS, 0, st>>>(map, (uint8_t *)dst, g);
+  else
+    k_transpose_tma<ES, int64_t><<<(unsigned)blocks, TMA_THREADS, 0, st>>>(map, (uint8_t *)dst, g);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_error("CUDA error %s in k_transpose_tma", cudaGetErrorString(e));
@@ -639,6 +657,7 @@ static ctn_status launch_perm(const void *src, void *dst, int rank, const uint64
         break;
       }
     const int64_t scale = vb / ES;  // elements per unit
+    for (int i = 0; i + 1 < r; ++i) g.in_stride_of_out[i] /= scale;  // exact: multiples of L
     const int64_t row_units = L / scale;
     const int64_t total_units = n / scale;
     const int64_t blocks = std::min<int64_t>((total_units + 255) / 256, (int64_t)nsm * 16);
@@ -646,10 +665,10 @@ static ctn_status launch_perm(const void *src, void *dst, int rank, const uint64
 #define CTN_ROW_GATHER(UT)                                                                                        \
   if (small)                                                                                                     \
     k_row_gather<UT, uint32_t><<<(unsigned)blocks, 256, 0, st>>>((const UT *)src, (UT *)dst, g, row_units,     \
-                                                                 total_units, scale);                         \
+                                                                 total_units);                                \
   else                                                                                                           \
     k_row_gather<UT, int64_t><<<(unsigned)blocks, 256, 0, st>>>((const UT *)src, (UT *)dst, g, row_units,      \
-                                                                total_units, scale);
+                                                                total_units);
     switch (vb) {
       case 16:
         CTN_ROW_GATHER(U128);
@@ -713,7 +732,11 @@ static ctn_status launch_perm(const void *src, void *dst, int rank, const uint64
   }
   const int64_t total = g.tiles_a * g.tiles_b * g.batch;
   const int64_t blocks = std::min<int64_t>(total, (int64_t)nsm * 32);
-  k_transpose<T><<<(unsigned)blocks, dim3(32, 8), 0, st>>>((const T *)src, (T *)dst, g);
+  // 32-bit tile arithmetic when the loop variable cannot pass 2^32 (t < total + grid)
+  if (total + blocks < ((int64_t)1 << 32))
+    k_transpose<T, uint32_t><<<(unsigned)blocks, dim3(32, 8), 0, st>>>((const T *)src, (T *)dst, g);
+  else
+    k_transpose<T, int64_t><<<(unsigned)blocks, dim3(32, 8), 0, st>>>((const T *)src, (T *)dst, g);
   CTN_CHECK_LAUNCH();
   return CTN_OK;
 }
