@@ -1031,10 +1031,14 @@ __device__ __forceinline__ void pack_tile_step(const PackTileParams &p, double (
   constexpr int PER = 32 * 8 * E / 256;
   const PackTileItem cur = w;
   __syncthreads();  // the previous item's readers are done with T
+  // column r of staged row k sits at r ^ (k / E % 8): the 8-byte reads below (thread (r, c)
+  // reads rows c * E + e) then spread over all 16 double-width banks (two threads each, the
+  // minimum); without it the BF16 reads were 4-way conflicts
 #pragma unroll
   for (int u = 0; u < PER; ++u) {
     const int idx = threadIdx.x + u * 256;
-    T[idx >> 5][idx & 31] = v[u];
+    const int k = idx >> 5;
+    T[k][(idx & 31) ^ ((k / E) & 7)] = v[u];
   }
   __syncthreads();
   if (next < p.nitems) {
@@ -1046,7 +1050,7 @@ __device__ __forceinline__ void pack_tile_step(const PackTileParams &p, double (
   const int64_t off = cur.panel_off + tc_panel_offset(cur.row0 + r, cur.k0 + c * E, cur.tile_rows, cur.kb, KIND);
   double x[8];
 #pragma unroll
-  for (int e = 0; e < 8; ++e) x[e] = e < E ? T[c * E + e][r] : 0.0;
+  for (int e = 0; e < 8; ++e) x[e] = e < E ? T[c * E + e][r ^ c] : 0.0;
   store_split<KIND>(x, p.hi, p.lo, off);
 }
 
