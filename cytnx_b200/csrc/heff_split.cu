@@ -44,11 +44,23 @@ struct WorkItem {
   int32_t seg0, seg1;  // first and last segment overlapping the item's chunks
   int64_t chunk0;      // global chunk index of the item's first chunk
 };
+// A work item inside one X3 block, with that block's descriptor and its first two terms inline
+// (term_count < 0: the item spans several blocks and takes the table path)
+struct alignas(16) MpoFat {
+  int64_t seg_chunk0;  // global chunk index of the block's first chunk
+  int64_t panel_off;
+  int32_t cols, row0, k0, kb;
+  int32_t term_begin, term_count;
+  int64_t x1_off[2];
+  int32_t ld[2];
+  float coef[2];
+};
 
 
 struct HeffSplit {
   int kind = TC_TF32;
   std::vector<WorkItem> items;
+  std::vector<MpoFat> fat;  // one per item
   TcGemm g1, g4;
   Packer pk_L, pk_P, pk_R;
   std::vector<MpoSegS> segs;
@@ -76,6 +88,40 @@ constexpr int KALIGN = 8;
 
 int64_t up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
+// Inline descriptors of the work items that lie inside one X3 block (D=4096 BF16x3 fold 37.9 ->
+// 35.8 us: a thread's X1 reads then wait on the item alone, not on the block and term tables).
+// Kept only for BF16 panels when at least half of the items are such: with many small blocks (the
+// Hubbard batch) most items span several blocks and the extra 80-byte read per item cost 1.5 %,
+// and the TF32 fold (4-element chunks) ran 1 us slower with them.
+void build_fat(HeffSplit *s) {
+  size_t single = 0;
+  for (const WorkItem &wi : s->items) single += wi.seg0 == wi.seg1;
+  s->fat.clear();
+  if (s->kind != TC_BF16 || 2 * single < s->items.size()) return;
+  s->fat.assign(s->items.size(), MpoFat{});
+  for (size_t i = 0; i < s->items.size(); ++i) {
+    const WorkItem &wi = s->items[i];
+    MpoFat &f = s->fat[i];
+    f.term_count = -1;
+    if (wi.seg0 != wi.seg1) continue;
+    const MpoSegS &sg = s->segs[wi.seg0];
+    f.seg_chunk0 = s->seg_begin[wi.seg0];
+    f.panel_off = sg.panel_off;
+    f.cols = sg.cols;
+    f.row0 = sg.row0;
+    f.k0 = sg.k0;
+    f.kb = sg.kb;
+    f.term_begin = sg.term_begin;
+    f.term_count = sg.term_count;
+    for (int t = 0; t < 2 && t < sg.term_count; ++t) {
+      const MpoTermS &tm = s->terms[sg.term_begin + t];
+      f.x1_off[t] = tm.x1_off;
+      f.ld[t] = (int32_t)tm.ld;
+      f.coef[t] = (float)tm.coef;
+    }
+  }
+}
+
 // workspace layout (bytes): [A1 panel][B1 panel][X1 f32][A4 panel][B4 panel][error word]
 void split_layout(HeffSplit *s) {
   int64_t o = 0;
@@ -94,6 +140,7 @@ void split_layout(HeffSplit *s) {
 }
 
 struct MpoSParams {
+  const MpoFat *fat;
   const MpoSegS *segs;
   const MpoTermS *terms;
   const WorkItem *items;
@@ -174,6 +221,52 @@ __global__ void __launch_bounds__(MPO_THREADS, 6) k_mpo_split(MpoSParams p) {
   constexpr int E = TF ? 4 : 8;
   constexpr int U = MPO_UNROLL;
   for (int64_t it = blockIdx.x; it < p.nitems; it += gridDim.x) {
+    if (p.fat && p.fat[it].term_count >= 0) {  // the item lies in one block: item -> X1, no table lookups
+      const MpoFat f = p.fat[it];
+      const int64_t g = it * MPO_ITEM + threadIdx.x;
+      if (g >= p.nchunks) continue;
+      const int nkc = (f.cols + E - 1) / E;
+      const int cl = (int)(g - f.seg_chunk0);
+      const int r = cl / nkc;
+      const int kloc = (cl - r * nkc) * E;
+      const int nv = min(E, f.cols - kloc);
+      float x[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) x[e] = 0.f;
+      auto add = [&](float cf, const float *src) {
+        if (nv == E) {
+          const float4 v = __ldg(reinterpret_cast<const float4 *>(src));
+          x[0] = fmaf(cf, v.x, x[0]);
+          x[1] = fmaf(cf, v.y, x[1]);
+          x[2] = fmaf(cf, v.z, x[2]);
+          x[3] = fmaf(cf, v.w, x[3]);
+          if (!TF) {
+            const float4 w = __ldg(reinterpret_cast<const float4 *>(src) + 1);
+            x[4] = fmaf(cf, w.x, x[4]);
+            x[5] = fmaf(cf, w.y, x[5]);
+            x[6] = fmaf(cf, w.z, x[6]);
+            x[7] = fmaf(cf, w.w, x[7]);
+          }
+        } else {
+#pragma unroll
+          for (int e = 0; e < E; ++e)
+            if (e < nv) x[e] = fmaf(cf, __ldg(src + e), x[e]);
+        }
+      };
+      if (f.term_count > 0) add(f.coef[0], p.x1 + f.x1_off[0] + (int64_t)r * f.ld[0] + kloc);
+      if (f.term_count > 1) add(f.coef[1], p.x1 + f.x1_off[1] + (int64_t)r * f.ld[1] + kloc);
+      for (int t = 2; t < f.term_count; ++t) {
+        const MpoTermS tm = p.terms[f.term_begin + t];
+        add((float)tm.coef, p.x1 + tm.x1_off + (int64_t)r * tm.ld + kloc);
+      }
+      MpoSegS sg;
+      sg.row0 = f.row0;
+      sg.k0 = f.k0;
+      sg.panel_off = f.panel_off;
+      sg.kb = f.kb;
+      mpo_store<KIND>(x, sg, r, kloc, p.hi, p.lo);
+      continue;
+    }
     const WorkItem wi = p.items[it];
     MpoSegS sg[U];
     int r[U], kloc[U], nv[U], nt[U];
@@ -403,6 +496,7 @@ ctn_status heff_split_prepare(ctn_heff2_plan *p, int kind) {
   }
   s->nchunks = s->seg_begin.back();
   chunk_items(s->seg_begin, MPO_ITEM, s->items);
+  build_fat(s.get());
   split_layout(s.get());
   p->split[kind] = s.release();
   heff_split_apply_epilogue(p, kind);
@@ -445,11 +539,14 @@ ctn_status split_set_env(HeffSplit *s, const void *L, const void *R, void *ws, c
   CTN_CUDA(cudaGetDevice(&dev));
   if (!s->d_mpo || s->d_dev != dev) {
     if (s->d_mpo) cudaFree(s->d_mpo);
-    const size_t bytes = s->segs.size() * sizeof(MpoSegS) + s->terms.size() * sizeof(MpoTermS) +
-                         s->items.size() * sizeof(WorkItem) + s->seg_begin.size() * sizeof(int64_t) + 64;
+    const size_t bytes = s->fat.size() * sizeof(MpoFat) + s->segs.size() * sizeof(MpoSegS) +
+                         s->terms.size() * sizeof(MpoTermS) + s->items.size() * sizeof(WorkItem) +
+                         s->seg_begin.size() * sizeof(int64_t) + 64;
     CTN_CUDA(cudaMalloc(&s->d_mpo, bytes));
     s->d_dev = dev;
     char *q = (char *)s->d_mpo;
+    if (!s->fat.empty()) CTN_CUDA(cudaMemcpyAsync(q, s->fat.data(), s->fat.size() * sizeof(MpoFat), cudaMemcpyHostToDevice, st));
+    q += s->fat.size() * sizeof(MpoFat);
     if (!s->segs.empty()) CTN_CUDA(cudaMemcpyAsync(q, s->segs.data(), s->segs.size() * sizeof(MpoSegS), cudaMemcpyHostToDevice, st));
     q += s->segs.size() * sizeof(MpoSegS);
     if (!s->terms.empty()) CTN_CUDA(cudaMemcpyAsync(q, s->terms.data(), s->terms.size() * sizeof(MpoTermS), cudaMemcpyHostToDevice, st));
@@ -491,6 +588,8 @@ ctn_status split_matvec(HeffSplit *s, const void *psi, void *out, cudaStream_t s
   if (!s->items.empty()) {
     MpoSParams prm;
     const char *q = (const char *)s->d_mpo;
+    prm.fat = s->fat.empty() ? nullptr : (const MpoFat *)q;
+    q += s->fat.size() * sizeof(MpoFat);
     prm.segs = (const MpoSegS *)q;
     prm.terms = (const MpoTermS *)(q + s->segs.size() * sizeof(MpoSegS));
     const size_t o_items = s->segs.size() * sizeof(MpoSegS) + s->terms.size() * sizeof(MpoTermS);
@@ -630,6 +729,7 @@ HeffSplit *split_batch(std::vector<ctn_heff2_plan *> &plans, const int64_t *psi_
   B->pk_R.finalize();
   B->nchunks = B->seg_begin.back();
   chunk_items(B->seg_begin, MPO_ITEM, B->items);
+  build_fat(B.get());
   split_layout(B.get());
   return B.release();
 }
