@@ -291,12 +291,14 @@ static int sm_count() {
 }
 
 // ---------------------------------------------------------------- TMA-staged transpose
-// Tile: TA = 128 / ES elements of axis a (one 128-byte swizzle row) x TB = 32 of axis b.
+// Tile: TA = 128 / ES elements of axis a (one 128-byte swizzle row) x TB = tma_tb(ES) of axis b.
 // The tensor map views the input as [batch2][batch1][batch0][b][a] (a fastest); the
 // shared-memory image of a box row b is 128 bytes whose 16-byte chunks are XOR-swizzled
-// with (b & 7).  Each of the 256 threads writes one 16-byte output vector (16 / ES
-// consecutive b of one a) per tile.
-constexpr int TMA_TB = 64;
+// with (b & 7).  The 256 threads write the tile as 16-byte output vectors (16 / ES
+// consecutive b of one a), TA * TB * ES / 4096 of them each.
+// b rows per staged tile: 128 for 1- and 2-byte elements (16 KB tiles; int16 4.37 -> 4.83 TB/s
+// against 64 rows), 64 for 4-byte ones (128 rows: f32 4.56 -> 4.30 TB/s)
+constexpr int tma_tb(int es) { return es <= 2 ? 128 : 64; }
 constexpr int TMA_THREADS = 256;
 constexpr long long TMA_SPIN = 1ll << 26;  // mbarrier probes before giving up
 
@@ -336,6 +338,7 @@ template <int ES, typename IT>
 __global__ void __launch_bounds__(TMA_THREADS) k_transpose_tma(const __grid_constant__ CUtensorMap in_map,
                                                               uint8_t *__restrict__ dst, TmaGeom g) {
   constexpr int TA = 128 / ES;
+  constexpr int TMA_TB = tma_tb(ES);
   constexpr int TILE = TMA_TB * 128;                   // bytes per staged tile
   constexpr int VEC = 16 / ES;                         // elements per output vector
   constexpr int CHUNKS = TMA_TB / VEC;                 // output vectors per a (along b)
@@ -493,6 +496,7 @@ template <int ES>
 static bool try_transpose_tma(const void *src, void *dst, int r, const int64_t *rshape, const int *rmap,
                               const int64_t *in_stride, const int64_t *out_stride, cudaStream_t st, ctn_status *res) {
   constexpr int TA = 128 / ES;
+  constexpr int TMA_TB = tma_tb(ES);
   const int a = r - 1, b = rmap[r - 1];
   if (r - 2 > 3) return false;
   int64_t nel = 1;
