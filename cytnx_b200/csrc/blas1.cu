@@ -719,13 +719,23 @@ static ctn_status krylov_step_any(const WT *w, const double *u, const double *up
   void (*kern)(const WT *, const double *, const double *, const double *, double *, int64_t, const double *,
                const double *, double *, double *, double *, double *, double *, unsigned *, unsigned, long long) =
       vec ? k_krylov_step<true, WT> : k_krylov_step<false, WT>;
-  int dev = 0, coop = 0, nsm = 0, occ = 0;
+  // resident CTAs of this kernel on the device (queried once per device: the step runs hundreds
+  // of times per solve); 0 = the device has no cooperative launch
+  static int resident[64][2];
+  static bool known[64][2];
+  int dev = 0;
   CTN_CUDA(cudaGetDevice(&dev));
-  CTN_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
-  if (!coop) return CTN_ERR_UNSUPPORTED;
-  CTN_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  CTN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, RT, 0));
-  const int g = std::min(grid_stream(n), std::max(1, nsm * occ));
+  const int di = dev & 63;
+  if (!known[di][vec]) {
+    int coop = 0, nsm = 0, occ = 0;
+    CTN_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    CTN_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    CTN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, RT, 0));
+    resident[di][vec] = coop ? std::max(1, nsm * occ) : 0;
+    known[di][vec] = true;
+  }
+  if (resident[di][vec] == 0) return CTN_ERR_UNSUPPORTED;
+  const int g = std::min(grid_stream(n), resident[di][vec]);
   void *args[] = {(void *)&w,   (void *)&u,         (void *)&up,        (void *)&q,   (void *)&dst,
                   (void *)&n,   (void *)&s,         (void *)&sp,        (void *)&out_alpha,
                   (void *)&out_gamma, (void *)&nrm, (void *)&ws,        (void *)&ws2, (void *)&err,
