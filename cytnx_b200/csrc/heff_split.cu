@@ -12,7 +12,7 @@
 //           out[(a',s1',s2') rows][b'] = X3_b'[rows][(w2,b) K] x R_b'[(w2,b)][b'],
 //           B = R (packed once), FP64 stores straight into the out blocks.
 // The K offsets of the R blocks inside a step-4 group are padded to multiples of 8 so
-// that every 16-byte panel chunk belongs to one X3 block.
+// that every 8-element chunk of the fold (16 bytes of BF16, 32 of TF32) belongs to one X3 block.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -88,16 +88,16 @@ constexpr int KALIGN = 8;
 
 int64_t up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
-// Inline descriptors of the work items that lie inside one X3 block (D=4096 BF16x3 fold 37.9 ->
-// 35.8 us: a thread's X1 reads then wait on the item alone, not on the block and term tables).
-// Kept only for BF16 panels when at least half of the items are such: with many small blocks (the
-// Hubbard batch) most items span several blocks and the extra 80-byte read per item cost 1.5 %,
-// and the TF32 fold (4-element chunks) ran 1 us slower with them.
+// Inline descriptors of the work items that lie inside one X3 block (D=4096 fold 37.9 -> 35.8 us
+// BF16x3, 49.2 -> 47.1 us 3xTF32: a thread's X1 reads then wait on the item alone, not on the
+// block and term tables).  Kept only when at least half of the items are such: with many small
+// blocks (the Hubbard batch) most items span several blocks and the extra 80-byte read per item
+// cost 1.5 %.
 void build_fat(HeffSplit *s) {
   size_t single = 0;
   for (const WorkItem &wi : s->items) single += wi.seg0 == wi.seg1;
   s->fat.clear();
-  if (s->kind != TC_BF16 || 2 * single < s->items.size()) return;
+  if (2 * single < s->items.size()) return;
   s->fat.assign(s->items.size(), MpoFat{});
   for (size_t i = 0; i < s->items.size(); ++i) {
     const WorkItem &wi = s->items[i];
@@ -180,15 +180,18 @@ __device__ __forceinline__ void mpo_store(const float (&x)[8], const MpoSegS &s,
   const int byte = TF ? ((kabs & 15) << 2) : ((kabs & 31) << 1);
   const int64_t off = s.panel_off + ((int64_t)(row >> 7) * s.kb + kslice) * (2 * TC_A_TILE) +
                       tc_tile_byte(rr, byte);  // hi tile; lo = hi + TC_A_TILE
-  if (TF) {
-    float h[4], l[4];
+  if (TF) {  // 8 TF32 = two 16-byte chunks of one 64-byte slice row (kabs is a multiple of 8)
+    const int64_t off1 = off - tc_tile_byte(rr, byte) + tc_tile_byte(rr, byte + 16);
+    float h[8], l[8];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
+    for (int e = 0; e < 8; ++e) {
       h[e] = tf32_rna(x[e]);
       l[e] = tf32_rna(x[e] - h[e]);  // exact in FP32
     }
     *(float4 *)(hi + off) = make_float4(h[0], h[1], h[2], h[3]);
     *(float4 *)(lo + off) = make_float4(l[0], l[1], l[2], l[3]);
+    *(float4 *)(hi + off1) = make_float4(h[4], h[5], h[6], h[7]);
+    *(float4 *)(lo + off1) = make_float4(l[4], l[5], l[6], l[7]);
   } else {
     uint32_t hw[4], lw[4];
 #pragma unroll
@@ -204,21 +207,21 @@ __device__ __forceinline__ void mpo_store(const float (&x)[8], const MpoSegS &s,
   }
 }
 
-// One CTA per work item of MPO_ITEM consecutive chunks (E = 4 TF32 / 8 BF16 elements of
-// one row) of the flattened X3 blocks; an item may span several small blocks (each
-// thread finds its block by a binary search over the blocks the item overlaps).  Blocks
-// are ordered by (a', b), so the blocks that read the same X1 inputs run together and
-// share them in L2.  X1 block rows start on 16-byte boundaries (padded step-1 columns),
-// so full chunks load as float4.  Each thread computes MPO_UNROLL chunks together, MPO_TERMS
-// terms per round (one: the kernel is close to issue-bound, and with 1.4 terms per chunk on
-// average wider rounds mostly issue predicated-off loads and multiplies by zero; 0.0386 ->
-// 0.0371 ms at D=4096 BF16x3 against four).
+// One CTA per work item of MPO_ITEM consecutive chunks (E = 8 elements of one row; 4-element
+// TF32 chunks made the 3xTF32 fold slower, its chunk count and table lookups being twice BF16's)
+// of the flattened X3 blocks; an item may span several small blocks (each thread then finds its
+// block by a binary search over the blocks the item overlaps; items inside one block carry it
+// inline).  Blocks are ordered by (a', b), so the blocks that read the same X1 inputs run
+// together and share them in L2.  X1 block rows start on 16-byte boundaries (padded step-1
+// columns), so full chunks load as float4.  Each thread computes MPO_UNROLL chunks together,
+// MPO_TERMS terms per round (one: with 1.4 terms per chunk on average wider rounds mostly issue
+// predicated-off loads and multiplies by zero; 0.0386 -> 0.0371 ms at D=4096 BF16x3 against
+// four).
 // Six CTAs per SM (40 registers): occupancy over registers, the loads are latency-bound
 // (39 vs 43 us at D=4096 BF16x3 against the unconstrained 44-register build).
 template <int KIND>
 __global__ void __launch_bounds__(MPO_THREADS, 6) k_mpo_split(MpoSParams p) {
-  constexpr bool TF = KIND == TC_TF32;
-  constexpr int E = TF ? 4 : 8;
+  constexpr int E = 8;  // elements per chunk (a thread's share): 32 bytes of X1 per term
   constexpr int U = MPO_UNROLL;
   for (int64_t it = blockIdx.x; it < p.nitems; it += gridDim.x) {
     if (p.fat && p.fat[it].term_count >= 0) {  // the item lies in one block: item -> X1, no table lookups
@@ -240,13 +243,11 @@ __global__ void __launch_bounds__(MPO_THREADS, 6) k_mpo_split(MpoSParams p) {
           x[1] = fmaf(cf, v.y, x[1]);
           x[2] = fmaf(cf, v.z, x[2]);
           x[3] = fmaf(cf, v.w, x[3]);
-          if (!TF) {
-            const float4 w = __ldg(reinterpret_cast<const float4 *>(src) + 1);
-            x[4] = fmaf(cf, w.x, x[4]);
-            x[5] = fmaf(cf, w.y, x[5]);
-            x[6] = fmaf(cf, w.z, x[6]);
-            x[7] = fmaf(cf, w.w, x[7]);
-          }
+          const float4 w = __ldg(reinterpret_cast<const float4 *>(src) + 1);
+          x[4] = fmaf(cf, w.x, x[4]);
+          x[5] = fmaf(cf, w.y, x[5]);
+          x[6] = fmaf(cf, w.z, x[6]);
+          x[7] = fmaf(cf, w.w, x[7]);
         } else {
 #pragma unroll
           for (int e = 0; e < E; ++e)
@@ -310,7 +311,7 @@ __global__ void __launch_bounds__(MPO_THREADS, 6) k_mpo_split(MpoSParams p) {
             cf[j][u] = (float)tm.coef;
             const float4 *src = reinterpret_cast<const float4 *>(p.x1 + tm.x1_off + (int64_t)r[j] * tm.ld + kloc[j]);
             v[j][u] = __ldg(src);
-            if (!TF) w[j][u] = __ldg(src + 1);
+            w[j][u] = __ldg(src + 1);
           }
         }
 #pragma unroll
@@ -321,12 +322,10 @@ __global__ void __launch_bounds__(MPO_THREADS, 6) k_mpo_split(MpoSParams p) {
           x[j][1] = fmaf(cf[j][u], v[j][u].y, x[j][1]);
           x[j][2] = fmaf(cf[j][u], v[j][u].z, x[j][2]);
           x[j][3] = fmaf(cf[j][u], v[j][u].w, x[j][3]);
-          if (!TF) {
-            x[j][4] = fmaf(cf[j][u], w[j][u].x, x[j][4]);
-            x[j][5] = fmaf(cf[j][u], w[j][u].y, x[j][5]);
-            x[j][6] = fmaf(cf[j][u], w[j][u].z, x[j][6]);
-            x[j][7] = fmaf(cf[j][u], w[j][u].w, x[j][7]);
-          }
+          x[j][4] = fmaf(cf[j][u], w[j][u].x, x[j][4]);
+          x[j][5] = fmaf(cf[j][u], w[j][u].y, x[j][5]);
+          x[j][6] = fmaf(cf[j][u], w[j][u].z, x[j][6]);
+          x[j][7] = fmaf(cf[j][u], w[j][u].w, x[j][7]);
         }
     }
 #pragma unroll
@@ -452,7 +451,7 @@ ctn_status heff_split_prepare(ctn_heff2_plan *p, int kind) {
     }
   // ---------------- MPO segments: X3 blocks into the step-4 A panels, ordered by (a', b)
   // (the blocks of one (a', b) read the same X1 blocks)
-  const int E = kind == TC_TF32 ? 4 : 8;
+  const int E = 8;  // fold chunk: 8 elements (16 bytes of BF16 or 32 bytes of TF32 per panel)
   std::map<std::pair<int64_t, int64_t>, std::vector<size_t>> by_ab;
   for (size_t i = 0; i < p->x3.size(); ++i) {
     const X3Info &xi = p->x3[i];
